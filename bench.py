@@ -1,0 +1,329 @@
+"""Benchmark: k-mers compacted per second on one B200 (plain single job).
+
+Workload (default): one synthetic 1 Gbp genome at 41% GC with 5% repeat
+families (300 bp-6 kb, 2-50 copies, 1-3% mutations per copy) and 0.1% SNPs,
+k = 31, ~1B distinct canonical 31-mers, shuffled, in the reference's text
+format, generated on the GPU from a seed.  A step is one pass of the whole
+path (pack, minimizer bucketing, tiles, stitch) over that text.
+
+  value  device-resident throughput: text already in HBM, lines left in HBM
+  e2e    the same through uc_compact_host: pinned host text -> host lines,
+         both copies inside the timed region
+  --impl reference   the CPU arm: the reference path timed on the host cores
+         over a bounded sample of the same workload
+
+Under torchrun every rank runs its own replica (the path does not shard:
+replicas only); value is the sum over ranks, timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "k-mers compacted/s on 1 B200 (plain single job)"
+UNIT = "k-mers/s"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.index), "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def algorithmic_bytes(st: dict, text_bytes: int, k: int) -> dict:
+    """Bytes each phase must move at minimum (each logical array element read
+    or written once), from the run's own counts."""
+    W = 8 if k <= 31 else 16
+    n, cp, S, ob = st["n_kmers"], st["n_copies"], st["n_segments"], st["out_bytes"]
+    return {
+        "pack": text_bytes + n * W,                                # text in, keys out
+        "bucket": n * W + n * 8 + (n * W + n * 8) + cp * (W + 4),  # minimizers+counts, scatter
+        "tiles": cp * (W + 4) + ob,                                # copies in, lines out
+        "stitch": S * 40,                                          # segment records, links, copy
+    }
+
+
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "uc_ref_large")
+
+
+def _cpu_sample(args):
+    """Bounded sample of the workload: the same genome model, shorter."""
+    import torch
+    from unitigcoarsening_b200 import synth
+    spec = synth.scale_plain(length=int(args.cpu_sample), seed=2)
+    with torch.no_grad():
+        return synth.make_text(spec, args.k, device="cpu").numpy().tobytes()
+
+
+def _run_reference_binary(text: bytes, k: int, l: int, threads: int):
+    """The reference's own driver (compiled from its sources against the
+    Kokkos-API shim, OpenMP backend): returns (seconds from its "Total time"
+    line, wall seconds)."""
+    import re
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        inp = os.path.join(td, "in.txt")
+        outp = os.path.join(td, "out.txt")
+        with open(inp, "wb") as f:
+            f.write(text)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="spread", OMP_PLACES="threads")
+        t0 = time.perf_counter()
+        r = subprocess.run([REF_BIN, inp, str(k), str(l), outp], capture_output=True, text=True, env=env,
+                           timeout=600)
+        wall = time.perf_counter() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"reference exited {r.returncode}: {r.stderr[-300:]}")
+        m = re.search(r"Total time: ([0-9.]+)s", r.stdout)
+        return (float(m.group(1)) if m else wall), wall
+
+
+def cpu_baseline(args, steps: int = 1):
+    """Reference CPU path (or, without its binary, the oracle port) timed on
+    the host over a bounded sample; returns the cpu_baseline object."""
+    text = _cpu_sample(args)
+    n = int(text[: text.index(b"\n")])
+    if os.path.exists(REF_BIN):
+        threads = os.cpu_count() or 1
+        ts = [_run_reference_binary(text, args.k, args.l, threads)[0] for _ in range(steps)]
+        sec = sum(ts) / len(ts)
+        kind, cores = "reference", threads
+    else:
+        from oracle import oracle as O
+        O.build()
+        ts = []
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            O.compact(text, args.k)
+            ts.append(time.perf_counter() - t0)
+        sec = sum(ts) / len(ts)
+        kind, cores = "port", 1
+    return {"value": n / sec, "unit": UNIT, "cores": cores, "kind": kind, "seconds": sec,
+            "sample": f"{args.cpu_sample / 1e6:g} Mbp genome of the same model (seed 2), {n} k-mers, "
+                      f"k={args.k}, l={args.l}, text in a file, lines to a file"}
+
+
+def reference_throughput(args):
+    for _ in range(args.warmup):
+        cpu_baseline(args, steps=1)
+    cb = cpu_baseline(args, steps=max(1, args.steps))
+    cfg = {"workload": f"plain single job (bounded CPU sample): {args.cpu_sample / 1e6:g} Mbp genome, 41% GC, "
+                       f"5% repeat families, 0.1% SNPs, k={args.k}", "k": args.k, "l": args.l}
+    return {"value": cb["value"], "ms_per_step": cb["seconds"] * 1e3, "config": cfg, "cpu_baseline": cb}
+
+
+def run_reference_arm(args, rank):
+    """CPU arm: the reference path on the host cores over a bounded sample."""
+    if rank != 0:
+        return
+    res = reference_throughput(args)
+    line = {"metric": METRIC, "impl": "reference", "value": res["value"], "unit": UNIT,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": res["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8/u64", "data": "synthetic",
+            "config": res["config"], "cpu_baseline": res["cpu_baseline"],
+            "e2e": {"value": res["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--genome", type=float, default=1e9, help="genome length (bp)")
+    ap.add_argument("--k", type=int, default=31)
+    ap.add_argument("--l", type=int, default=8)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-sample", type=float, default=4e6, help="genome length of the CPU sample")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from unitigcoarsening_b200 import Compactor, synth
+    from unitigcoarsening_b200 import build as B
+    B.build()
+
+    t0 = time.time()
+    spec = synth.scale_plain(length=int(args.genome), seed=2 + rank)
+    with torch.no_grad():
+        text = synth.make_text(spec, args.k, device="cuda")
+    torch.cuda.synchronize()
+    gen_s = time.time() - t0
+    text_bytes = text.numel()
+    torch.cuda.empty_cache()
+
+    comp = Compactor(local)
+    out = torch.empty(comp.output_bound(text_bytes, args.k), dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    st = None
+    for _ in range(max(3, args.warmup)):
+        res, st = comp.compact(text, args.k, args.l, out=out, stats=True)
+    torch.cuda.synchronize()
+    n = int(st["n_kmers"])
+
+    # timed region: device-resident text (> L2, so no flush is needed)
+    phase = {"pack": 0.0, "bucket": 0.0, "tiles": 0.0, "stitch": 0.0}
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            res, st = comp.compact(text, args.k, args.l, out=out, stats=True)
+            for p in phase:
+                phase[p] += st["ms_" + p]
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    for p in phase:
+        phase[p] /= args.steps
+    value = world * n / (ms / 1e3)
+
+    # roofline of the dominant phase
+    peak, peak_kind = peaks()
+    alg = algorithmic_bytes(st, text_bytes, args.k)
+    dom = max(phase, key=lambda p: phase[p])
+    achieved = alg[dom] / (phase[dom] / 1e3) / 1e9
+    whole = sum(alg.values()) / (ms / 1e3) / 1e9
+
+    # e2e: host text -> host lines through the C ABI
+    e2e = None
+    if not args.no_e2e:
+        import psutil
+        need = 2 * text_bytes + (1 << 30)
+        if psutil.virtual_memory().available > need:
+            htext = torch.empty(text_bytes, dtype=torch.uint8, pin_memory=True)
+            htext.copy_(text)
+            hout = torch.empty(comp.output_bound(text_bytes, args.k), dtype=torch.uint8, pin_memory=True)
+            del text
+            torch.cuda.empty_cache()
+            comp.compact_host(htext, args.k, args.l, out=hout)
+            t1 = time.perf_counter()
+            for _ in range(args.e2e_steps):
+                r, est = comp.compact_host(htext, args.k, args.l, out=hout, stats=True)
+            e2e_s = (time.perf_counter() - t1) / args.e2e_steps
+            e2e = {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": text_bytes,
+                   "d2h_bytes_per_step": int(est["out_bytes"]), "ms_per_step": e2e_s * 1e3,
+                   "pinned": True}
+        else:
+            e2e = {"value": None, "unit": UNIT, "skipped": f"host RAM below {need >> 30} GiB"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(args)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8/u64 (2-bit packed keys, 32-bit ids)", "data": "synthetic",
+            "config": {"workload": f"plain single job: {args.genome / 1e9:g} Gbp genome, 41% GC, 5% repeat "
+                                   f"families, 0.1% SNPs, k={args.k}", "k": args.k, "l": args.l,
+                       "n_kmers": n, "text_bytes": text_bytes, "l2_flush": "inputs larger than L2",
+                       "parallelism": f"replicas x{world}", "genome_seed": 2},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                         "whole_path_achieved": whole, "whole_path_frac": whole / peak},
+            "phase_ms": phase, "algorithmic_bytes": alg,
+            "stats": {k2: (float(v) if isinstance(v, float) else int(v)) for k2, v in st.items()},
+            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "gpu_launches": int(st.get("launches", 0)) * args.steps if "launches" in st else None,
+            "gen_seconds": gen_s,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

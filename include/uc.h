@@ -1,0 +1,168 @@
+/*
+ * uc.h — C ABI of the B200 unitig compactor (libuc.so).
+ *
+ * The reference (euphoricpoptarts/UnitigCoarsening) has no library interface:
+ * its driver calls C++ functions that take Kokkos views.  Each entry point
+ * below replaces one of those calls with plain pointers and sizes; the
+ * comment names the reference function (file:line) it stands in for.
+ *
+ * Conventions
+ *  - Every call returns uc_status; uc_last_error(ctx) gives a one-line reason.
+ *  - "d_" pointers are device pointers on the context's device; every call is
+ *    enqueued on the context's stream (uc_ctx_set_stream to share a stream
+ *    with the caller) and returns after the work is enqueued unless it has to
+ *    read a size back, in which case it synchronizes that stream.
+ *  - Packed k-mers ("keys") use the reference's bit layout (driver.cpp:236-246:
+ *    char x at bits 2x, A=0 C=1 G=2 T=3, any other byte packs as A) stored in
+ *    64-bit words: one word per k-mer for k <= 31, two for 32 <= k <= 63.
+ *  - Vertex ids are input line numbers (0-based); UC_NONE marks "no vertex".
+ *  - A context is not thread safe; use one context per host thread.
+ */
+#ifndef UC_H
+#define UC_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UC_NONE 0xFFFFFFFFu
+
+typedef enum uc_status {
+    UC_OK = 0,
+    UC_EINPUT = 1,     /* malformed text, count mismatch, k or l out of range */
+    UC_ENOMEM = 2,     /* a device or host allocation failed */
+    UC_EBUDGET = 3,    /* the job does not fit the context's HBM budget */
+    UC_ETIMEOUT = 4,   /* a bounded device wait ran out */
+    UC_EINTERNAL = 5,  /* an internal bound or invariant failed */
+    UC_ECUDA = 6,      /* a CUDA runtime call failed */
+    UC_EBUSY = 7       /* job not finished (uc_job_result before completion) */
+} uc_status;
+
+/* Contraction strategies for uc_contract / the stitch step. */
+enum { UC_CONTRACT_POINTER_JUMP = 0, UC_CONTRACT_HEC = 1 };
+
+typedef struct uc_ctx uc_ctx;
+typedef struct uc_job uc_job;
+
+/* Per-run counters and phase times (milliseconds, CUDA events). */
+typedef struct uc_stats {
+    uint64_t n_kmers, n_copies, n_cross, n_tiles, n_big_tiles;
+    uint64_t n_segments, n_unitigs, n_cycles, out_bytes;
+    uint32_t l_used, bucket_bits, tile_capacity, stitch_rounds;
+    float ms_pack, ms_bucket, ms_tiles, ms_stitch, ms_total;
+} uc_stats;
+
+/* Tuning knobs (0 = automatic).  Filled by the autotuner or by hand. */
+typedef struct uc_tuning {
+    uint32_t tile_capacity;   /* copies per shared-memory tile (max 8192) */
+    uint32_t tile_threads;    /* threads per tile CTA (256, 512 or 1024) */
+    uint32_t bucket_bits;     /* log2 of the bucket count */
+    uint32_t load_factor_pct; /* tile hash slots per copy, percent (>=150) */
+    uint32_t contract_method; /* UC_CONTRACT_* for the segment stitch */
+} uc_tuning;
+
+/* ---- context --------------------------------------------------------- */
+
+/* Replaces Kokkos::initialize (driver.cpp:433).  hbm_budget 0 = 90% of free. */
+uc_status uc_ctx_create(int device, size_t hbm_budget, uc_ctx **out);
+uc_status uc_ctx_destroy(uc_ctx *ctx);
+uc_status uc_ctx_set_stream(uc_ctx *ctx, void *cuda_stream);
+uc_status uc_ctx_sync(uc_ctx *ctx);
+uc_status uc_ctx_set_tuning(uc_ctx *ctx, const uc_tuning *t);
+uc_status uc_ctx_get_tuning(const uc_ctx *ctx, uc_tuning *t);
+const char *uc_last_error(const uc_ctx *ctx);
+const char *uc_status_str(uc_status s);
+
+/* ---- phases (device memory) ------------------------------------------ */
+
+/* Header line of the k-mer text: the count n and the offset of the first
+ * k-mer line.  load_kmers header parse, driver.cpp:296-304. */
+uc_status uc_parse_header(uc_ctx *ctx, const char *d_text, size_t bytes,
+                          uint64_t *n, uint64_t *body_offset);
+
+/* Text -> packed keys (n * words).  load_kmers line parse + compact_kmers,
+ * driver.cpp:257-354 and 227-249.  Fails with UC_EINPUT on a line shorter
+ * than k or a count that disagrees with the number of lines. */
+uc_status uc_pack(uc_ctx *ctx, const char *d_text, size_t bytes, int k,
+                  uint64_t *d_keys, uint64_t *n_out);
+
+/* Prefix/suffix L-minimizer priorities per k-mer.  get_double_lmin,
+ * lmin_buckets.h:67-94, with the l-mer priority table of
+ * generate_permutation (driver.cpp:356-402) replaced by a seeded bijection of
+ * [0, 4^l); d_table (4^l entries) overrides it when not NULL. */
+uc_status uc_minimizers(uc_ctx *ctx, const uint64_t *d_keys, uint64_t n,
+                        int k, int l, uint64_t seed, const uint32_t *d_table,
+                        uint32_t *d_l1, uint32_t *d_l2);
+
+/* Bucketed edge finding: succ[u] = v iff v is u's only (k-1)-overlap
+ * successor and u is v's only predecessor; pred is the inverse.
+ * find_l_minimizer (lmin_buckets.h:288-433) + generate_hashmap
+ * (assembler.h:120-150) + assemble_pruned_graph (assembler.h:164-214). */
+uc_status uc_find_edges(uc_ctx *ctx, const uint64_t *d_keys, uint64_t n,
+                        int k, int l, uint64_t seed, uint32_t *d_succ,
+                        uint32_t *d_pred);
+
+/* Path contraction: head[v] = first vertex of v's unitig, rank[v] = its
+ * position (cycles start at their smallest key).  Replaces the round loop
+ * coarsen_de_bruijn_full_cycle (coarseners.h:437-485) with its HEC matching
+ * (heuristics.h:205-256) and member ordering (coarseners.h:182-235,
+ * compact_graph.h:55-112).  method: UC_CONTRACT_*. */
+uc_status uc_contract(uc_ctx *ctx, const uint64_t *d_keys,
+                      const uint32_t *d_succ, const uint32_t *d_pred,
+                      uint64_t n, int k, int method, uint32_t *d_head,
+                      uint32_t *d_rank, uint64_t *n_cycles);
+
+/* Unitig lines (first k-mer in full, then the last char of each later
+ * k-mer, '\n'), ordered by head id.  write_intra_bucket_outputs,
+ * compact.h:161-210.  d_out may be NULL to only size. */
+uc_status uc_emit(uc_ctx *ctx, const uint64_t *d_keys, const uint32_t *d_succ,
+                  const uint32_t *d_head, const uint32_t *d_rank, uint64_t n,
+                  int k, char *d_out, uint64_t cap, uint64_t *out_bytes);
+
+/* ---- fused path ------------------------------------------------------ */
+
+/* Whole path on device-resident text: pack, minimizer bucketing, per-tile
+ * edge finding + contraction + emission, cross-tile stitch.  The body of the
+ * reference's main (driver.cpp:433-659).  Line order is unspecified (the
+ * reference's is too); d_out needs at most bytes(text) bytes.  stats may be
+ * NULL. */
+uc_status uc_compact_device(uc_ctx *ctx, const char *d_text, size_t bytes,
+                            int k, int l, char *d_out, uint64_t cap,
+                            uint64_t *out_bytes, uc_stats *stats);
+
+/* Upper bound of the output size of uc_compact_device for this text. */
+uint64_t uc_output_bound(size_t text_bytes, int k);
+
+/* Synchronous host-memory form: host text in, lines into the caller's host
+ * buffer (pinned memory gives full PCIe bandwidth).  *out_bytes receives the
+ * length.  main, driver.cpp:422-662, without the file I/O. */
+uc_status uc_compact_host(uc_ctx *ctx, const char *text, size_t bytes, int k,
+                          int l, char *out, size_t cap, size_t *out_bytes,
+                          uc_stats *stats);
+
+/* ---- host-memory jobs ------------------------------------------------- */
+
+/* Submit host text (pageable or pinned); the job copies it to the device,
+ * runs the fused path and copies the lines back.  main, driver.cpp:422-662,
+ * without the file I/O. */
+uc_status uc_job_submit(uc_ctx *ctx, const char *text, size_t bytes, int k,
+                        int l, uc_job **job);
+uc_status uc_job_poll(uc_job *job, int *done);
+uc_status uc_job_wait(uc_job *job);
+/* Owned result buffer (free with uc_free) and its length. */
+uc_status uc_job_result(uc_job *job, char **buf, size_t *len,
+                        uc_stats *stats);
+uc_status uc_job_release(uc_job *job);
+void uc_free(void *p);
+
+/* File to file, appending to out_path like write_to_f (compact.h:7-37).
+ * The reference CLI `main <k-mer file> k l <output file>`. */
+uc_status uc_compact_file(uc_ctx *ctx, const char *in_path, int k, int l,
+                          const char *out_path, uc_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,32 @@
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    from oracle import oracle as O
+    O.build()
+    return O
+
+
+@pytest.fixture(scope="session")
+def comp():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from unitigcoarsening_b200 import build as B
+    B.build()
+    from unitigcoarsening_b200 import Compactor
+    c = Compactor(0)
+    yield c
+    c.close()

@@ -1,0 +1,172 @@
+"""GPU parity: every phase of the CUDA path through the C ABI against the CPU
+oracle on the same seeded inputs; bit-exact (keys, minimizers, edges, ranks,
+bytes, sorted lines)."""
+import numpy as np
+import pytest
+import torch
+
+from tests.cases import MICRO, cyclic_kmers, distinct_path, shuffled, sorted_lines, text_of, walk_kmers
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(b: bytes) -> torch.Tensor:
+    return torch.frombuffer(bytearray(b), dtype=torch.uint8).cuda()
+
+
+def fused_lines(comp, text: bytes, k: int, l: int):
+    out = comp.compact(dev(text), k, l)
+    torch.cuda.synchronize()
+    return sorted_lines(out.cpu().numpy().tobytes())
+
+
+@pytest.mark.parametrize("name,k,kmers,expected", MICRO, ids=[m[0] for m in MICRO])
+def test_micro_fused(comp, name, k, kmers, expected):
+    got = fused_lines(comp, text_of(kmers), k, min(8, k - 1))
+    assert got == sorted(x.encode() for x in expected)
+
+
+def _synth(kind: str):
+    from unitigcoarsening_b200 import synth
+    if kind == "small_plain":
+        return synth.make_text(synth.small_plain(), 31).numpy().tobytes(), 31
+    if kind == "wide_k63":
+        return synth.make_text(synth.wide_k(length=400_000, seed=11), 63).numpy().tobytes(), 63
+    if kind == "k15":
+        return synth.make_text(synth.GenomeSpec(length=60_000, gc=0.45, seed=5, snp_rate=0.002), 15).numpy().tobytes(), 15
+    if kind == "k47":
+        return synth.make_text(synth.GenomeSpec(length=200_000, gc=0.55, seed=6, snp_rate=0.001,
+                                                tandem_frac=0.02), 47).numpy().tobytes(), 47
+    if kind == "scale_sample":
+        return synth.make_text(synth.scale_plain(length=600_000, seed=12), 31).numpy().tobytes(), 31
+    if kind == "batched_job":
+        return synth.make_text(synth.batched_job(3, scale=0.1), 31).numpy().tobytes(), 31
+    raise KeyError(kind)
+
+
+CONFIGS = ["small_plain", "wide_k63", "k15", "k47", "scale_sample", "batched_job"]
+
+
+@pytest.fixture(scope="module")
+def texts():
+    return {c: _synth(c) for c in CONFIGS}
+
+
+@pytest.mark.parametrize("cfg", CONFIGS)
+def test_phases_bit_exact(comp, oracle, texts, cfg):
+    text, k = texts[cfg]
+    l = min(8, k - 1)
+    seed = 0x1234
+    words = oracle.parse(text, k)
+    keys = comp.load_kmers(dev(text), k)
+    from unitigcoarsening_b200 import as_u32, keys_to_words
+    assert np.array_equal(keys_to_words(keys, k), words)
+    l1, l2 = comp.find_l_minimizer(keys, k, l, seed)
+    o1, o2 = oracle.lmin(words, k, l, seed)
+    assert np.array_equal(as_u32(l1), o1) and np.array_equal(as_u32(l2), o2)
+    succ, pred = comp.assemble_pruned_graph(keys, k, l, seed)
+    osucc, opred = oracle.edges(words, k)
+    assert np.array_equal(as_u32(succ), osucc)
+    assert np.array_equal(as_u32(pred), opred)
+    head, rank, cyc = comp.coarsen_de_bruijn_full_cycle(keys, succ, pred, k)
+    ohead, orank, ocyc = oracle.contract(words, k, osucc, opred)
+    assert np.array_equal(as_u32(head), ohead) and np.array_equal(as_u32(rank), orank)
+    assert cyc == ocyc
+    lines = comp.write_unitigs(keys, succ, head, rank, k).cpu().numpy().tobytes()
+    assert lines == oracle.emit(words, k, osucc, ohead, orank)
+
+
+@pytest.mark.parametrize("cfg", CONFIGS)
+def test_fused_matches_oracle(comp, oracle, texts, cfg):
+    text, k = texts[cfg]
+    want, n, _ = oracle.compact(text, k)
+    got = fused_lines(comp, text, k, min(8, k - 1))
+    assert got == sorted_lines(want)
+
+
+@pytest.mark.parametrize("cap,bits", [(256, 0), (256, 4), (1024, 12), (2048, 8), (8192, 9)])
+def test_fused_independent_of_tiling(comp, oracle, texts, cap, bits):
+    text, k = texts["scale_sample"]
+    want, _, _ = oracle.compact(text, k)
+    comp.set_tuning(tile_capacity=cap, bucket_bits=bits)
+    try:
+        got = fused_lines(comp, text, k, 8)
+    finally:
+        comp.set_tuning(tile_capacity=0, bucket_bits=0)
+    assert got == sorted_lines(want)
+
+
+@pytest.mark.parametrize("l", [3, 8, 12, 16])
+def test_fused_independent_of_l(comp, oracle, texts, l):
+    text, k = texts["small_plain"]
+    want, _, _ = oracle.compact(text, k)
+    assert fused_lines(comp, text, k, l) == sorted_lines(want)
+
+
+@pytest.mark.parametrize("k", [31, 63])
+def test_cycles_across_tiles(comp, oracle, k):
+    km = cyclic_kmers(500, k, seed=k) + walk_kmers(distinct_path(300, k, seed=3 * k), k)
+    text = text_of(shuffled(km, 5))
+    want, _, ocyc = oracle.compact(text, k)
+    assert ocyc == 1
+    for cap, bits in [(0, 0), (256, 6)]:
+        comp.set_tuning(tile_capacity=cap, bucket_bits=bits)
+        try:
+            assert fused_lines(comp, text, k, 6) == sorted_lines(want)
+        finally:
+            comp.set_tuning(tile_capacity=0, bucket_bits=0)
+
+
+def test_cycle_inside_one_tile(comp, oracle):
+    km = cyclic_kmers(60, 21, seed=9)
+    text = text_of(shuffled(km, 2))
+    want, _, _ = oracle.compact(text, 21)
+    comp.set_tuning(bucket_bits=0)
+    try:
+        assert fused_lines(comp, text, 21, 6) == sorted_lines(want)
+    finally:
+        comp.set_tuning(bucket_bits=0)
+
+
+def test_general_line_layout(comp, oracle):
+    seq = distinct_path(400, 31, seed=1)
+    km = shuffled(walk_kmers(seq, 31), 3)
+    for text in [text_of(km, extra="\t12"), text_of(km, crlf=True), text_of(km) + b"\n\n"]:
+        assert fused_lines(comp, text, 31, 8) == [seq.encode()]
+    # non-ACGT bytes pack as A
+    t = text_of(["ACGTN" + "A" * 26])
+    assert fused_lines(comp, t, 31, 8) == [b"ACGTA" + b"A" * 26]
+
+
+def test_empty_and_tiny(comp):
+    out = comp.compact(dev(b"0\n"), 31, 8)
+    assert out.numel() == 0
+    assert fused_lines(comp, text_of(["ACGTACGTACGTACGTACGTACGTACGTACG"]), 31, 8) == [
+        b"ACGTACGTACGTACGTACGTACGTACGTACG"]
+
+
+def test_malformed_inputs_raise(comp):
+    from unitigcoarsening_b200 import UCError
+    with pytest.raises(UCError) as e:
+        comp.compact(dev(text_of(["ACG", "AC"])), 3, 2)
+    assert e.value.status == 1
+    with pytest.raises(UCError) as e:
+        comp.compact(dev(text_of(["ACG", "CGT"], header=3)), 3, 2)
+    assert e.value.status == 1
+    with pytest.raises(UCError):
+        comp.compact(dev(text_of(["ACG"])), 3, 3)  # l must be < k
+
+
+def test_host_path_and_file(comp, oracle, texts, tmp_path):
+    text, k = texts["small_plain"]
+    want, _, _ = oracle.compact(text, k)
+    got = comp.compact_host(text, k, 8)
+    assert sorted_lines(got.numpy().tobytes()) == sorted_lines(want)
+    inp = tmp_path / "in.txt"
+    outp = tmp_path / "out.txt"
+    inp.write_bytes(text)
+    comp.compact_file(str(inp), k, 8, str(outp))
+    comp.compact_file(str(inp), k, 8, str(outp))  # appends like the reference
+    data = outp.read_bytes()
+    assert len(data) == 2 * len(want)
+    assert sorted_lines(data) == sorted(sorted_lines(want) * 2)

@@ -1,0 +1,280 @@
+"""Python binding of libuc.so (the C ABI in include/uc.h).
+
+The functions keep the names of the reference's steps so a caller of the
+reference can find each one:
+
+=============================  ==========================================
+this module                    reference (euphoricpoptarts/UnitigCoarsening)
+=============================  ==========================================
+``Compactor.load_kmers``       ``load_kmers`` + ``compact_kmers``  (driver.cpp:257, 227)
+``Compactor.find_l_minimizer`` ``get_double_lmin`` (lmin_buckets.h:67)
+``Compactor.assemble_pruned_graph``  ``generate_hashmap`` + ``assemble_pruned_graph``
+                               (assembler.h:120, 164), bucketed as ``find_l_minimizer``
+``Compactor.coarsen_de_bruijn_full_cycle``  ``coarsen_de_bruijn_full_cycle``
+                               (coarseners.h:437) -> (head, rank) per k-mer
+``Compactor.write_unitigs``    ``write_intra_bucket_outputs`` (compact.h:161)
+``Compactor.compact``          ``main`` pipeline on device-resident text (driver.cpp:422)
+``Compactor.compact_host``     the same from host memory to host memory
+``Compactor.compact_file``     the CLI ``main <k-mer file> k l <output file>``
+=============================  ==========================================
+
+Device buffers are torch CUDA tensors; the library runs on torch's current
+stream.  There is no CPU fallback: without the CUDA library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libuc.so")
+NONE = 0xFFFFFFFF
+
+CONTRACT_POINTER_JUMP = 0
+CONTRACT_HEC = 1
+
+STATUS = {0: "ok", 1: "invalid input", 2: "out of memory", 3: "HBM budget exceeded",
+          4: "device wait timed out", 5: "internal error", 6: "CUDA error", 7: "job not finished"}
+
+
+class UCError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in (
+        "n_kmers", "n_copies", "n_cross", "n_tiles", "n_big_tiles",
+        "n_segments", "n_unitigs", "n_cycles", "out_bytes")] + \
+        [(n, ctypes.c_uint32) for n in ("l_used", "bucket_bits", "tile_capacity", "stitch_rounds")] + \
+        [(n, ctypes.c_float) for n in ("ms_pack", "ms_bucket", "ms_tiles", "ms_stitch", "ms_total")]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+class Tuning(ctypes.Structure):
+    _fields_ = [("tile_capacity", ctypes.c_uint32), ("tile_threads", ctypes.c_uint32),
+                ("bucket_bits", ctypes.c_uint32), ("load_factor_pct", ctypes.c_uint32),
+                ("contract_method", ctypes.c_uint32)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libuc.so; raises if it was not built (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with unitigcoarsening_b200.build.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        vp, sz, i, u64, u32 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32
+        pu64 = ctypes.POINTER(ctypes.c_uint64)
+        sig = {
+            "uc_ctx_create": ([i, sz, ctypes.POINTER(vp)], i),
+            "uc_ctx_destroy": ([vp], i),
+            "uc_ctx_set_stream": ([vp, vp], i),
+            "uc_ctx_sync": ([vp], i),
+            "uc_ctx_set_tuning": ([vp, ctypes.POINTER(Tuning)], i),
+            "uc_ctx_get_tuning": ([vp, ctypes.POINTER(Tuning)], i),
+            "uc_last_error": ([vp], ctypes.c_char_p),
+            "uc_status_str": ([i], ctypes.c_char_p),
+            "uc_parse_header": ([vp, vp, sz, pu64, pu64], i),
+            "uc_pack": ([vp, vp, sz, i, vp, pu64], i),
+            "uc_minimizers": ([vp, vp, u64, i, i, u64, vp, vp, vp], i),
+            "uc_find_edges": ([vp, vp, u64, i, i, u64, vp, vp], i),
+            "uc_contract": ([vp, vp, vp, vp, u64, i, i, vp, vp, pu64], i),
+            "uc_emit": ([vp, vp, vp, vp, vp, u64, i, vp, u64, pu64], i),
+            "uc_compact_device": ([vp, vp, sz, i, i, vp, u64, pu64, ctypes.POINTER(Stats)], i),
+            "uc_output_bound": ([sz, i], u64),
+            "uc_compact_host": ([vp, vp, sz, i, i, vp, sz, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(Stats)], i),
+            "uc_job_submit": ([vp, vp, sz, i, i, ctypes.POINTER(vp)], i),
+            "uc_job_poll": ([vp, ctypes.POINTER(ctypes.c_int)], i),
+            "uc_job_wait": ([vp], i),
+            "uc_job_result": ([vp, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(Stats)], i),
+            "uc_job_release": ([vp], i),
+            "uc_free": ([vp], None),
+            "uc_compact_file": ([vp, ctypes.c_char_p, i, i, ctypes.c_char_p, ctypes.POINTER(Stats)], i),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def key_words(k: int) -> int:
+    """64-bit words per packed k-mer."""
+    return 1 if k <= 31 else 2
+
+
+def _ptr(t: torch.Tensor | None):
+    return None if t is None else ctypes.c_void_p(t.data_ptr())
+
+
+class Compactor:
+    """One library context bound to one GPU (uc_ctx)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the unitig compactor needs a CUDA device")
+        self.device = device
+        self._L = lib()
+        h = ctypes.c_void_p()
+        st = self._L.uc_ctx_create(device, hbm_budget, ctypes.byref(h))
+        if st:
+            raise UCError(st, "uc_ctx_create failed")
+        self._h = h
+
+    # -- plumbing
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.uc_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _bind_stream(self):
+        with torch.cuda.device(self.device):
+            s = torch.cuda.current_stream().cuda_stream
+        self._L.uc_ctx_set_stream(self._h, ctypes.c_void_p(s))
+
+    def _check(self, st: int):
+        if st:
+            raise UCError(st, self._L.uc_last_error(self._h).decode())
+
+    def set_tuning(self, **kw):
+        t = Tuning()
+        self._check(self._L.uc_ctx_get_tuning(self._h, ctypes.byref(t)))
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._check(self._L.uc_ctx_set_tuning(self._h, ctypes.byref(t)))
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        self._check(self._L.uc_ctx_get_tuning(self._h, ctypes.byref(t)))
+        return {n: getattr(t, n) for n, _ in Tuning._fields_}
+
+    def _dev(self):
+        return torch.device("cuda", self.device)
+
+    # -- phases
+    def load_kmers(self, text: torch.Tensor, k: int) -> torch.Tensor:
+        """Text (uint8 CUDA tensor) -> packed keys, shape (n, words)."""
+        self._bind_stream()
+        n = ctypes.c_uint64()
+        bn = ctypes.c_uint64()
+        self._check(self._L.uc_parse_header(self._h, _ptr(text), text.numel(), ctypes.byref(n), ctypes.byref(bn)))
+        keys = torch.empty((max(n.value, 1), key_words(k)), dtype=torch.int64, device=self._dev())
+        self._check(self._L.uc_pack(self._h, _ptr(text), text.numel(), k, _ptr(keys), ctypes.byref(n)))
+        return keys[: n.value]
+
+    def find_l_minimizer(self, keys: torch.Tensor, k: int, l: int, seed: int = 0,
+                         table: torch.Tensor | None = None):
+        self._bind_stream()
+        n = keys.shape[0]
+        l1 = torch.empty(max(n, 1), dtype=torch.int32, device=self._dev())
+        l2 = torch.empty_like(l1)
+        self._check(self._L.uc_minimizers(self._h, _ptr(keys), n, k, l, seed, _ptr(table), _ptr(l1), _ptr(l2)))
+        return l1[:n], l2[:n]
+
+    def assemble_pruned_graph(self, keys: torch.Tensor, k: int, l: int, seed: int = 0):
+        """Kept-edge graph by id: (succ, pred) int32 (UC_NONE = -1)."""
+        self._bind_stream()
+        n = keys.shape[0]
+        succ = torch.empty(max(n, 1), dtype=torch.int32, device=self._dev())
+        pred = torch.empty_like(succ)
+        self._check(self._L.uc_find_edges(self._h, _ptr(keys), n, k, l, seed, _ptr(succ), _ptr(pred)))
+        return succ[:n], pred[:n]
+
+    def coarsen_de_bruijn_full_cycle(self, keys, succ, pred, k: int, method: int = CONTRACT_POINTER_JUMP):
+        """(head, rank, n_cycles) per k-mer."""
+        self._bind_stream()
+        n = keys.shape[0]
+        head = torch.empty(max(n, 1), dtype=torch.int32, device=self._dev())
+        rank = torch.empty_like(head)
+        cyc = ctypes.c_uint64()
+        self._check(self._L.uc_contract(self._h, _ptr(keys), _ptr(succ), _ptr(pred), n, k, method,
+                                        _ptr(head), _ptr(rank), ctypes.byref(cyc)))
+        return head[:n], rank[:n], cyc.value
+
+    def write_unitigs(self, keys, succ, head, rank, k: int) -> torch.Tensor:
+        """Unitig lines ordered by head id, as a uint8 CUDA tensor."""
+        self._bind_stream()
+        n = keys.shape[0]
+        nb = ctypes.c_uint64()
+        self._check(self._L.uc_emit(self._h, _ptr(keys), _ptr(succ), _ptr(head), _ptr(rank), n, k,
+                                    None, 0, ctypes.byref(nb)))
+        out = torch.empty(max(nb.value, 1), dtype=torch.uint8, device=self._dev())
+        self._check(self._L.uc_emit(self._h, _ptr(keys), _ptr(succ), _ptr(head), _ptr(rank), n, k,
+                                    _ptr(out), out.numel(), ctypes.byref(nb)))
+        return out[: nb.value]
+
+    # -- whole path
+    def output_bound(self, text_bytes: int, k: int) -> int:
+        return int(self._L.uc_output_bound(text_bytes, k))
+
+    def compact(self, text: torch.Tensor, k: int, l: int, out: torch.Tensor | None = None,
+                stats: bool = False):
+        """Device-resident text -> unitig lines (uint8 CUDA tensor)."""
+        self._bind_stream()
+        cap = self.output_bound(text.numel(), k)
+        if out is None or out.numel() < cap:
+            out = torch.empty(cap, dtype=torch.uint8, device=self._dev())
+        nb = ctypes.c_uint64()
+        st = Stats()
+        self._check(self._L.uc_compact_device(self._h, _ptr(text), text.numel(), k, l, _ptr(out), out.numel(),
+                                              ctypes.byref(nb), ctypes.byref(st)))
+        res = out[: nb.value]
+        return (res, st.as_dict()) if stats else res
+
+    def compact_host(self, text, k: int, l: int, out=None, stats: bool = False):
+        """Host text (bytes, numpy uint8 or CPU tensor, pinned or not) ->
+        host lines.  With ``out`` (a CPU uint8 tensor) the lines land there."""
+        if isinstance(text, (bytes, bytearray)):
+            src = np.frombuffer(text, dtype=np.uint8)
+            tp, tn = src.ctypes.data_as(ctypes.c_void_p), src.nbytes
+        elif isinstance(text, np.ndarray):
+            tp, tn = text.ctypes.data_as(ctypes.c_void_p), text.nbytes
+        else:
+            tp, tn = ctypes.c_void_p(text.data_ptr()), text.numel()
+        cap = self.output_bound(tn, k)
+        if out is None:
+            out = torch.empty(cap, dtype=torch.uint8)
+        ob = ctypes.c_size_t()
+        st = Stats()
+        self._check(self._L.uc_compact_host(self._h, tp, tn, k, l, ctypes.c_void_p(out.data_ptr()), out.numel(),
+                                            ctypes.byref(ob), ctypes.byref(st)))
+        res = out[: ob.value]
+        return (res, st.as_dict()) if stats else res
+
+    def compact_file(self, in_path: str, k: int, l: int, out_path: str) -> dict:
+        st = Stats()
+        self._check(self._L.uc_compact_file(self._h, in_path.encode(), k, l, out_path.encode(), ctypes.byref(st)))
+        return st.as_dict()
+
+
+def keys_to_words(keys: torch.Tensor, k: int) -> np.ndarray:
+    """Packed keys -> the reference's uint32 word layout (n, ceil(k/16))."""
+    a = keys.detach().cpu().contiguous().numpy().view(np.uint32).reshape(keys.shape[0], -1)
+    return np.ascontiguousarray(a[:, : (k + 15) // 16])
+
+
+def as_u32(t: torch.Tensor) -> np.ndarray:
+    return t.detach().cpu().numpy().view(np.uint32)

@@ -1,0 +1,388 @@
+// uc_capi.cu — the extern "C" boundary of libuc.so (declared in include/uc.h).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+
+#include "../../include/uc.h"
+#include "uc_pipeline.h"
+
+struct uc_ctx {
+  uc::Env env;
+  // host-path device buffers (grow only)
+  char* io_text = nullptr;
+  size_t io_text_cap = 0;
+  char* io_out = nullptr;
+  size_t io_out_cap = 0;
+};
+
+struct uc_job {
+  uc_ctx* ctx = nullptr;
+  uc_status status = UC_OK;
+  char* result = nullptr;
+  size_t len = 0;
+  uc_stats stats{};
+  int done = 0;
+};
+
+namespace {
+
+uc_status as_status(int r) { return static_cast<uc_status>(r); }
+
+uc_status cuda_fail(uc_ctx* c, cudaError_t e, const char* what) {
+  cudaGetLastError();
+  c->env.err = std::string(what) + ": " + cudaGetErrorString(e);
+  return UC_ECUDA;
+}
+
+
+uc_status set_device(uc_ctx* c) {
+  const cudaError_t e = cudaSetDevice(c->env.device);
+  return e == cudaSuccess ? UC_OK : cuda_fail(c, e, "cudaSetDevice");
+}
+
+uc_status grow(uc_ctx* c, char** buf, size_t* cap, size_t want) {
+  if (*cap >= want) return UC_OK;
+  if (*buf) cudaFree(*buf);
+  *buf = nullptr;
+  *cap = 0;
+  const size_t sz = want + (want >> 4) + 4096;
+  const cudaError_t e = cudaMalloc(buf, sz);
+  if (e != cudaSuccess) {
+    *buf = nullptr;
+    return cuda_fail(c, e, "cudaMalloc (job buffers)");
+  }
+  *cap = sz;
+  return UC_OK;
+}
+
+// Host text in, host lines out (synchronous).
+uc_status run_host(uc_ctx* c, const char* text, size_t bytes, int k, int l, char** out_owned,
+                   char* out_user, size_t out_cap, size_t* out_len, uc_stats* st) {
+  uc_status s = set_device(c);
+  if (s) return s;
+  s = grow(c, &c->io_text, &c->io_text_cap, bytes + 64);
+  if (s) return s;
+  const uint64_t bound = uc::output_bound(bytes, k);
+  s = grow(c, &c->io_out, &c->io_out_cap, bound);
+  if (s) return s;
+  cudaError_t e = cudaMemcpyAsync(c->io_text, text, bytes, cudaMemcpyHostToDevice, c->env.stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemcpyAsync H2D");
+  uint64_t ob = 0;
+  const int r = uc::compact_device(c->env, c->io_text, bytes, k, l, c->io_out, bound, ob, st);
+  if (r) return as_status(r);
+  char* dst = out_user;
+  if (!dst) {
+    dst = static_cast<char*>(std::malloc(ob ? ob : 1));
+    if (!dst) {
+      c->env.err = "host malloc of the result failed";
+      return UC_ENOMEM;
+    }
+  } else if (ob > out_cap) {
+    c->env.err = "result buffer too small";
+    return UC_EINPUT;
+  }
+  if (ob) {
+    e = cudaMemcpyAsync(dst, c->io_out, ob, cudaMemcpyDeviceToHost, c->env.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->env.stream);
+    if (e != cudaSuccess) {
+      if (!out_user) std::free(dst);
+      return cuda_fail(c, e, "cudaMemcpyAsync D2H");
+    }
+  }
+  if (out_owned) *out_owned = dst;
+  *out_len = ob;
+  return UC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* uc_status_str(uc_status s) {
+  switch (s) {
+    case UC_OK: return "ok";
+    case UC_EINPUT: return "invalid input";
+    case UC_ENOMEM: return "out of memory";
+    case UC_EBUDGET: return "HBM budget exceeded";
+    case UC_ETIMEOUT: return "device wait timed out";
+    case UC_EINTERNAL: return "internal error";
+    case UC_ECUDA: return "CUDA error";
+    case UC_EBUSY: return "job not finished";
+  }
+  return "unknown status";
+}
+
+uc_status uc_ctx_create(int device, size_t hbm_budget, uc_ctx** out) {
+  if (!out) return UC_EINPUT;
+  *out = nullptr;
+  uc_ctx* c = new (std::nothrow) uc_ctx();
+  if (!c) return UC_ENOMEM;
+  c->env.device = device;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) {
+    delete c;
+    cudaGetLastError();
+    return UC_ECUDA;
+  }
+  cudaDeviceProp prop{};
+  cudaGetDeviceProperties(&prop, device);
+  c->env.sm_count = prop.multiProcessorCount;
+  c->env.smem_optin = int(prop.sharedMemPerBlockOptin);
+  size_t fr = 0, tot = 0;
+  cudaMemGetInfo(&fr, &tot);
+  c->env.budget = hbm_budget ? hbm_budget : size_t(double(fr) * 0.9);
+  e = cudaStreamCreateWithFlags(&c->env.stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&c->env.ctr, sizeof(uc::Counters));
+  if (e == cudaSuccess) e = cudaMallocHost(&c->env.h_ctr, sizeof(uc::Counters));
+  for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->env.ev[i]);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    uc_ctx_destroy(c);
+    return UC_ECUDA;
+  }
+  c->env.own_stream = true;
+  *out = c;
+  return UC_OK;
+}
+
+uc_status uc_ctx_destroy(uc_ctx* c) {
+  if (!c) return UC_OK;
+  cudaSetDevice(c->env.device);
+  if (c->env.stream) cudaStreamSynchronize(c->env.stream);
+  if (c->env.arena) cudaFree(c->env.arena);
+  if (c->env.big_buf) cudaFree(c->env.big_buf);
+  if (c->io_text) cudaFree(c->io_text);
+  if (c->io_out) cudaFree(c->io_out);
+  if (c->env.ctr) cudaFree(c->env.ctr);
+  if (c->env.h_ctr) cudaFreeHost(c->env.h_ctr);
+  for (int i = 0; i < 8; ++i)
+    if (c->env.ev[i]) cudaEventDestroy(c->env.ev[i]);
+  if (c->env.own_stream && c->env.stream) cudaStreamDestroy(c->env.stream);
+  delete c;
+  return UC_OK;
+}
+
+uc_status uc_ctx_set_stream(uc_ctx* c, void* stream) {
+  if (!c) return UC_EINPUT;
+  if (c->env.own_stream && c->env.stream) {
+    cudaStreamSynchronize(c->env.stream);
+    cudaStreamDestroy(c->env.stream);
+  }
+  c->env.stream = static_cast<cudaStream_t>(stream);
+  c->env.own_stream = false;
+  return UC_OK;
+}
+
+uc_status uc_ctx_sync(uc_ctx* c) {
+  if (!c) return UC_EINPUT;
+  const cudaError_t e = cudaStreamSynchronize(c->env.stream);
+  return e == cudaSuccess ? UC_OK : cuda_fail(c, e, "cudaStreamSynchronize");
+}
+
+uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
+  if (!c || !t) return UC_EINPUT;
+  if (t->tile_capacity && (t->tile_capacity < 256 || t->tile_capacity > 8192)) {
+    c->env.err = "tile_capacity must be in [256, 8192]";
+    return UC_EINPUT;
+  }
+  if (t->tile_threads && t->tile_threads != 256 && t->tile_threads != 512 && t->tile_threads != 1024) {
+    c->env.err = "tile_threads must be 256, 512 or 1024";
+    return UC_EINPUT;
+  }
+  if (t->bucket_bits > 24) {
+    c->env.err = "bucket_bits must be <= 24";
+    return UC_EINPUT;
+  }
+  c->env.tune = *t;
+  return UC_OK;
+}
+
+uc_status uc_ctx_get_tuning(const uc_ctx* c, uc_tuning* t) {
+  if (!c || !t) return UC_EINPUT;
+  *t = c->env.tune;
+  return UC_OK;
+}
+
+const char* uc_last_error(const uc_ctx* c) { return c ? c->env.err.c_str() : "no context"; }
+
+uc_status uc_parse_header(uc_ctx* c, const char* d_text, size_t bytes, uint64_t* n, uint64_t* body) {
+  if (!c || !d_text || !n || !body) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  return as_status(uc::parse_header(c->env, d_text, bytes, *n, *body));
+}
+
+uc_status uc_pack(uc_ctx* c, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t* n_out) {
+  if (!c || !d_text || !n_out) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  c->env.used = 0;
+  uint64_t n = 0;
+  int r = uc::pack(c->env, d_text, bytes, k, d_keys, n);
+  c->env.used = 0;
+  *n_out = n;
+  return as_status(r);
+}
+
+uc_status uc_minimizers(uc_ctx* c, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed,
+                        const uint32_t* d_table, uint32_t* d_l1, uint32_t* d_l2) {
+  if (!c || (n && (!d_keys || !d_l1 || !d_l2))) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  return as_status(uc::minimizers(c->env, d_keys, n, k, l, seed, d_table, d_l1, d_l2));
+}
+
+uc_status uc_find_edges(uc_ctx* c, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed,
+                        uint32_t* d_succ, uint32_t* d_pred) {
+  if (!c || (n && (!d_keys || !d_succ || !d_pred))) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  c->env.used = 0;
+  const int r = uc::find_edges(c->env, d_keys, n, k, l, seed, d_succ, d_pred);
+  c->env.used = 0;
+  return as_status(r);
+}
+
+uc_status uc_contract(uc_ctx* c, const uint64_t* d_keys, const uint32_t* d_succ, const uint32_t* d_pred,
+                      uint64_t n, int k, int method, uint32_t* d_head, uint32_t* d_rank, uint64_t* n_cycles) {
+  if (!c || (n && (!d_keys || !d_succ || !d_pred || !d_head || !d_rank))) return UC_EINPUT;
+  if (method != UC_CONTRACT_POINTER_JUMP && method != UC_CONTRACT_HEC) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  c->env.used = 0;
+  uint64_t cyc = 0;
+  const int r = uc::contract(c->env, d_keys, d_succ, d_pred, n, k, method, d_head, d_rank, cyc);
+  c->env.used = 0;
+  if (n_cycles) *n_cycles = cyc;
+  return as_status(r);
+}
+
+uc_status uc_emit(uc_ctx* c, const uint64_t* d_keys, const uint32_t* d_succ, const uint32_t* d_head,
+                  const uint32_t* d_rank, uint64_t n, int k, char* d_out, uint64_t cap, uint64_t* out_bytes) {
+  if (!c || !out_bytes || (n && (!d_keys || !d_head || !d_rank))) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  c->env.used = 0;
+  uint64_t ob = 0;
+  const int r = uc::emit(c->env, d_keys, d_succ, d_head, d_rank, n, k, d_out, cap, ob);
+  c->env.used = 0;
+  *out_bytes = ob;
+  return as_status(r);
+}
+
+uint64_t uc_output_bound(size_t text_bytes, int k) { return uc::output_bound(text_bytes, k); }
+
+uc_status uc_compact_device(uc_ctx* c, const char* d_text, size_t bytes, int k, int l, char* d_out, uint64_t cap,
+                            uint64_t* out_bytes, uc_stats* stats) {
+  if (!c || !d_text || !d_out || !out_bytes) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  uint64_t ob = 0;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  const int r = uc::compact_device(c->env, d_text, bytes, k, l, d_out, cap, ob, stats);
+  c->env.used = 0;
+  *out_bytes = ob;
+  return as_status(r);
+}
+
+uc_status uc_compact_host(uc_ctx* c, const char* text, size_t bytes, int k, int l, char* out, size_t cap,
+                          size_t* out_bytes, uc_stats* stats) {
+  if (!c || !text || !out || !out_bytes) return UC_EINPUT;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  return run_host(c, text, bytes, k, l, nullptr, out, cap, out_bytes, stats);
+}
+
+uc_status uc_job_submit(uc_ctx* c, const char* text, size_t bytes, int k, int l, uc_job** job) {
+  if (!c || !text || !job) return UC_EINPUT;
+  uc_job* j = new (std::nothrow) uc_job();
+  if (!j) return UC_ENOMEM;
+  j->ctx = c;
+  j->status = run_host(c, text, bytes, k, l, &j->result, nullptr, 0, &j->len, &j->stats);
+  j->done = 1;
+  *job = j;
+  return j->status;
+}
+
+uc_status uc_job_poll(uc_job* j, int* done) {
+  if (!j || !done) return UC_EINPUT;
+  *done = j->done;
+  return UC_OK;
+}
+
+uc_status uc_job_wait(uc_job* j) { return j ? j->status : UC_EINPUT; }
+
+uc_status uc_job_result(uc_job* j, char** buf, size_t* len, uc_stats* stats) {
+  if (!j || !buf || !len) return UC_EINPUT;
+  if (!j->done) return UC_EBUSY;
+  if (j->status) return j->status;
+  *buf = j->result;
+  *len = j->len;
+  j->result = nullptr;
+  if (stats) *stats = j->stats;
+  return UC_OK;
+}
+
+uc_status uc_job_release(uc_job* j) {
+  if (!j) return UC_OK;
+  std::free(j->result);
+  delete j;
+  return UC_OK;
+}
+
+void uc_free(void* p) { std::free(p); }
+
+uc_status uc_compact_file(uc_ctx* c, const char* in_path, int k, int l, const char* out_path, uc_stats* stats) {
+  if (!c || !in_path || !out_path) return UC_EINPUT;
+  FILE* f = std::fopen(in_path, "rb");
+  if (!f) {
+    c->env.err = std::string("could not open input file ") + in_path;
+    return UC_EINPUT;
+  }
+  std::fseek(f, 0, SEEK_END);
+  const long sz = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  char* text = nullptr;
+  if (cudaMallocHost(&text, size_t(sz > 0 ? sz : 1)) != cudaSuccess) {
+    cudaGetLastError();
+    std::fclose(f);
+    c->env.err = "pinned host buffer for the input";
+    return UC_ENOMEM;
+  }
+  const size_t got = sz > 0 ? std::fread(text, 1, size_t(sz), f) : 0;
+  std::fclose(f);
+  if (got != size_t(sz > 0 ? sz : 0)) {
+    cudaFreeHost(text);
+    c->env.err = "short read of the input file";
+    return UC_EINPUT;
+  }
+  char* out = nullptr;
+  const size_t cap = size_t(uc::output_bound(got, k));
+  if (cudaMallocHost(&out, cap) != cudaSuccess) {
+    cudaGetLastError();
+    cudaFreeHost(text);
+    c->env.err = "pinned host buffer for the output";
+    return UC_ENOMEM;
+  }
+  size_t ob = 0;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  uc_status s = run_host(c, text, got, k, l, nullptr, out, cap, &ob, stats);
+  cudaFreeHost(text);
+  if (s == UC_OK) {
+    FILE* o = std::fopen(out_path, "ab");  // append, as write_to_f does
+    if (!o) {
+      c->env.err = std::string("could not open output file ") + out_path;
+      s = UC_EINPUT;
+    } else {
+      if (ob && std::fwrite(out, 1, ob, o) != ob) {
+        c->env.err = "short write of the output file";
+        s = UC_EINPUT;
+      }
+      std::fclose(o);
+    }
+  }
+  cudaFreeHost(out);
+  return s;
+}
+
+}  // extern "C"

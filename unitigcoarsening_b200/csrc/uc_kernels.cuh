@@ -1,0 +1,65 @@
+// uc_kernels.cuh — kernel declarations and launch helpers shared by the
+// pipeline (uc_pipeline.cu) and the C ABI (uc_capi.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "uc_common.cuh"
+
+namespace uc {
+
+// Device-side counters of one pipeline run (one allocation, zeroed per run).
+struct Counters {
+  unsigned long long out_cursor;     // bytes of finished lines written
+  unsigned long long seg_char_cursor;
+  unsigned long long n_copies;
+  unsigned long long cycles;
+  uint32_t seg_count;
+  uint32_t cross_count;
+  uint32_t ntiles;
+  uint32_t tile_next;
+  uint32_t nbig;
+  uint32_t active;                   // stitch: active list length
+  uint32_t active_next;
+  uint32_t err;
+  uint32_t pad[4];
+};
+
+struct TileParams {
+  const uint64_t* pkeys;        // copies (NW words each, role bits in the last word)
+  const uint32_t* plink;        // cross index (fused) or k-mer id (edges)
+  const unsigned long long* tile_begin;  // [ntiles + 1] copy offsets
+  Counters* ctr;
+  const uint32_t* big_list;     // big-tile launch: tile ids
+  char* big_scratch;
+  const unsigned long long* big_off;
+  int k;
+  uint32_t cap;                 // shared-memory tile capacity (copies)
+  uint32_t tslots;              // shared-memory hash slots (power of two >= 2*cap)
+  int mode;                     // 0 = edges by id, 1 = fused emission
+  uint32_t* succ;
+  uint32_t* pred;
+  char* out;
+  unsigned long long out_cap;
+  char* segchars;
+  unsigned long long segchars_cap;
+  uint32_t seg_cap;
+  unsigned long long* seg_off;
+  uint32_t* seg_len;
+  uint32_t* seg_sx;
+  uint32_t* seg_ex;
+  uint32_t* start_seg;
+  uint32_t* end_seg;
+};
+
+__host__ __device__ inline size_t tile_bytes(int nw, uint32_t cap, uint32_t tslots) {
+  return size_t(cap) * (8u * nw + 4u + 16u) + size_t(tslots) * 4u;
+}
+
+__host__ __device__ inline uint32_t pow2_at_least(uint64_t x) {
+  uint32_t p = 1;
+  while (p < x) p <<= 1;
+  return p;
+}
+
+}  // namespace uc

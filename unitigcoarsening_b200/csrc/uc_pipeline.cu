@@ -1,0 +1,1542 @@
+// uc_pipeline.cu — CUDA kernels of the unitig compactor and the host code
+// that sequences them.
+//
+// Data flow of the fused path (all device resident):
+//   text --k_pack--> keys[n] --k_lmin_count--> (b1,b2)[n] + bucket counts
+//   --scan/plan--> tiles of whole buckets --k_scatter--> copies in bucket order
+//   --k_tile (persistent, one tile per CTA in shared memory)--> finished lines
+//   + open segments --stitch (list ranking over segments)--> cross lines.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/uc.h"
+#include "uc_kernels.cuh"
+#include "uc_pipeline.h"
+
+namespace uc {
+
+// ===================================================================== scan
+
+template <typename Tin, typename Tout>
+__global__ void k_scan_reduce(const Tin* __restrict__ in, uint64_t n, Tout* __restrict__ bsum,
+                              uint32_t per_block) {
+  __shared__ Tout sh[33];
+  const uint64_t b0 = uint64_t(blockIdx.x) * per_block;
+  Tout acc = 0;
+  for (uint64_t i = b0 + threadIdx.x; i < min(n, b0 + per_block); i += blockDim.x) acc += Tout(in[i]);
+  Tout total;
+  block_excl_scan(acc, sh, &total);
+  if (threadIdx.x == 0) bsum[blockIdx.x] = total;
+}
+
+// Exclusive scan of one block's slice, offset by the scanned block sums.
+template <typename Tin, typename Tout>
+__global__ void k_scan_down(const Tin* __restrict__ in, uint64_t n, Tout* __restrict__ out,
+                            const Tout* __restrict__ boff, uint32_t per_block, Tout* total_out) {
+  __shared__ Tout sh[33];
+  const uint64_t b0 = uint64_t(blockIdx.x) * per_block;
+  const uint64_t b1 = min(n, b0 + per_block);
+  const uint32_t per_thread = (per_block + blockDim.x - 1) / blockDim.x;
+  const uint64_t lo = b0 + uint64_t(threadIdx.x) * per_thread;
+  const uint64_t hi = min(b1, lo + per_thread);
+  Tout acc = 0;
+  for (uint64_t i = lo; i < hi; ++i) acc += Tout(in[i]);
+  Tout total;
+  Tout pre = block_excl_scan(acc, sh, &total) + boff[blockIdx.x];
+  for (uint64_t i = lo; i < hi; ++i) {
+    const Tout v = Tout(in[i]);
+    out[i] = pre;
+    pre += v;
+  }
+  if (total_out && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
+    *total_out = boff[blockIdx.x] + total;
+    out[n] = boff[blockIdx.x] + total;
+  }
+}
+
+// Exclusive scan in[0..n) -> out[0..n], out[n] = total.  tmp needs
+// scan_tmp_elems(n) elements of Tout.
+template <typename Tin, typename Tout>
+static void scan_excl(const Tin* in, uint64_t n, Tout* out, Tout* tmp, cudaStream_t s,
+                      Tout* total_out = nullptr) {
+  const uint32_t per_block = 1024 * 8;
+  const uint64_t nb = std::max<uint64_t>(1, (n + per_block - 1) / per_block);
+  Tout* bsum = tmp;
+  Tout* boff = tmp + nb;
+  Tout* rest = tmp + 2 * nb + 1;
+  k_scan_reduce<Tin, Tout><<<unsigned(nb), 1024, 0, s>>>(in, n, bsum, per_block);
+  if (nb == 1) {
+    cudaMemsetAsync(boff, 0, sizeof(Tout), s);
+  } else {
+    scan_excl<Tout, Tout>(bsum, nb, boff, rest, s);
+  }
+  k_scan_down<Tin, Tout><<<unsigned(nb), 1024, 0, s>>>(in, n, out, boff, per_block, total_out);
+}
+
+static uint64_t scan_tmp_elems(uint64_t n) {
+  uint64_t t = 0;
+  const uint64_t per_block = 1024 * 8;
+  for (;;) {
+    const uint64_t nb = std::max<uint64_t>(1, (n + per_block - 1) / per_block);
+    t += 2 * nb + 1;
+    if (nb == 1) break;
+    n = nb;
+  }
+  return t + 8;
+}
+
+// ===================================================================== pack
+
+__device__ __forceinline__ uint32_t base_code(uint32_t c) {
+  // char_map of compact_kmers (driver.cpp:228-232): A=0 C=1 G=2 T=3, else 0
+  return (c == 'C') ? 1u : (c == 'G') ? 2u : (c == 'T') ? 3u : 0u;
+}
+
+// One warp packs 32 consecutive lines; lane j handles chars j and j+32 of a
+// line, so each line is one coalesced 32-byte read, and the 2-bit codes are
+// gathered with warp OR-reductions.  Lane i keeps line i's key.
+template <int NW>
+__global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, uint64_t body,
+                                              uint64_t end, const unsigned long long* __restrict__ starts,
+                                              uint32_t stride, uint64_t n, int k,
+                                              uint64_t* __restrict__ keys, uint32_t* err) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  const uint32_t sh = 2u * uint32_t(lane & 15);
+  uint32_t bad = 0;
+  for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
+    const int cnt = int(n - base < 32 ? n - base : 32);
+    Key<NW> mine;
+#pragma unroll
+    for (int w = 0; w < NW; ++w) mine.w[w] = 0;
+    for (int j = 0; j < cnt; ++j) {
+      const uint64_t line = base + j;
+      const uint64_t s = starts ? uint64_t(starts[line]) : body + line * stride;
+      uint32_t v[NW];
+      bool lbad = false;
+#pragma unroll
+      for (int h = 0; h < NW; ++h) {
+        const int ci = lane + 32 * h;
+        const uint64_t pos = s + ci;
+        const uint32_t c = (pos < end) ? uint32_t(__ldg(text + pos)) : uint32_t('\n');
+        if (ci < k) {
+          lbad |= (c == '\n') || (pos >= end);
+          v[h] = base_code(c);
+        } else {
+          v[h] = 0;
+          // fixed-width layout: the byte after the k-mer must end the line
+          if (!starts && ci == k && line + 1 < n && c != '\n') lbad = true;
+        }
+      }
+      if (__any_sync(0xFFFFFFFFu, lbad)) bad = 1;
+#pragma unroll
+      for (int h = 0; h < NW; ++h) {
+        const uint32_t x = v[h] << sh;
+        const uint32_t lo = __reduce_or_sync(0xFFFFFFFFu, lane < 16 ? x : 0u);
+        const uint32_t hi = __reduce_or_sync(0xFFFFFFFFu, lane >= 16 ? x : 0u);
+        if (lane == j) mine.w[h] = uint64_t(lo) | (uint64_t(hi) << 32);
+      }
+    }
+    if (lane < cnt) st_key<NW>(keys, base + lane, mine);
+  }
+  if (bad && lane == 0) atomicOr(err, starts ? ERR_LINE : ERR_LAYOUT);
+}
+
+// Line starts for the general layout: '\n' positions in [body, end).
+__global__ void k_count_nl(const uint8_t* __restrict__ text, uint64_t body, uint64_t end,
+                           uint32_t* __restrict__ cnt, uint32_t chunk) {
+  const uint64_t c0 = body + uint64_t(blockIdx.x) * chunk;
+  const uint64_t c1 = min(end, c0 + chunk);
+  uint32_t acc = 0;
+  for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) acc += (text[i] == '\n');
+  acc = __reduce_add_sync(0xFFFFFFFFu, acc);
+  __shared__ uint32_t sh[32];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < int(blockDim.x >> 5); ++w) t += sh[w];
+    cnt[blockIdx.x] = t;
+  }
+}
+
+__global__ void k_write_starts(const uint8_t* __restrict__ text, uint64_t body, uint64_t end,
+                               const unsigned long long* __restrict__ off, uint32_t chunk,
+                               unsigned long long* __restrict__ starts, uint64_t nlines) {
+  const uint64_t c0 = body + uint64_t(blockIdx.x) * chunk;
+  const uint64_t c1 = min(end, c0 + chunk);
+  if (blockIdx.x == 0 && threadIdx.x == 0) starts[0] = body;
+  // serial within a warp-strided pass: each thread scans a sub-range in order
+  const uint32_t per = (chunk + blockDim.x - 1) / blockDim.x;
+  const uint64_t lo = c0 + uint64_t(threadIdx.x) * per;
+  const uint64_t hi = min(c1, lo + per);
+  uint32_t mine = 0;
+  for (uint64_t i = lo; i < hi; ++i) mine += (text[i] == '\n');
+  __shared__ uint32_t sc[33];
+  uint32_t tot;
+  uint64_t r = off[blockIdx.x] + block_excl_scan(mine, sc, &tot);
+  for (uint64_t i = lo; i < hi; ++i) {
+    if (text[i] == '\n') {
+      ++r;
+      if (r < nlines) starts[r] = i + 1;
+    }
+  }
+}
+
+// ============================================================== minimizers
+
+template <int NW>
+__global__ void k_lmin(const uint64_t* __restrict__ keys, uint64_t n, int k, int l, uint64_t seed,
+                       const uint32_t* __restrict__ table, uint32_t* __restrict__ l1,
+                       uint32_t* __restrict__ l2) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    uint32_t a, b;
+    lmins<NW>(ld_key<NW>(keys, i), k, l, seed, table, a, b);
+    l1[i] = a;
+    l2[i] = b;
+  }
+}
+
+// Minimizers -> prefix bucket b1 and suffix bucket b2, counted per bucket
+// (find_l_minimizer "calc lmins" + "count lmins", lmin_buckets.h:299-318).
+template <int NW>
+__global__ void __launch_bounds__(256) k_lmin_count(const uint64_t* __restrict__ keys, uint64_t n,
+                                                    int k, int l, uint64_t seed, uint32_t bbits,
+                                                    uint32_t* __restrict__ b1, uint32_t* __restrict__ b2,
+                                                    uint32_t* __restrict__ counts) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += uint64_t(gridDim.x) * blockDim.x) {
+    uint32_t a, b;
+    lmins<NW>(ld_key<NW>(keys, i), k, l, seed, nullptr, a, b);
+    a = bucket_of(a, bbits);
+    b = bucket_of(b, bbits);
+    b1[i] = a;
+    b2[i] = b;
+    atomicAdd(counts + a, 1u);
+    if (a != b) atomicAdd(counts + b, 1u);
+  }
+}
+
+// ============================================================ tile planning
+
+// A bucket starts a new tile when its offset enters a new window of `win`
+// copies, or when it or its predecessor is larger than `small` (such buckets
+// sit alone).  Every packed tile then holds < win + small <= capacity copies.
+__global__ void k_tile_flags(const uint32_t* __restrict__ counts, const unsigned long long* __restrict__ off,
+                             uint32_t m, uint32_t win, uint32_t small, uint32_t* __restrict__ flag) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < m; b += gridDim.x * blockDim.x) {
+    uint32_t f = (b == 0);
+    if (b > 0) {
+      f |= (off[b] / win) != (off[b - 1] / win);
+      f |= counts[b] > small;
+      f |= counts[b - 1] > small;
+    }
+    flag[b] = f;
+  }
+}
+
+__global__ void k_tile_write(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ fidx,
+                             const unsigned long long* __restrict__ off, uint32_t m,
+                             unsigned long long* __restrict__ tile_begin, Counters* ctr) {
+  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < m; b += gridDim.x * blockDim.x) {
+    if (flag[b]) tile_begin[fidx[b]] = off[b];
+    if (b == m - 1) {
+      const uint32_t nt = fidx[b] + flag[b];
+      tile_begin[nt] = off[m];
+      ctr->ntiles = nt;
+    }
+  }
+}
+
+__global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Counters* ctr, uint32_t cap,
+                           uint32_t* __restrict__ big_list, unsigned long long* __restrict__ big_size,
+                           int nw) {
+  const uint32_t nt = ctr->ntiles;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+    const uint64_t c = tile_begin[t + 1] - tile_begin[t];
+    if (c > cap) {
+      const uint32_t i = atomicAdd(&ctr->nbig, 1u);
+      big_list[i] = t;
+      const uint64_t ts = uint64_t(pow2_at_least(2 * c));
+      big_size[i] = (c * (8ull * nw + 20ull) + ts * 4ull + 255ull) & ~255ull;
+    }
+  }
+}
+
+// ================================================================= scatter
+
+// Write every k-mer into its prefix bucket (role P) and, when its suffix
+// minimizer lands in another bucket, a second copy into that bucket (role S)
+// ("partition by lmins" + "write kmers", lmin_buckets.h:357-407).  The two
+// copies of a cross k-mer share one cross index; in edges mode every copy
+// carries the k-mer's id instead.
+template <int NW>
+__global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ keys,
+                                                 const uint32_t* __restrict__ b1,
+                                                 const uint32_t* __restrict__ b2, uint64_t n,
+                                                 unsigned long long* __restrict__ cursor,
+                                                 uint64_t* __restrict__ pkeys,
+                                                 uint32_t* __restrict__ plink, int ids_mode,
+                                                 Counters* ctr) {
+  const int lane = threadIdx.x & 31;
+  for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < n;
+       base += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t i = base + threadIdx.x;
+    const bool live = i < n;
+    uint32_t a = 0, b = 0;
+    Key<NW> key;
+    if (live) {
+      key = ld_key<NW>(keys, i);
+      a = b1[i];
+      b = b2[i];
+    }
+    const bool cross = live && (a != b);
+    uint32_t x = NONE;
+    if (!ids_mode) {
+      const uint32_t m = __ballot_sync(0xFFFFFFFFu, cross);
+      uint32_t basex = 0;
+      if (m) {
+        if (lane == __ffs(m) - 1) basex = atomicAdd(&ctr->cross_count, uint32_t(__popc(m)));
+        basex = __shfl_sync(0xFFFFFFFFu, basex, __ffs(m) - 1);
+      }
+      if (cross) x = basex + __popc(m & ((1u << lane) - 1u));
+    }
+    if (live) {
+      const uint32_t link = ids_mode ? uint32_t(i) : x;
+      Key<NW> kp = key;
+      kp.w[NW - 1] |= ROLE_P | (cross ? 0ull : ROLE_S);
+      const uint64_t p = atomicAdd(cursor + a, 1ull);
+      st_key<NW>(pkeys, p, kp);
+      plink[p] = link;
+      if (cross) {
+        Key<NW> ks = key;
+        ks.w[NW - 1] |= ROLE_S;
+        const uint64_t q = atomicAdd(cursor + b, 1ull);
+        st_key<NW>(pkeys, q, ks);
+        plink[q] = link;
+      }
+    }
+  }
+}
+
+// ==================================================================== tiles
+
+constexpr uint32_t DUP = 0x80000000u;
+constexpr uint32_t CAND_NONE = 0x7FFFFFFFu;
+
+template <int NW>
+struct TileMem {
+  uint64_t* key;   // [cap * NW]
+  uint32_t* link;  // [cap]
+  uint32_t* A;     // cand | DUP -> local successor
+  uint32_t* B;     // in-count -> rank
+  uint32_t* P;     // who -> local predecessor
+  uint32_t* Q;     // rank pointer
+  uint32_t* T;     // hash slots [ts] (>= 2*cap), later scratch
+  uint32_t ts;
+};
+
+template <int NW>
+__device__ __forceinline__ TileMem<NW> carve(char* base, uint32_t cap, uint32_t ts) {
+  TileMem<NW> m;
+  m.key = reinterpret_cast<uint64_t*>(base);
+  m.link = reinterpret_cast<uint32_t*>(m.key + size_t(cap) * NW);
+  m.A = m.link + cap;
+  m.B = m.A + cap;
+  m.P = m.B + cap;
+  m.Q = m.P + cap;
+  m.T = m.Q + cap;
+  m.ts = ts;
+  return m;
+}
+
+template <int NW>
+__device__ __forceinline__ Key<NW> skey(const TileMem<NW>& m, uint32_t i) {
+  Key<NW> k;
+#pragma unroll
+  for (int w = 0; w < NW; ++w) k.w[w] = m.key[size_t(i) * NW + w];
+  return k;
+}
+
+// Pointer jumping over the local predecessor links: Q[i] -> segment start,
+// B[i] -> distance from it.  Uses T[0..2c) as the second buffer and leaves
+// the result in (Q, B).
+template <int NW>
+__device__ void tile_rank(const TileMem<NW>& m, uint32_t c) {
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    const uint32_t p = m.P[i];
+    m.Q[i] = (p == NONE) ? i : p;
+    m.B[i] = (p == NONE) ? 0u : 1u;
+  }
+  __syncthreads();
+  uint32_t *px = m.Q, *rx = m.B, *py = m.T, *ry = m.T + c;
+  uint32_t rounds = 0;
+  for (uint32_t lim = 2; lim < 2 * c + 2; lim <<= 1) ++rounds;
+  rounds += 1;
+  for (uint32_t r = 0; r < rounds; ++r) {
+    int changed = 0;
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      const uint32_t p = px[i];
+      const uint32_t np = px[p];
+      py[i] = np;
+      ry[i] = rx[i] + rx[p];
+      changed |= (np != p);
+    }
+    uint32_t* t = px; px = py; py = t;
+    t = rx; rx = ry; ry = t;
+    if (!__syncthreads_or(changed)) break;
+  }
+  if (px != m.Q) {
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      m.Q[i] = px[i];
+      m.B[i] = rx[i];
+    }
+  }
+  __syncthreads();
+}
+
+template <int NW>
+__device__ void process_tile(const TileParams& p, const TileMem<NW>& m, uint64_t beg, uint32_t c) {
+  const PrefMask pm = pref_mask(p.k);
+  const uint32_t tmask = m.ts - 1;
+  const int k = p.k;
+  // ---- stage the tile's copies
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    const Key<NW> x = ld_key<NW>(p.pkeys, beg + i);
+#pragma unroll
+    for (int w = 0; w < NW; ++w) m.key[size_t(i) * NW + w] = x.w[w];
+    m.link[i] = p.plink[beg + i];
+    m.A[i] = CAND_NONE;
+    m.B[i] = 0;
+    m.P[i] = NONE;
+  }
+  for (uint32_t i = threadIdx.x; i < m.ts; i += blockDim.x) m.T[i] = NONE;
+  __syncthreads();
+  // ---- prefix table of the P copies (generate_hashmap, assembler.h:120-150):
+  // one slot per distinct (k-1)-prefix; a prefix shared by two copies marks
+  // the slot's copy DUP ("nullified")
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    const Key<NW> x = skey(m, i);
+    if (!(roles(x) & ROLE_P)) continue;
+    const Key<NW> pf = prefix_of(x, pm);
+    uint32_t h = key_hash(pf) & tmask;
+    for (uint32_t probe = 0; probe <= tmask; ++probe) {
+      const uint32_t cur = atomicCAS(m.T + h, NONE, i);
+      if (cur == NONE) break;
+      if (key_eq(prefix_of(skey(m, cur), pm), pf)) {
+        atomicOr(m.A + cur, DUP);
+        break;
+      }
+      h = (h + 1) & tmask;
+    }
+  }
+  __syncthreads();
+  // ---- suffix lookups of the S copies (find_vtx_from_edge, assembler.h:89-111)
+  // and in-degree counts ("count edges", assembler.h:180-188)
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    const Key<NW> x = skey(m, i);
+    if (!(roles(x) & ROLE_S)) continue;
+    const Key<NW> sf = suffix_of(x, pm);
+    uint32_t h = key_hash(sf) & tmask;
+    uint32_t cand = CAND_NONE;
+    for (uint32_t probe = 0; probe <= tmask; ++probe) {
+      const uint32_t cur = m.T[h];
+      if (cur == NONE) break;
+      if (key_eq(prefix_of(skey(m, cur), pm), sf)) {
+        if (!(m.A[cur] & DUP)) cand = cur;
+        break;
+      }
+      h = (h + 1) & tmask;
+    }
+    if (cand != CAND_NONE) {
+      atomicAdd(m.B + cand, 1u);
+      m.P[cand] = i;
+    }
+    m.A[i] = (m.A[i] & DUP) | cand;
+  }
+  __syncthreads();
+  // ---- kept edges: u->v iff v is u's unique successor and u is v's only
+  // predecessor ("write edges", assembler.h:189-197)
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    const uint32_t cand = m.A[i] & CAND_NONE;
+    const uint32_t s = (cand != CAND_NONE && m.B[cand] == 1u) ? cand : NONE;
+    const uint32_t q = (m.B[i] == 1u) ? m.P[i] : NONE;
+    __syncwarp();
+    m.A[i] = s;
+    m.P[i] = q;
+  }
+  __syncthreads();
+  if (p.mode == 0) {
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      const uint64_t r = roles(skey(m, i));
+      if (r & ROLE_S) p.succ[m.link[i]] = (m.A[i] == NONE) ? NONE : m.link[m.A[i]];
+      if (r & ROLE_P) p.pred[m.link[i]] = (m.P[i] == NONE) ? NONE : m.link[m.P[i]];
+    }
+    return;
+  }
+  // ---- local segments: list ranking by pointer jumping
+  tile_rank(m, c);
+  // ---- local cycles (every copy has a local predecessor): cut each at its
+  // smallest key, then rank again
+  int cyc = 0;
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    // after ranking, a path copy points at its start (no predecessor); a
+    // cycle copy points at another cycle copy.  Flag cycle copies in A's top
+    // bit (A holds a local index < 2^31 or NONE; a cycle copy has a successor).
+    if (m.P[m.Q[i]] != NONE) {
+      m.A[i] |= DUP;
+      cyc = 1;
+    }
+  }
+  if (__syncthreads_or(cyc)) {
+    uint32_t *lx = m.T, *jx = m.T + c, *ly = m.B, *jy = m.Q;  // B/Q recomputed below
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      lx[i] = i;
+      jx[i] = (m.P[i] == NONE) ? i : m.P[i];
+    }
+    __syncthreads();
+    uint32_t rounds = 1;
+    for (uint32_t lim = 1; lim < c; lim <<= 1) ++rounds;
+    for (uint32_t r = 0; r < rounds; ++r) {
+      for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+        const uint32_t j = jx[i];
+        const uint32_t a = lx[i], b = lx[j];
+        ly[i] = key_lt(skey(m, b), skey(m, a)) ? b : a;
+        jy[i] = jx[j];
+      }
+      __syncthreads();
+      uint32_t* t = lx; lx = ly; ly = t;
+      t = jx; jx = jy; jy = t;
+    }
+    // After ceil(log2 c)+1 rounds a cycle copy's label covers its whole
+    // cycle, so exactly one copy per cycle (the smallest key) is its own
+    // label.  Cut the edge into it; path copies are not touched.
+    int cut = 0;
+    // (a cycle copy always has a successor, so its A is index | DUP, never NONE)
+    auto on_cycle = [](uint32_t a) { return a != NONE && (a & DUP); };
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      if (on_cycle(m.A[i]) && lx[i] == i) cut = 1;
+    }
+    (void)cut;
+    __syncthreads();
+    // the cycle minimum loses its in-edge: its predecessor becomes the end
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      if (on_cycle(m.A[i]) && lx[i] == i) {
+        const uint32_t q = m.P[i];
+        m.A[q] = NONE;
+        m.P[i] = NONE;
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      const uint32_t a = m.A[i];
+      if (on_cycle(a)) m.A[i] = a & ~DUP;
+    }
+    __syncthreads();
+    tile_rank(m, c);
+  }
+  // every copy now reaches a segment start
+
+  // ---- emission: closed segments (start has role P, end has role S) are
+  // whole unitigs; the others are stitched across tiles
+  __shared__ unsigned long long sc64[33];
+  __shared__ unsigned long long s_base[3];
+  __shared__ int s_skip;
+  const uint32_t chunk = (c + blockDim.x - 1) / blockDim.x;
+  const uint32_t lo = min(c, threadIdx.x * chunk), hi = min(c, lo + chunk);
+  unsigned long long cb = 0, ob = 0, oc = 0;
+  for (uint32_t i = lo; i < hi; ++i) {
+    if (m.A[i] != NONE) continue;
+    const uint32_t s = m.Q[i];
+    const uint32_t len = m.B[i] + 1;
+    const bool closed = (roles(skey(m, s)) & ROLE_P) && (roles(skey(m, i)) & ROLE_S);
+    if (closed) cb += uint64_t(k) + len;
+    else { ob += uint64_t(k) - 1 + len; oc += 1; }
+  }
+  unsigned long long tcb, tob, toc;
+  unsigned long long pcb = block_excl_scan(cb, sc64, &tcb);
+  unsigned long long pob = block_excl_scan(ob, sc64, &tob);
+  unsigned long long poc = block_excl_scan(oc, sc64, &toc);
+  if (threadIdx.x == 0) {
+    s_skip = 0;
+    s_base[0] = tcb ? atomicAdd(&p.ctr->out_cursor, tcb) : 0ull;
+    s_base[1] = tob ? atomicAdd(&p.ctr->seg_char_cursor, tob) : 0ull;
+    s_base[2] = toc ? atomicAdd(&p.ctr->seg_count, uint32_t(toc)) : 0u;
+    if (s_base[0] + tcb > p.out_cap || s_base[1] + tob > p.segchars_cap ||
+        s_base[2] + toc > p.seg_cap) {
+      atomicOr(&p.ctr->err, ERR_CAPACITY);
+      s_skip = 1;
+    }
+  }
+  __syncthreads();
+  if (s_skip) return;
+  const unsigned long long cbase = s_base[0], obase = s_base[1], sbase = s_base[2];
+  // per segment start: tile-local byte offset (T[s]) and local segment index
+  // (T[c + s], NONE for a closed segment)
+  for (uint32_t i = lo; i < hi; ++i) {
+    if (m.A[i] != NONE) continue;
+    const uint32_t s = m.Q[i];
+    const uint32_t len = m.B[i] + 1;
+    const bool closed = (roles(skey(m, s)) & ROLE_P) && (roles(skey(m, i)) & ROLE_S);
+    if (closed) {
+      m.T[s] = uint32_t(pcb);
+      m.T[c + s] = NONE;
+      pcb += uint64_t(k) + len;
+    } else {
+      m.T[s] = uint32_t(pob);
+      m.T[c + s] = uint32_t(poc);
+      pob += uint64_t(k) - 1 + len;
+      poc += 1;
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    const uint32_t s = m.Q[i];
+    const uint32_t r = m.B[i];
+    const uint32_t loc = m.T[s];
+    const uint32_t sid = m.T[c + s];
+    const Key<NW> x = skey(m, i);
+    char* dst = (sid == NONE) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
+    if (r == 0) {
+      for (int ch = 0; ch < k; ++ch) dst[ch] = acgt(key_char(x, ch));
+    } else {
+      dst[k - 1 + r] = acgt(key_char(x, k - 1));
+    }
+    if (m.A[i] == NONE) {
+      if (sid == NONE) {
+        dst[k + r] = '\n';
+      } else {
+        const uint32_t g = uint32_t(sbase) + sid;
+        const bool s_only = (roles(skey(m, s)) & ROLE_P) == 0;
+        const bool p_only = (roles(x) & ROLE_S) == 0;
+        p.seg_off[g] = obase + loc;
+        p.seg_len[g] = r + 1;
+        p.seg_sx[g] = s_only ? m.link[s] : NONE;
+        p.seg_ex[g] = p_only ? m.link[i] : NONE;
+        if (s_only) p.start_seg[m.link[s]] = g;
+        if (p_only) p.end_seg[m.link[i]] = g;
+      }
+    }
+  }
+}
+
+// Persistent tile kernel: each CTA takes the next tile from a global
+// counter until none are left; tiles larger than the capacity are left for
+// k_tile_big.
+template <int NW>
+__global__ void __launch_bounds__(512) k_tile(TileParams p) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ uint32_t s_t;
+  const TileMem<NW> m = carve<NW>(smem, p.cap, p.tslots);
+  const uint32_t nt = p.ctr->ntiles;
+  for (;;) {
+    if (threadIdx.x == 0) s_t = atomicAdd(&p.ctr->tile_next, 1u);
+    __syncthreads();
+    const uint32_t t = s_t;
+    __syncthreads();
+    if (t >= nt) break;
+    const uint64_t beg = p.tile_begin[t];
+    const uint64_t c = p.tile_begin[t + 1] - beg;
+    if (c == 0 || c > p.cap) continue;
+    process_tile<NW>(p, m, beg, uint32_t(c));
+    __syncthreads();
+  }
+}
+
+// One CTA per oversized tile, working in global scratch.
+template <int NW>
+__global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
+  const uint32_t t = p.big_list[blockIdx.x];
+  const uint64_t beg = p.tile_begin[t];
+  const uint64_t c = p.tile_begin[t + 1] - beg;
+  const uint32_t ts = pow2_at_least(2 * c);
+  const TileMem<NW> m = carve<NW>(p.big_scratch + p.big_off[blockIdx.x], uint32_t(c), ts);
+  process_tile<NW>(p, m, beg, uint32_t(c));
+}
+
+// ================================================================= stitch
+
+// next/prev/weight of each open segment.  A segment ending in a P-only copy
+// of cross k-mer x continues with the segment starting at x's S-only copy;
+// both hold x, so every later segment drops its first k chars
+// (write_unitigs4, compact.h:59-112).
+__global__ void k_seg_link(const Counters* __restrict__ ctr, const uint32_t* __restrict__ seg_sx,
+                           const uint32_t* __restrict__ seg_ex, const uint32_t* __restrict__ seg_len,
+                           const uint32_t* __restrict__ start_seg, const uint32_t* __restrict__ end_seg,
+                           uint32_t* __restrict__ next, uint32_t* __restrict__ prev,
+                           uint32_t* __restrict__ w, int k) {
+  const uint32_t S = ctr->seg_count;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+    const uint32_t ex = seg_ex[s], sx = seg_sx[s];
+    const uint32_t nx = (ex == NONE) ? NONE : start_seg[ex];
+    const uint32_t pv = (sx == NONE) ? NONE : end_seg[sx];
+    next[s] = nx;
+    prev[s] = pv;
+    w[s] = (pv == NONE) ? uint32_t(k) - 1u + seg_len[s] : seg_len[s] - 1u;
+  }
+}
+
+__device__ __forceinline__ unsigned long long pk(uint32_t p, uint32_t o) {
+  return (static_cast<unsigned long long>(o) << 32) | p;
+}
+__device__ __forceinline__ uint32_t pk_p(unsigned long long v) { return uint32_t(v); }
+__device__ __forceinline__ uint32_t pk_o(unsigned long long v) { return uint32_t(v >> 32); }
+// A head's own entry carries HEAD_BIT in its pointer, so "reached a head" is
+// a property of the target entry, not a self-pointer (which a pointer running
+// around a cycle can also produce).  Entry counts stay below 2^31.
+constexpr uint32_t HEAD_BIT = 0x80000000u;
+__device__ __forceinline__ uint32_t ptr_of(unsigned long long v) { return pk_p(v) & ~HEAD_BIT; }
+__device__ __forceinline__ bool is_head_entry(unsigned long long v) { return (pk_p(v) & HEAD_BIT) != 0; }
+
+// X[v] = (start pointer, weight distance); heads point at themselves.
+__global__ void k_rank_init(const uint32_t* __restrict__ prev, const uint32_t* __restrict__ w,
+                            uint64_t n, const Counters* ctr, unsigned long long* __restrict__ X,
+                            uint32_t* __restrict__ act, uint32_t* act_count) {
+  const uint64_t N = ctr ? uint64_t(ctr->seg_count) : n;
+  for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < N;
+       s += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t pv = prev[s];
+    if (pv == NONE) {
+      X[s] = pk(uint32_t(s) | HEAD_BIT, 0);
+    } else {
+      X[s] = pk(pv, w ? w[pv] : 1u);
+      act[atomicAdd(act_count, 1u)] = uint32_t(s);
+    }
+  }
+}
+
+// One round of asynchronous pointer jumping over the active list.  Entries
+// are (pointer, distance) pairs in one 64-bit word, so a concurrent reader
+// always sees a consistent pair; the list keeps the entries whose pointer
+// does not yet reach a head.
+__global__ void k_rank_round(unsigned long long* __restrict__ X, const uint32_t* __restrict__ act,
+                             const uint32_t* act_count, uint32_t* __restrict__ act_out,
+                             uint32_t* act_out_count) {
+  const uint32_t na = *act_count;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < na; j += gridDim.x * blockDim.x) {
+    const uint32_t s = act[j];
+    const unsigned long long v = reinterpret_cast<volatile unsigned long long*>(X)[s];
+    const unsigned long long u = reinterpret_cast<volatile unsigned long long*>(X)[ptr_of(v)];
+    if (is_head_entry(u)) continue;  // already points at a head
+    const unsigned long long nv = pk(ptr_of(u), pk_o(v) + pk_o(u));
+    reinterpret_cast<volatile unsigned long long*>(X)[s] = nv;
+    const unsigned long long z = reinterpret_cast<volatile unsigned long long*>(X)[ptr_of(nv)];
+    if (!is_head_entry(z)) act_out[atomicAdd(act_out_count, 1u)] = s;
+  }
+}
+
+// Line length of each chain, stored at its head.
+__global__ void k_chain_len(const Counters* __restrict__ ctr, const unsigned long long* __restrict__ X,
+                            const uint32_t* __restrict__ next, const uint32_t* __restrict__ w,
+                            const uint8_t* __restrict__ oncycle, uint32_t* __restrict__ linelen) {
+  const uint32_t S = ctr->seg_count;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+    if (next[s] == NONE && !oncycle[s]) {
+      const unsigned long long v = X[s];
+      linelen[ptr_of(v)] = pk_o(v) + w[s] + 1u;
+    }
+  }
+}
+
+__global__ void k_head_len(const Counters* __restrict__ ctr, const uint32_t* __restrict__ prev,
+                           const uint32_t* __restrict__ linelen, uint32_t* __restrict__ v) {
+  const uint32_t S = ctr->seg_count;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x)
+    v[s] = (prev[s] == NONE) ? linelen[s] : 0u;
+}
+
+// Copy each segment's chars into its line (warp per segment).
+__global__ void k_seg_copy(Counters* __restrict__ ctr, const unsigned long long* __restrict__ X,
+                           const uint32_t* __restrict__ next, const uint32_t* __restrict__ prev,
+                           const uint32_t* __restrict__ w, const uint8_t* __restrict__ oncycle,
+                           const unsigned long long* __restrict__ seg_off,
+                           const unsigned long long* __restrict__ loff, const char* __restrict__ segchars,
+                           char* __restrict__ out, unsigned long long base, int k) {
+  const uint32_t S = ctr->seg_count;
+  const int lane = threadIdx.x & 31;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (uint32_t s = warp; s < S; s += nwarps) {
+    if (oncycle[s]) continue;
+    const unsigned long long v = X[s];
+    char* dst = out + base + loff[ptr_of(v)] + pk_o(v);
+    const char* src = segchars + seg_off[s] + ((prev[s] == NONE) ? 0 : k);
+    const uint32_t nb = w[s];
+    for (uint32_t j = lane; j < nb; j += 32) dst[j] = src[j];
+    if (lane == 0 && next[s] == NONE) dst[nb] = '\n';
+  }
+}
+
+__global__ void k_mark_cycle(const uint32_t* __restrict__ act, const uint32_t* act_count,
+                             uint8_t* __restrict__ oncycle) {
+  const uint32_t na = *act_count;
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < na; j += gridDim.x * blockDim.x)
+    oncycle[act[j]] = 1;
+}
+
+// Cycles of segments (rare): one thread spells each cycle starting at its
+// smallest k-mer.  The cycle's distinct k-mers are the last chars of each
+// segment after its first k-mer, read circularly.
+template <int NW>
+__global__ void k_seg_cycles(Counters* ctr, const uint32_t* __restrict__ act, uint32_t na,
+                             uint8_t* __restrict__ oncycle, const uint32_t* __restrict__ next,
+                             const uint32_t* __restrict__ seg_len,
+                             const unsigned long long* __restrict__ seg_off,
+                             const char* __restrict__ segchars, char* __restrict__ out,
+                             unsigned long long out_cap, int k) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (uint32_t j = 0; j < na; ++j) {
+    const uint32_t s0 = act[j];
+    if (oncycle[s0] != 1) continue;
+    // total distinct k-mers N and the circular char accessor
+    uint64_t N = 0;
+    uint32_t s = s0;
+    do {
+      N += seg_len[s] - 1u;
+      oncycle[s] = 2;
+      s = next[s];
+    } while (s != s0 && s != NONE);
+    if (s == NONE || N == 0) {
+      atomicOr(&ctr->err, ERR_INTERNAL);
+      continue;
+    }
+    // char q of the circular string: segment chars after the first k
+    auto at = [&](uint64_t q) -> char {
+      uint32_t t = s0;
+      for (;;) {
+        const uint64_t m = seg_len[t] - 1u;
+        if (q < m) return segchars[seg_off[t] + k + q];
+        q -= m;
+        t = next[t];
+      }
+    };
+    // the k-mer ending at circular position q; find the smallest
+    auto kmer_at = [&](uint64_t q) {
+      Key<NW> x;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) x.w[w] = 0;
+      for (int c = 0; c < k; ++c) {
+        const char ch = at((q + N * 64 - (k - 1) + c) % N);
+        const uint64_t code = (ch == 'C') ? 1 : (ch == 'G') ? 2 : (ch == 'T') ? 3 : 0;
+        if (c < 32) x.w[0] |= code << (2 * c);
+        else if (NW == 2) x.w[NW - 1] |= code << (2 * (c - 32));
+      }
+      return x;
+    };
+    uint64_t best = 0;
+    Key<NW> bk = kmer_at(0);
+    for (uint64_t q = 1; q < N; ++q) {
+      const Key<NW> x = kmer_at(q);
+      if (key_lt(x, bk)) { bk = x; best = q; }
+    }
+    const uint64_t len = uint64_t(k) + N;  // k + (N - 1) chars + '\n'
+    const unsigned long long o = atomicAdd(&ctr->out_cursor, len);
+    if (o + len > out_cap) {
+      atomicOr(&ctr->err, ERR_CAPACITY);
+      return;
+    }
+    for (uint64_t t = 0; t + 1 < len; ++t) out[o + t] = at((best + N * 64 - (k - 1) + t) % N);
+    out[o + len - 1] = '\n';
+    atomicAdd(&ctr->cycles, 1ull);
+  }
+}
+
+__global__ void k_add_cursor(Counters* ctr, const unsigned long long* total) {
+  ctr->out_cursor += *total;
+}
+
+// ======================================================= phase-API helpers
+
+__global__ void k_head_rank(const unsigned long long* __restrict__ X, uint64_t n,
+                            uint32_t* __restrict__ head, uint32_t* __restrict__ rank) {
+  for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+       v += uint64_t(gridDim.x) * blockDim.x) {
+    const unsigned long long x = X[v];
+    head[v] = ptr_of(x);
+    rank[v] = pk_o(x);
+  }
+}
+
+// Cycle vertices of the global graph (rare): one thread ranks each cycle from
+// its smallest key.
+template <int NW>
+__global__ void k_vertex_cycles(const uint32_t* __restrict__ act, uint32_t na,
+                                const uint32_t* __restrict__ succ, const uint64_t* __restrict__ keys,
+                                uint32_t* __restrict__ head, uint32_t* __restrict__ rank,
+                                uint8_t* __restrict__ seen, unsigned long long* ncyc) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  for (uint32_t j = 0; j < na; ++j) {
+    const uint32_t v0 = act[j];
+    if (seen[v0]) continue;
+    uint32_t best = v0;
+    Key<NW> bk = ld_key<NW>(keys, v0);
+    for (uint32_t x = succ[v0]; x != v0 && x != NONE; x = succ[x]) {
+      const Key<NW> xk = ld_key<NW>(keys, x);
+      if (key_lt(xk, bk)) { bk = xk; best = x; }
+    }
+    uint32_t r = 0, x = best;
+    do {
+      head[x] = best;
+      rank[x] = r++;
+      seen[x] = 1;
+      x = succ[x];
+    } while (x != best && x != NONE);
+    ++*ncyc;
+  }
+}
+
+__global__ void k_count_members(const uint32_t* __restrict__ head, uint64_t n, uint32_t* __restrict__ cnt) {
+  for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+       v += uint64_t(gridDim.x) * blockDim.x)
+    atomicAdd(cnt + head[v], 1u);
+}
+
+__global__ void k_line_len(const uint32_t* __restrict__ head, const uint32_t* __restrict__ cnt,
+                           uint64_t n, int k, uint32_t* __restrict__ len) {
+  for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+       v += uint64_t(gridDim.x) * blockDim.x)
+    len[v] = (head[v] == uint32_t(v)) ? uint32_t(k) + cnt[v] : 0u;
+}
+
+// Spell each vertex's chars at its line offset (write_intra_bucket_outputs,
+// compact.h:187-208): rank 0 writes the whole k-mer, rank r writes its last
+// char at k-1+r, the last member adds '\n'.
+template <int NW>
+__global__ void k_spell(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ head,
+                        const uint32_t* __restrict__ rank, const uint32_t* __restrict__ cnt,
+                        const unsigned long long* __restrict__ loff, uint64_t n, int k,
+                        char* __restrict__ out) {
+  for (uint64_t v = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; v < n;
+       v += uint64_t(gridDim.x) * blockDim.x) {
+    const Key<NW> x = ld_key<NW>(keys, v);
+    const uint32_t h = head[v], r = rank[v];
+    char* dst = out + loff[h];
+    if (r == 0) {
+      for (int c = 0; c < k; ++c) dst[c] = acgt(key_char(x, c));
+    } else {
+      dst[k - 1 + r] = acgt(key_char(x, k - 1));
+    }
+    if (r + 1 == cnt[h]) dst[k + r] = '\n';
+  }
+}
+
+// =========================================================== host pipeline
+
+static int grid_for(const Env& e, uint64_t work, int block) {
+  const uint64_t want = (work + block - 1) / block;
+  const uint64_t cap = uint64_t(e.sm_count) * 16;
+  return int(std::max<uint64_t>(1, std::min(want, cap)));
+}
+
+#define UC_CK(call)                                                            \
+  do {                                                                         \
+    cudaError_t _e = (call);                                                   \
+    if (_e != cudaSuccess) return e.fail(UC_ECUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+int Env::fail(int code, const std::string& msg) {
+  err = msg;
+  return code;
+}
+
+void* Env::take(size_t bytes) {
+  const size_t a = (used + 255) & ~size_t(255);
+  if (a + bytes > cap) return nullptr;
+  used = a + bytes;
+  return arena + a;
+}
+
+int Env::reserve(size_t bytes) {
+  bytes = (bytes + (size_t(64) << 20));
+  if (bytes <= cap) return UC_OK;
+  if (bytes > budget) return fail(UC_EBUDGET, "job needs " + std::to_string(bytes >> 20) + " MiB, budget " +
+                                                  std::to_string(budget >> 20) + " MiB");
+  if (arena) {
+    cudaStreamSynchronize(stream);
+    cudaFree(arena);
+    arena = nullptr;
+    cap = 0;
+  }
+  if (cudaMalloc(&arena, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    arena = nullptr;
+    return fail(UC_ENOMEM, "cudaMalloc of " + std::to_string(bytes >> 20) + " MiB failed");
+  }
+  cap = bytes;
+  return UC_OK;
+}
+
+int Env::check_err(const Counters* h) {
+  const uint32_t f = h->err;
+  if (!f) return UC_OK;
+  if (f & ERR_LINE) return fail(UC_EINPUT, "a k-mer line is shorter than k");
+  if (f & ERR_COUNT) return fail(UC_EINPUT, "header count differs from the number of lines");
+  if (f & ERR_TIMEOUT) return fail(UC_ETIMEOUT, "a bounded device wait ran out");
+  if (f & ERR_CAPACITY) return fail(UC_EINTERNAL, "an output bound was exceeded");
+  return fail(UC_EINTERNAL, "internal invariant failed (flags " + std::to_string(f) + ")");
+}
+
+// Parse the count line: reads the first bytes back to the host.
+int parse_header(Env& e, const char* d_text, size_t bytes, uint64_t& n, uint64_t& body) {
+  std::vector<char> h;
+  size_t want = std::min<size_t>(bytes, 256);
+  for (;;) {
+    h.resize(want);
+    if (want) UC_CK(cudaMemcpyAsync(h.data(), d_text, want, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    size_t p = 0;
+    while (p < want && (h[p] == ' ' || h[p] == '\t' || h[p] == '\r')) ++p;
+    if (p >= want || h[p] < '0' || h[p] > '9') {
+      if (want < bytes && p >= want) { want = std::min(bytes, want * 4); continue; }
+      return e.fail(UC_EINPUT, "missing k-mer count header");
+    }
+    uint64_t v = 0;
+    while (p < want && h[p] >= '0' && h[p] <= '9') {
+      v = v * 10 + uint64_t(h[p] - '0');
+      if (v > 0xFFFFFFFEull) return e.fail(UC_EINPUT, "k-mer count too large");
+      ++p;
+    }
+    while (p < want && h[p] != '\n') ++p;
+    if (p >= want && want < bytes) { want = std::min(bytes, want * 4); continue; }
+    n = v;
+    body = (p < want) ? p + 1 : want;
+    return UC_OK;
+  }
+}
+
+// Scratch of the general-layout line index.
+static size_t line_index_bytes(size_t bytes, uint64_t n) {
+  const uint64_t nchunks = bytes / (1 << 16) + 2;
+  return nchunks * 4 + (nchunks + 1) * 8 + scan_tmp_elems(nchunks) * 8 + (n + 1) * 8 + 8 * 256;
+}
+
+// End of the k-mer lines: trailing '\n' / '\r' bytes are not a line.
+static int text_end(Env& e, const char* d_text, size_t bytes, uint64_t body, uint64_t& end) {
+  end = bytes;
+  char tail[256];
+  while (end > body) {
+    const size_t take = std::min<uint64_t>(256, end - body);
+    UC_CK(cudaMemcpyAsync(tail, d_text + end - take, take, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    size_t j = take;
+    while (j > 0 && (tail[j - 1] == '\n' || tail[j - 1] == '\r')) --j;
+    end -= (take - j);
+    if (j > 0) break;
+  }
+  return UC_OK;
+}
+
+int pack(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t& n_out) {
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  uint64_t n = 0, body = 0, end = 0;
+  int st = parse_header(e, d_text, bytes, n, body);
+  if (st) return st;
+  st = text_end(e, d_text, bytes, body, end);
+  if (st) return st;
+  n_out = n;
+  const uint8_t* text = reinterpret_cast<const uint8_t*>(d_text);
+  UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+  if (n == 0) {
+    if (end > body) return e.fail(UC_EINPUT, "header count differs from the number of lines");
+    return UC_OK;
+  }
+  const int nw = (k <= 31) ? 1 : 2;
+  const uint32_t stride = uint32_t(k) + 1;
+  bool fixed = (end - body) == n * stride - 1;
+  const int block = 256;
+  const int grid = grid_for(e, (n + 7) / 8 * 32, block);
+  if (fixed) {
+    if (nw == 1) k_pack<1><<<grid, block, 0, e.stream>>>(text, body, end, nullptr, stride, n, k, d_keys, &e.ctr->err);
+    else k_pack<2><<<grid, block, 0, e.stream>>>(text, body, end, nullptr, stride, n, k, d_keys, &e.ctr->err);
+    UC_CK(cudaGetLastError());
+    UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    if (e.h_ctr->err & ERR_LAYOUT) {
+      fixed = false;
+      UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+    } else if (e.h_ctr->err) {
+      return e.check_err(e.h_ctr);
+    }
+  }
+  if (!fixed) {
+    // general layout: index the line starts
+    const uint32_t chunk = 1 << 16;
+    const uint64_t nchunks = std::max<uint64_t>(1, (end - body + chunk - 1) / chunk);
+    if (e.used == 0) {
+      const int r = e.reserve(line_index_bytes(bytes, n));
+      if (r) return r;
+    }
+    const size_t mark = e.used;
+    uint32_t* cnt = static_cast<uint32_t*>(e.take(nchunks * 4));
+    unsigned long long* off = static_cast<unsigned long long*>(e.take((nchunks + 1) * 8));
+    unsigned long long* tmp = static_cast<unsigned long long*>(e.take(scan_tmp_elems(nchunks) * 8));
+    unsigned long long* starts = static_cast<unsigned long long*>(e.take((n + 1) * 8));
+    if (!cnt || !off || !tmp || !starts) return e.fail(UC_EBUDGET, "scratch for the line index");
+    k_count_nl<<<unsigned(nchunks), 256, 0, e.stream>>>(text, body, end, cnt, chunk);
+    scan_excl<uint32_t, unsigned long long>(cnt, nchunks, off, tmp, e.stream);
+    unsigned long long lines_m1 = 0;
+    UC_CK(cudaMemcpyAsync(&lines_m1, off + nchunks, 8, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    if (lines_m1 + 1 != n) return e.fail(UC_EINPUT, "header count differs from the number of lines");
+    k_write_starts<<<unsigned(nchunks), 256, 0, e.stream>>>(text, body, end, off, chunk, starts, n);
+    if (nw == 1) k_pack<1><<<grid, block, 0, e.stream>>>(text, body, end, starts, stride, n, k, d_keys, &e.ctr->err);
+    else k_pack<2><<<grid, block, 0, e.stream>>>(text, body, end, starts, stride, n, k, d_keys, &e.ctr->err);
+    UC_CK(cudaGetLastError());
+    UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    e.used = mark;
+    if (e.h_ctr->err) return e.check_err(e.h_ctr);
+  }
+  return UC_OK;
+}
+
+int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed,
+               const uint32_t* d_table, uint32_t* l1, uint32_t* l2) {
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
+  if (n == 0) return UC_OK;
+  const int grid = grid_for(e, n, 256);
+  if (k <= 31) k_lmin<1><<<grid, 256, 0, e.stream>>>(d_keys, n, k, l, seed, d_table, l1, l2);
+  else k_lmin<2><<<grid, 256, 0, e.stream>>>(d_keys, n, k, l, seed, d_table, l1, l2);
+  UC_CK(cudaGetLastError());
+  return UC_OK;
+}
+
+// Bucket plan for n k-mers: bucket bits and the minimizer length actually used.
+void plan_buckets(const Env& e, uint64_t n, int k, int l, uint32_t& bbits, int& l_used, uint32_t& cap,
+                  uint32_t& win, uint32_t& small) {
+  cap = e.tune.tile_capacity ? e.tune.tile_capacity : 4096;
+  // the tile (copies + hash slots) must fit one block's shared memory
+  const int nw = (k <= 31) ? 1 : 2;
+  while (cap > 256 && tile_bytes(nw, cap, pow2_at_least(2ull * cap)) > size_t(e.smem_optin)) cap -= 256;
+  const uint64_t copies = n + n / 8 + 1;
+  if (e.tune.bucket_bits) {
+    bbits = e.tune.bucket_bits;
+  } else {
+    // ~cap/8 copies per bucket on average
+    bbits = 0;
+    while ((copies >> bbits) > cap / 8 && bbits < 24) ++bbits;
+  }
+  // enough l-mers that each bucket gathers several of them
+  int lmin = int((bbits + 2 + 1) / 2);
+  l_used = std::max(l, lmin);
+  l_used = std::min(l_used, std::min(16, k - 1));
+  win = cap - cap / 4;
+  small = cap / 4;
+}
+
+struct Fused {
+  uint64_t* keys;
+  uint32_t *b1, *b2, *counts;
+  unsigned long long *boff, *cursor, *tile_begin, *scan_tmp;
+  uint32_t *flag, *fidx, *big_list;
+  unsigned long long* big_size;
+  uint64_t* pkeys;
+  uint32_t* plink;
+};
+
+// Shared front half: pack, minimizers, counts, scan, tile plan, scatter.
+static int front(Env& e, const char* d_text, size_t bytes, int k, int l, int ids_mode,
+                 const uint64_t* given_keys, uint64_t given_n, uint64_t seed, Fused& f,
+                 uint64_t& n, uint32_t& cap, uint32_t& tslots, uc_stats* st, int& l_used,
+                 uint32_t& bbits) {
+  const int nw = (k <= 31) ? 1 : 2;
+  if (given_keys) {
+    n = given_n;
+  } else {
+    uint64_t body = 0;
+    int r = parse_header(e, d_text, bytes, n, body);
+    if (r) return r;
+  }
+  uint32_t win, small;
+  plan_buckets(e, n, k, l, bbits, l_used, cap, win, small);
+  const uint64_t M = 1ull << bbits;
+  tslots = pow2_at_least(uint64_t(cap) * std::max<uint32_t>(200, e.tune.load_factor_pct) / 100);
+  if (tslots < 2 * cap) tslots = pow2_at_least(2ull * cap);
+  while (tslots > pow2_at_least(2ull * cap) && tile_bytes(nw, cap, tslots) > size_t(e.smem_optin)) tslots >>= 1;
+  // allocations (upper bounds from n)
+  const uint64_t ncp = 2 * n + 1;
+  size_t need = 0;
+  auto add = [&](size_t b) { need += (b + 255) & ~size_t(255); };
+  if (!given_keys) {
+    add(n * 8 * nw);
+    add(line_index_bytes(bytes, n));
+  }
+  add(n * 4); add(n * 4); add(M * 4); add((M + 1) * 8); add(M * 8); add((M + 2) * 8);
+  add(scan_tmp_elems(M) * 8); add(M * 4); add((M + 1) * 4); add(M * 4); add(M * 8);
+  add(ncp * 8 * nw); add(ncp * 4);
+  int r = e.reserve(e.used + need + e.extra_need);
+  if (r) return r;
+  f.keys = given_keys ? const_cast<uint64_t*>(given_keys) : static_cast<uint64_t*>(e.take(n * 8 * nw));
+  f.b1 = static_cast<uint32_t*>(e.take(n * 4));
+  f.b2 = static_cast<uint32_t*>(e.take(n * 4));
+  f.counts = static_cast<uint32_t*>(e.take(M * 4));
+  f.boff = static_cast<unsigned long long*>(e.take((M + 1) * 8));
+  f.cursor = static_cast<unsigned long long*>(e.take(M * 8));
+  f.tile_begin = static_cast<unsigned long long*>(e.take((M + 2) * 8));
+  f.scan_tmp = static_cast<unsigned long long*>(e.take(scan_tmp_elems(M) * 8));
+  f.flag = static_cast<uint32_t*>(e.take(M * 4));
+  f.fidx = static_cast<uint32_t*>(e.take((M + 1) * 4));
+  f.big_list = static_cast<uint32_t*>(e.take(M * 4));
+  f.big_size = static_cast<unsigned long long*>(e.take(M * 8));
+  f.pkeys = static_cast<uint64_t*>(e.take(ncp * 8 * nw));
+  f.plink = static_cast<uint32_t*>(e.take(ncp * 4));
+  if (!f.plink) return e.fail(UC_EBUDGET, "arena overflow");
+  if (!given_keys) {
+    uint64_t n2 = 0;
+    cudaEventRecord(e.ev[0], e.stream);
+    r = pack(e, d_text, bytes, k, f.keys, n2);
+    if (r) return r;
+  } else {
+    UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+    cudaEventRecord(e.ev[0], e.stream);
+  }
+  cudaEventRecord(e.ev[1], e.stream);
+  UC_CK(cudaMemsetAsync(f.counts, 0, M * 4, e.stream));
+  if (n > 0) {
+    const int grid = grid_for(e, n, 256);
+    if (nw == 1) k_lmin_count<1><<<grid, 256, 0, e.stream>>>(f.keys, n, k, l_used, seed, bbits, f.b1, f.b2, f.counts);
+    else k_lmin_count<2><<<grid, 256, 0, e.stream>>>(f.keys, n, k, l_used, seed, bbits, f.b1, f.b2, f.counts);
+    UC_CK(cudaGetLastError());
+  }
+  scan_excl<uint32_t, unsigned long long>(f.counts, M, f.boff, f.scan_tmp, e.stream);
+  UC_CK(cudaMemcpyAsync(f.cursor, f.boff, M * 8, cudaMemcpyDeviceToDevice, e.stream));
+  const int gm = grid_for(e, M, 256);
+  k_tile_flags<<<gm, 256, 0, e.stream>>>(f.counts, f.boff, uint32_t(M), win, small, f.flag);
+  scan_excl<uint32_t, uint32_t>(f.flag, M, f.fidx, reinterpret_cast<uint32_t*>(f.scan_tmp), e.stream);
+  k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), f.tile_begin, e.ctr);
+  UC_CK(cudaMemsetAsync(&e.ctr->seg_count, 0, 8, e.stream));  // seg_count + cross_count reused as cross cursor
+  if (n > 0) {
+    const int grid = grid_for(e, n, 256);
+    if (nw == 1) k_scatter<1><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, f.pkeys, f.plink, ids_mode, e.ctr);
+    else k_scatter<2><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, f.pkeys, f.plink, ids_mode, e.ctr);
+    UC_CK(cudaGetLastError());
+  }
+  k_find_big<<<grid_for(e, M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, cap, f.big_list, f.big_size, nw);
+  cudaEventRecord(e.ev[2], e.stream);
+  if (st) {
+    st->l_used = uint32_t(l_used);
+    st->bucket_bits = bbits;
+    st->tile_capacity = cap;
+  }
+  return UC_OK;
+}
+
+template <int NW>
+static int run_tiles(Env& e, TileParams& tp, const Fused& f, uint32_t threads) {
+  const size_t smem = tile_bytes(NW, tp.cap, tp.tslots);
+  UC_CK(cudaFuncSetAttribute(k_tile<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  int occ = 0;
+  UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<NW>, int(threads), smem));
+  if (occ < 1) return e.fail(UC_EINTERNAL, "tile kernel does not fit an SM");
+  k_tile<NW><<<e.sm_count * occ, threads, smem, e.stream>>>(tp);
+  UC_CK(cudaGetLastError());
+  // oversized tiles: one CTA each in global scratch
+  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  const uint32_t nbig = e.h_ctr->nbig;
+  if (nbig) {
+    std::vector<unsigned long long> sz(nbig), off(nbig);
+    UC_CK(cudaMemcpy(sz.data(), f.big_size, nbig * 8, cudaMemcpyDeviceToHost));
+    unsigned long long tot = 0;
+    for (uint32_t i = 0; i < nbig; ++i) { off[i] = tot; tot += sz[i]; }
+    const size_t want = size_t(tot) + size_t(nbig) * 8 + 4096;
+    if (want > e.big_cap) {
+      if (e.big_buf) cudaFree(e.big_buf);
+      e.big_buf = nullptr;
+      e.big_cap = 0;
+      if (want > e.budget) return e.fail(UC_EBUDGET, "scratch for oversized buckets");
+      if (cudaMalloc(&e.big_buf, want) != cudaSuccess) {
+        cudaGetLastError();
+        e.big_buf = nullptr;
+        return e.fail(UC_ENOMEM, "scratch for oversized buckets");
+      }
+      e.big_cap = want;
+    }
+    unsigned long long* d_off = reinterpret_cast<unsigned long long*>(e.big_buf);
+    char* scratch = e.big_buf + ((size_t(nbig) * 8 + 255) & ~size_t(255));
+    UC_CK(cudaMemcpyAsync(d_off, off.data(), nbig * 8, cudaMemcpyHostToDevice, e.stream));
+    tp.big_list = f.big_list;
+    tp.big_scratch = scratch;
+    tp.big_off = d_off;
+    k_tile_big<NW><<<nbig, 1024, 0, e.stream>>>(tp);
+    UC_CK(cudaGetLastError());
+    UC_CK(cudaStreamSynchronize(e.stream));
+  }
+  return UC_OK;
+}
+
+int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed, uint32_t* succ,
+               uint32_t* pred) {
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
+  if (n >= 0xFFFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 32-bit ids");
+  const size_t mark = e.used;
+  Fused f{};
+  uint32_t cap, tslots, bbits;
+  int l_used;
+  uint64_t nn = n;
+  e.extra_need = 0;
+  int r = front(e, nullptr, 0, k, l, 1, d_keys, n, seed, f, nn, cap, tslots, nullptr, l_used, bbits);
+  if (r) return r;
+  TileParams tp{};
+  tp.pkeys = f.pkeys;
+  tp.plink = f.plink;
+  tp.tile_begin = f.tile_begin;
+  tp.ctr = e.ctr;
+  tp.k = k;
+  tp.cap = cap;
+  tp.tslots = tslots;
+  tp.mode = 0;
+  tp.succ = succ;
+  tp.pred = pred;
+  r = (k <= 31) ? run_tiles<1>(e, tp, f, 512) : run_tiles<2>(e, tp, f, 512);
+  if (r) return r;
+  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  e.used = mark;
+  return e.check_err(e.h_ctr);
+}
+
+// Weighted list ranking over `prev` by asynchronous pointer jumping.
+// Returns the number of entries left on cycles (in act[0..left)).
+static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t n, bool count_on_device,
+                      unsigned long long* X, uint32_t* act0, uint32_t* act1, uint32_t& left,
+                      uint32_t& rounds_used, uint32_t*& act_final) {
+  uint32_t* cnt = &e.ctr->active;
+  uint32_t* cnt2 = &e.ctr->active_next;
+  UC_CK(cudaMemsetAsync(cnt, 0, 8, e.stream));
+  const int grid = grid_for(e, n ? n : 1, 256);
+  k_rank_init<<<grid, 256, 0, e.stream>>>(prev, w, n, count_on_device ? e.ctr : nullptr, X, act0, cnt);
+  uint32_t* a = act0;
+  uint32_t* b = act1;
+  uint32_t maxr = 2;
+  for (uint64_t t = 1; t < n; t <<= 1) ++maxr;
+  uint32_t h = 0;
+  rounds_used = 0;
+  for (uint32_t r = 0; r < maxr + 2; ++r) {
+    UC_CK(cudaMemcpyAsync(&e.h_ctr->active, cnt, 4, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    h = e.h_ctr->active;
+    if (h == 0) break;
+    UC_CK(cudaMemsetAsync(cnt2, 0, 4, e.stream));
+    k_rank_round<<<grid_for(e, h, 256), 256, 0, e.stream>>>(X, a, cnt, b, cnt2);
+    UC_CK(cudaMemcpyAsync(cnt, cnt2, 4, cudaMemcpyDeviceToDevice, e.stream));
+    std::swap(a, b);
+    ++rounds_used;
+  }
+  UC_CK(cudaMemcpyAsync(&e.h_ctr->active, cnt, 4, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  left = e.h_ctr->active;
+  act_final = a;
+  return UC_OK;
+}
+
+int contract(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* pred, uint64_t n, int k,
+             int method, uint32_t* head, uint32_t* rank, uint64_t& ncyc) {
+  (void)method;
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  ncyc = 0;
+  if (n == 0) return UC_OK;
+  const size_t mark = e.used;
+  int r = e.reserve(e.used + n * (8 + 4 + 4 + 1) + (size_t(1) << 20));
+  if (r) return r;
+  unsigned long long* X = static_cast<unsigned long long*>(e.take(n * 8));
+  uint32_t* a0 = static_cast<uint32_t*>(e.take(n * 4));
+  uint32_t* a1 = static_cast<uint32_t*>(e.take(n * 4));
+  uint8_t* seen = static_cast<uint8_t*>(e.take(n));
+  unsigned long long* dcyc = static_cast<unsigned long long*>(e.take(8));
+  if (!dcyc) return e.fail(UC_EBUDGET, "arena overflow");
+  uint32_t left = 0, rounds = 0;
+  uint32_t* act = nullptr;
+  r = rank_lists(e, pred, nullptr, n, false, X, a0, a1, left, rounds, act);
+  if (r) return r;
+  k_head_rank<<<grid_for(e, n, 256), 256, 0, e.stream>>>(X, n, head, rank);
+  if (left) {
+    UC_CK(cudaMemsetAsync(seen, 0, n, e.stream));
+    UC_CK(cudaMemsetAsync(dcyc, 0, 8, e.stream));
+    if (k <= 31) k_vertex_cycles<1><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, head, rank, seen, dcyc);
+    else k_vertex_cycles<2><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, head, rank, seen, dcyc);
+    unsigned long long hc = 0;
+    UC_CK(cudaMemcpyAsync(&hc, dcyc, 8, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    ncyc = hc;
+  }
+  UC_CK(cudaStreamSynchronize(e.stream));
+  e.used = mark;
+  return UC_OK;
+}
+
+int emit(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* head, const uint32_t* rank,
+         uint64_t n, int k, char* out, uint64_t cap, uint64_t& out_bytes) {
+  (void)succ;
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  out_bytes = 0;
+  if (n == 0) return UC_OK;
+  const size_t mark = e.used;
+  int r = e.reserve(e.used + n * 16 + scan_tmp_elems(n) * 8 + (size_t(1) << 20));
+  if (r) return r;
+  uint32_t* cnt = static_cast<uint32_t*>(e.take(n * 4));
+  uint32_t* len = static_cast<uint32_t*>(e.take(n * 4));
+  unsigned long long* loff = static_cast<unsigned long long*>(e.take((n + 1) * 8));
+  unsigned long long* tmp = static_cast<unsigned long long*>(e.take(scan_tmp_elems(n) * 8));
+  if (!tmp) return e.fail(UC_EBUDGET, "arena overflow");
+  UC_CK(cudaMemsetAsync(cnt, 0, n * 4, e.stream));
+  const int grid = grid_for(e, n, 256);
+  k_count_members<<<grid, 256, 0, e.stream>>>(head, n, cnt);
+  k_line_len<<<grid, 256, 0, e.stream>>>(head, cnt, n, k, len);
+  scan_excl<uint32_t, unsigned long long>(len, n, loff, tmp, e.stream);
+  unsigned long long total = 0;
+  UC_CK(cudaMemcpyAsync(&total, loff + n, 8, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  out_bytes = total;
+  if (out) {
+    if (total > cap) return e.fail(UC_EINPUT, "output buffer too small");
+    if (k <= 31) k_spell<1><<<grid, 256, 0, e.stream>>>(d_keys, head, rank, cnt, loff, n, k, out);
+    else k_spell<2><<<grid, 256, 0, e.stream>>>(d_keys, head, rank, cnt, loff, n, k, out);
+    UC_CK(cudaGetLastError());
+    UC_CK(cudaStreamSynchronize(e.stream));
+  }
+  e.used = mark;
+  return UC_OK;
+}
+
+uint64_t output_bound(size_t text_bytes, int k) {
+  (void)k;
+  return uint64_t(text_bytes) + 64;
+}
+
+int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char* out, uint64_t cap,
+                   uint64_t& out_bytes, uc_stats* st) {
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
+  const int nw = (k <= 31) ? 1 : 2;
+  e.used = 0;
+  uint64_t n = 0, body = 0;
+  int r = parse_header(e, d_text, bytes, n, body);
+  if (r) return r;
+  if (n >= 0xFFFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 32-bit ids");
+  // Segment bounds.  Every open segment holds a P-only end or an S-only
+  // start, so there are at most 2 * cross + closed-free segments <= copies;
+  // its chars are k-1+m <= k per copy.
+  const uint64_t ncp = 2 * n + 1;
+  const uint64_t segchars = ncp * uint64_t(k) + 64;
+  e.extra_need = ncp * (8 + 4 + 4 + 4 + 4 + 4 + 4 + 4 + 4 + 8 + 8 + 1 + 4) + segchars +
+                 scan_tmp_elems(ncp) * 8 + 2 * (n + 1) * 4 + (size_t(8) << 20);
+  Fused f{};
+  uint32_t tcap, tslots, bbits;
+  int l_used;
+  r = front(e, d_text, bytes, k, l, 0, nullptr, 0, e.seed, f, n, tcap, tslots, st, l_used, bbits);
+  if (r) return r;
+  auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(c * 8)); };
+  auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(c * 4)); };
+  unsigned long long* seg_off = T64(ncp);
+  uint32_t* seg_len = T32(ncp);
+  uint32_t* seg_sx = T32(ncp);
+  uint32_t* seg_ex = T32(ncp);
+  uint32_t* start_seg = T32(n + 1);
+  uint32_t* end_seg = T32(n + 1);
+  char* segc = static_cast<char*>(e.take(segchars));
+  uint32_t* next = T32(ncp);
+  uint32_t* prev = T32(ncp);
+  uint32_t* wgt = T32(ncp);
+  uint32_t* act0 = T32(ncp);
+  uint32_t* act1 = T32(ncp);
+  uint32_t* llen = T32(ncp);
+  uint32_t* hlen = T32(ncp);
+  unsigned long long* X = T64(ncp);
+  unsigned long long* loff = T64(ncp + 1);
+  uint8_t* oncyc = static_cast<uint8_t*>(e.take(ncp));
+  unsigned long long* stmp = T64(scan_tmp_elems(ncp));
+  unsigned long long* dtotal = T64(1);
+  if (!dtotal) return e.fail(UC_EBUDGET, "arena overflow");
+
+  TileParams tp{};
+  tp.pkeys = f.pkeys;
+  tp.plink = f.plink;
+  tp.tile_begin = f.tile_begin;
+  tp.ctr = e.ctr;
+  tp.k = k;
+  tp.cap = tcap;
+  tp.tslots = tslots;
+  tp.mode = 1;
+  tp.out = out;
+  tp.out_cap = cap;
+  tp.segchars = segc;
+  tp.segchars_cap = segchars;
+  tp.seg_cap = uint32_t(std::min<uint64_t>(ncp, 0xFFFFFFFEull));
+  tp.seg_off = seg_off;
+  tp.seg_len = seg_len;
+  tp.seg_sx = seg_sx;
+  tp.seg_ex = seg_ex;
+  tp.start_seg = start_seg;
+  tp.end_seg = end_seg;
+  // seg_count served as nothing before; cross_count now holds the cross k-mers
+  UC_CK(cudaMemsetAsync(&e.ctr->seg_count, 0, 4, e.stream));
+  const uint32_t threads = e.tune.tile_threads ? e.tune.tile_threads : 512;
+  r = (nw == 1) ? run_tiles<1>(e, tp, f, threads) : run_tiles<2>(e, tp, f, threads);
+  if (r) return r;
+  cudaEventRecord(e.ev[3], e.stream);
+  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  if (e.h_ctr->err) return e.check_err(e.h_ctr);
+  const uint32_t S = e.h_ctr->seg_count;
+  const unsigned long long closed_bytes = e.h_ctr->out_cursor;
+  uint32_t rounds = 0, left = 0;
+  if (S) {
+    const int gs = grid_for(e, S, 256);
+    k_seg_link<<<gs, 256, 0, e.stream>>>(e.ctr, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k);
+    uint32_t* act = nullptr;
+    r = rank_lists(e, prev, wgt, S, true, X, act0, act1, left, rounds, act);
+    if (r) return r;
+    UC_CK(cudaMemsetAsync(oncyc, 0, S, e.stream));
+    if (left) k_mark_cycle<<<grid_for(e, left, 256), 256, 0, e.stream>>>(act, &e.ctr->active, oncyc);
+    k_chain_len<<<gs, 256, 0, e.stream>>>(e.ctr, X, next, wgt, oncyc, llen);
+    k_head_len<<<gs, 256, 0, e.stream>>>(e.ctr, prev, llen, hlen);
+    scan_excl<uint32_t, unsigned long long>(hlen, S, loff, stmp, e.stream, dtotal);
+    k_seg_copy<<<grid_for(e, uint64_t(S) * 32, 256), 256, 0, e.stream>>>(e.ctr, X, next, prev, wgt, oncyc, seg_off,
+                                                                          loff, segc, out, closed_bytes, k);
+    k_add_cursor<<<1, 1, 0, e.stream>>>(e.ctr, dtotal);
+    if (left) {
+      if (nw == 1) k_seg_cycles<1><<<1, 1, 0, e.stream>>>(e.ctr, act, left, oncyc, next, seg_len, seg_off, segc, out, cap, k);
+      else k_seg_cycles<2><<<1, 1, 0, e.stream>>>(e.ctr, act, left, oncyc, next, seg_len, seg_off, segc, out, cap, k);
+    }
+    UC_CK(cudaGetLastError());
+  }
+  cudaEventRecord(e.ev[4], e.stream);
+  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  if (e.h_ctr->err) return e.check_err(e.h_ctr);
+  out_bytes = e.h_ctr->out_cursor;
+  if (out_bytes > cap) return e.fail(UC_EINTERNAL, "output bound exceeded");
+  if (st) {
+    st->n_kmers = n;
+    st->n_copies = n + e.h_ctr->cross_count;
+    st->n_cross = e.h_ctr->cross_count;
+    st->n_tiles = e.h_ctr->ntiles;
+    st->n_big_tiles = e.h_ctr->nbig;
+    st->n_segments = S;
+    st->n_cycles = e.h_ctr->cycles;
+    st->out_bytes = out_bytes;
+    st->stitch_rounds = rounds;
+    float a = 0, b = 0, c = 0, d = 0;
+    cudaEventElapsedTime(&a, e.ev[0], e.ev[1]);
+    cudaEventElapsedTime(&b, e.ev[1], e.ev[2]);
+    cudaEventElapsedTime(&c, e.ev[2], e.ev[3]);
+    cudaEventElapsedTime(&d, e.ev[3], e.ev[4]);
+    st->ms_pack = a;
+    st->ms_bucket = b;
+    st->ms_tiles = c;
+    st->ms_stitch = d;
+    st->ms_total = a + b + c + d;
+  }
+  e.used = 0;
+  return UC_OK;
+}
+
+}  // namespace uc

@@ -1,0 +1,55 @@
+// uc_pipeline.h — host-side pipeline entry points used by the C ABI.
+#pragma once
+#include <cstdint>
+#include <string>
+
+#include <cuda_runtime.h>
+
+#include "../../include/uc.h"
+#include "uc_kernels.cuh"
+
+namespace uc {
+
+// Per-context state: stream, device scratch arena, counters, tuning.
+struct Env {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 148;
+  size_t budget = 0;
+  char* arena = nullptr;
+  size_t cap = 0;
+  size_t used = 0;
+  size_t extra_need = 0;
+  Counters* ctr = nullptr;    // device
+  Counters* h_ctr = nullptr;  // pinned host mirror
+  cudaEvent_t ev[8] = {};
+  uc_tuning tune{};
+  uint64_t seed = 0x00C0FFEE5EEDull;
+  int smem_optin = 232448;     // max dynamic shared memory per block
+  char* big_buf = nullptr;     // scratch of oversized tiles (grow only)
+  size_t big_cap = 0;
+  std::string err;
+
+  int fail(int code, const std::string& msg);
+  void* take(size_t bytes);
+  // Make the arena hold `bytes`; only valid while nothing is taken (used == 0).
+  int reserve(size_t bytes);
+  int check_err(const Counters* h);
+};
+
+int parse_header(Env& e, const char* d_text, size_t bytes, uint64_t& n, uint64_t& body);
+int pack(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t& n_out);
+int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed,
+               const uint32_t* d_table, uint32_t* l1, uint32_t* l2);
+int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed,
+               uint32_t* succ, uint32_t* pred);
+int contract(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* pred, uint64_t n,
+             int k, int method, uint32_t* head, uint32_t* rank, uint64_t& ncyc);
+int emit(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* head,
+         const uint32_t* rank, uint64_t n, int k, char* out, uint64_t cap, uint64_t& out_bytes);
+int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char* out, uint64_t cap,
+                   uint64_t& out_bytes, uc_stats* st);
+uint64_t output_bound(size_t text_bytes, int k);
+
+}  // namespace uc
