@@ -56,9 +56,11 @@ __host__ __device__ inline size_t tile_bytes(int nw, uint32_t cap, uint32_t tslo
   return size_t(cap) * (8u * nw + 4u + 16u) + size_t(tslots) * 4u;
 }
 
+// Smallest power of two >= x, for x <= 2^31 (callers bound x first); larger
+// x returns 2^31 after at most 31 doublings.
 __host__ __device__ inline uint32_t pow2_at_least(uint64_t x) {
   uint32_t p = 1;
-  while (p < x) p <<= 1;
+  for (int i = 0; i < 31 && p < x; ++i) p <<= 1;
   return p;
 }
 

@@ -51,9 +51,9 @@ __global__ void k_scan_down(const Tin* __restrict__ in, uint64_t n, Tout* __rest
     out[i] = pre;
     pre += v;
   }
-  if (total_out && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
-    *total_out = boff[blockIdx.x] + total;
+  if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) {
     out[n] = boff[blockIdx.x] + total;
+    if (total_out) *total_out = boff[blockIdx.x] + total;
   }
 }
 
@@ -259,6 +259,10 @@ __global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Co
   const uint32_t nt = ctr->ntiles;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     const uint64_t c = tile_begin[t + 1] - tile_begin[t];
+    if (tile_begin[t + 1] < tile_begin[t] || c > (1ull << 30)) {
+      atomicOr(&ctr->err, ERR_INTERNAL);
+      continue;
+    }
     if (c > cap) {
       const uint32_t i = atomicAdd(&ctr->nbig, 1u);
       big_list[i] = t;
@@ -466,7 +470,6 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW>& m, uint64_t
     const uint32_t cand = m.A[i] & CAND_NONE;
     const uint32_t s = (cand != CAND_NONE && m.B[cand] == 1u) ? cand : NONE;
     const uint32_t q = (m.B[i] == 1u) ? m.P[i] : NONE;
-    __syncwarp();
     m.A[i] = s;
     m.P[i] = q;
   }
@@ -795,25 +798,28 @@ __global__ void k_seg_cycles(Counters* ctr, const uint32_t* __restrict__ act, ui
     if (oncycle[s0] != 1) continue;
     // total distinct k-mers N and the circular char accessor
     uint64_t N = 0;
-    uint32_t s = s0;
+    uint32_t s = s0, steps = 0;
+    const uint32_t S = ctr->seg_count;
     do {
       N += seg_len[s] - 1u;
       oncycle[s] = 2;
       s = next[s];
-    } while (s != s0 && s != NONE);
-    if (s == NONE || N == 0) {
+    } while (s != s0 && s != NONE && ++steps <= S);
+    if (s != s0 || N == 0) {
       atomicOr(&ctr->err, ERR_INTERNAL);
       continue;
     }
     // char q of the circular string: segment chars after the first k
+    // (q < N and the cycle was walked above, so the loop ends within it)
     auto at = [&](uint64_t q) -> char {
       uint32_t t = s0;
-      for (;;) {
+      for (uint32_t guard = 0; guard <= S; ++guard) {
         const uint64_t m = seg_len[t] - 1u;
         if (q < m) return segchars[seg_off[t] + k + q];
         q -= m;
         t = next[t];
       }
+      return 'A';
     };
     // the k-mer ending at circular position q; find the smallest
     auto kmer_at = [&](uint64_t q) {
@@ -867,7 +873,7 @@ __global__ void k_head_rank(const unsigned long long* __restrict__ X, uint64_t n
 template <int NW>
 __global__ void k_vertex_cycles(const uint32_t* __restrict__ act, uint32_t na,
                                 const uint32_t* __restrict__ succ, const uint64_t* __restrict__ keys,
-                                uint32_t* __restrict__ head, uint32_t* __restrict__ rank,
+                                uint64_t n_all, uint32_t* __restrict__ head, uint32_t* __restrict__ rank,
                                 uint8_t* __restrict__ seen, unsigned long long* ncyc) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   for (uint32_t j = 0; j < na; ++j) {
@@ -875,17 +881,22 @@ __global__ void k_vertex_cycles(const uint32_t* __restrict__ act, uint32_t na,
     if (seen[v0]) continue;
     uint32_t best = v0;
     Key<NW> bk = ld_key<NW>(keys, v0);
-    for (uint32_t x = succ[v0]; x != v0 && x != NONE; x = succ[x]) {
+    uint64_t steps = 0;
+    uint32_t x = succ[v0];
+    for (; x != v0 && x != NONE && steps < n_all; x = succ[x], ++steps) {
       const Key<NW> xk = ld_key<NW>(keys, x);
       if (key_lt(xk, bk)) { bk = xk; best = x; }
     }
-    uint32_t r = 0, x = best;
+    if (x != v0) continue;  // not a cycle: left as ranked
+    uint32_t r = 0;
+    x = best;
+    steps = 0;
     do {
       head[x] = best;
       rank[x] = r++;
       seen[x] = 1;
       x = succ[x];
-    } while (x != best && x != NONE);
+    } while (x != best && x != NONE && ++steps < n_all);
     ++*ncyc;
   }
 }
@@ -1360,8 +1371,8 @@ int contract(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_
   if (left) {
     UC_CK(cudaMemsetAsync(seen, 0, n, e.stream));
     UC_CK(cudaMemsetAsync(dcyc, 0, 8, e.stream));
-    if (k <= 31) k_vertex_cycles<1><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, head, rank, seen, dcyc);
-    else k_vertex_cycles<2><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, head, rank, seen, dcyc);
+    if (k <= 31) k_vertex_cycles<1><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, n, head, rank, seen, dcyc);
+    else k_vertex_cycles<2><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, n, head, rank, seen, dcyc);
     unsigned long long hc = 0;
     UC_CK(cudaMemcpyAsync(&hc, dcyc, 8, cudaMemcpyDeviceToHost, e.stream));
     UC_CK(cudaStreamSynchronize(e.stream));
