@@ -50,7 +50,7 @@ typedef struct uc_job uc_job;
 typedef struct uc_stats {
     uint64_t n_kmers, n_copies, n_cross, n_tiles, n_big_tiles;
     uint64_t n_segments, n_unitigs, n_cycles, out_bytes;
-    uint32_t l_used, bucket_bits, tile_capacity, stitch_rounds;
+    uint32_t l_used, bucket_bits, tile_capacity, stitch_rounds, launches;
     float ms_pack, ms_bucket, ms_tiles, ms_stitch, ms_total;
 } uc_stats;
 

@@ -50,7 +50,7 @@ class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "n_kmers", "n_copies", "n_cross", "n_tiles", "n_big_tiles",
         "n_segments", "n_unitigs", "n_cycles", "out_bytes")] + \
-        [(n, ctypes.c_uint32) for n in ("l_used", "bucket_bits", "tile_capacity", "stitch_rounds")] + \
+        [(n, ctypes.c_uint32) for n in ("l_used", "bucket_bits", "tile_capacity", "stitch_rounds", "launches")] + \
         [(n, ctypes.c_float) for n in ("ms_pack", "ms_bucket", "ms_tiles", "ms_stitch", "ms_total")]
 
     def as_dict(self) -> dict:

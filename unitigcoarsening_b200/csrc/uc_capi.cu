@@ -150,7 +150,8 @@ uc_status uc_ctx_destroy(uc_ctx* c) {
   if (!c) return UC_OK;
   cudaSetDevice(c->env.device);
   if (c->env.stream) cudaStreamSynchronize(c->env.stream);
-  if (c->env.arena) cudaFree(c->env.arena);
+  for (auto& a : c->env.ar)
+    if (a.base) cudaFree(a.base);
   if (c->env.big_buf) cudaFree(c->env.big_buf);
   if (c->io_text) cudaFree(c->io_text);
   if (c->io_out) cudaFree(c->io_out);
@@ -217,10 +218,10 @@ uc_status uc_pack(uc_ctx* c, const char* d_text, size_t bytes, int k, uint64_t* 
   if (!c || !d_text || !n_out) return UC_EINPUT;
   uc_status s = set_device(c);
   if (s) return s;
-  c->env.used = 0;
+  c->env.reset();
   uint64_t n = 0;
   int r = uc::pack(c->env, d_text, bytes, k, d_keys, n);
-  c->env.used = 0;
+  c->env.reset();
   *n_out = n;
   return as_status(r);
 }
@@ -238,9 +239,9 @@ uc_status uc_find_edges(uc_ctx* c, const uint64_t* d_keys, uint64_t n, int k, in
   if (!c || (n && (!d_keys || !d_succ || !d_pred))) return UC_EINPUT;
   uc_status s = set_device(c);
   if (s) return s;
-  c->env.used = 0;
+  c->env.reset();
   const int r = uc::find_edges(c->env, d_keys, n, k, l, seed, d_succ, d_pred);
-  c->env.used = 0;
+  c->env.reset();
   return as_status(r);
 }
 
@@ -250,10 +251,10 @@ uc_status uc_contract(uc_ctx* c, const uint64_t* d_keys, const uint32_t* d_succ,
   if (method != UC_CONTRACT_POINTER_JUMP && method != UC_CONTRACT_HEC) return UC_EINPUT;
   uc_status s = set_device(c);
   if (s) return s;
-  c->env.used = 0;
+  c->env.reset();
   uint64_t cyc = 0;
   const int r = uc::contract(c->env, d_keys, d_succ, d_pred, n, k, method, d_head, d_rank, cyc);
-  c->env.used = 0;
+  c->env.reset();
   if (n_cycles) *n_cycles = cyc;
   return as_status(r);
 }
@@ -263,10 +264,10 @@ uc_status uc_emit(uc_ctx* c, const uint64_t* d_keys, const uint32_t* d_succ, con
   if (!c || !out_bytes || (n && (!d_keys || !d_head || !d_rank))) return UC_EINPUT;
   uc_status s = set_device(c);
   if (s) return s;
-  c->env.used = 0;
+  c->env.reset();
   uint64_t ob = 0;
   const int r = uc::emit(c->env, d_keys, d_succ, d_head, d_rank, n, k, d_out, cap, ob);
-  c->env.used = 0;
+  c->env.reset();
   *out_bytes = ob;
   return as_status(r);
 }
@@ -281,7 +282,7 @@ uc_status uc_compact_device(uc_ctx* c, const char* d_text, size_t bytes, int k, 
   uint64_t ob = 0;
   if (stats) std::memset(stats, 0, sizeof(*stats));
   const int r = uc::compact_device(c->env, d_text, bytes, k, l, d_out, cap, ob, stats);
-  c->env.used = 0;
+  c->env.reset();
   *out_bytes = ob;
   return as_status(r);
 }

@@ -95,26 +95,58 @@ __device__ __forceinline__ uint32_t base_code(uint32_t c) {
   return (c == 'C') ? 1u : (c == 'G') ? 2u : (c == 'T') ? 3u : 0u;
 }
 
-// One warp packs 32 consecutive lines; lane j handles chars j and j+32 of a
-// line, so each line is one coalesced 32-byte read, and the 2-bit codes are
-// gathered with warp OR-reductions.  Lane i keeps line i's key.
-template <int NW>
-__global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, uint64_t body,
-                                              uint64_t end, const unsigned long long* __restrict__ starts,
+// A block packs 256 consecutive lines per pass.  It first stages the text
+// span of those lines in shared memory with 16-byte loads issued by every
+// thread (so the block has the whole span in flight at once), then each warp
+// packs its 32 lines from shared memory: lane j takes chars j and j+32 of a
+// line and the 2-bit codes are gathered with warp OR-reductions; lane i keeps
+// line i's key.  With FUSE the prefix/suffix minimizer buckets of every key
+// are computed and counted in the same pass (lmin_buckets.h:299-318).
+constexpr int PACK_LINES = 256;
+constexpr int PACK_BUF = 20480;
+
+template <int NW, bool FUSE>
+__global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, uint64_t tbytes,
+                                              uint64_t body, uint64_t end,
+                                              const unsigned long long* __restrict__ starts,
                                               uint32_t stride, uint64_t n, int k,
-                                              uint64_t* __restrict__ keys, uint32_t* err) {
-  const int lane = threadIdx.x & 31;
-  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+                                              uint64_t* __restrict__ keys, uint32_t* err, int l,
+                                              uint64_t seed, uint32_t bbits, uint32_t* __restrict__ b1,
+                                              uint32_t* __restrict__ b2, uint32_t* __restrict__ counts) {
+  __shared__ __align__(16) uint8_t buf[PACK_BUF];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const uint32_t sh = 2u * uint32_t(lane & 15);
+  const uintptr_t tb = reinterpret_cast<uintptr_t>(text);
   uint32_t bad = 0;
-  for (uint64_t base = warp * 32; base < n; base += nwarps * 32) {
-    const int cnt = int(n - base < 32 ? n - base : 32);
+  for (uint64_t b0 = uint64_t(blockIdx.x) * PACK_LINES; b0 < n; b0 += uint64_t(gridDim.x) * PACK_LINES) {
+    const uint32_t cnt = uint32_t((n - b0) < PACK_LINES ? (n - b0) : PACK_LINES);
+    const uint64_t s0 = starts ? uint64_t(starts[b0]) : body + b0 * stride;
+    const uint64_t s1 = (b0 + cnt < n) ? (starts ? uint64_t(starts[b0 + cnt]) : body + (b0 + cnt) * stride) : end;
+    const uintptr_t A0 = (tb + s0) & ~uintptr_t(15);
+    const uint64_t span = (tb + s1) - A0;
+    const bool staged = span + 16 <= PACK_BUF;
+    if (staged) {
+      const uint32_t nch = uint32_t((span + 15) / 16);
+      for (uint32_t c = threadIdx.x; c < nch; c += blockDim.x) {
+        const uintptr_t a = A0 + 16u * c;
+        if (a >= tb && a + 16 <= tb + tbytes) {
+          *reinterpret_cast<uint4*>(buf + 16u * c) = __ldg(reinterpret_cast<const uint4*>(a));
+        } else {
+          for (int q = 0; q < 16; ++q) {
+            const uintptr_t x = a + q;
+            buf[16u * c + q] = (x >= tb && x < tb + tbytes) ? *reinterpret_cast<const uint8_t*>(x) : uint8_t('\n');
+          }
+        }
+      }
+    }
+    __syncthreads();
+    const int wl0 = wid * 32;
+    const int wcnt = int(cnt) - wl0 < 0 ? 0 : (int(cnt) - wl0 > 32 ? 32 : int(cnt) - wl0);
     Key<NW> mine;
 #pragma unroll
     for (int w = 0; w < NW; ++w) mine.w[w] = 0;
-    for (int j = 0; j < cnt; ++j) {
-      const uint64_t line = base + j;
+    for (int j = 0; j < wcnt; ++j) {
+      const uint64_t line = b0 + wl0 + j;
       const uint64_t s = starts ? uint64_t(starts[line]) : body + line * stride;
       uint32_t v[NW];
       bool lbad = false;
@@ -122,7 +154,9 @@ __global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, 
       for (int h = 0; h < NW; ++h) {
         const int ci = lane + 32 * h;
         const uint64_t pos = s + ci;
-        const uint32_t c = (pos < end) ? uint32_t(__ldg(text + pos)) : uint32_t('\n');
+        uint32_t c;
+        if (staged) c = (pos < s1) ? uint32_t(buf[(tb + pos) - A0]) : uint32_t('\n');
+        else c = (pos < end) ? uint32_t(__ldg(text + pos)) : uint32_t('\n');
         if (ci < k) {
           lbad |= (c == '\n') || (pos >= end);
           v[h] = base_code(c);
@@ -141,7 +175,21 @@ __global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, 
         if (lane == j) mine.w[h] = uint64_t(lo) | (uint64_t(hi) << 32);
       }
     }
-    if (lane < cnt) st_key<NW>(keys, base + lane, mine);
+    if (lane < wcnt) {
+      const uint64_t i = b0 + wl0 + lane;
+      st_key<NW>(keys, i, mine);
+      if constexpr (FUSE) {
+        uint32_t a, b;
+        lmins<NW>(mine, k, l, seed, nullptr, a, b);
+        a = bucket_of(a, bbits);
+        b = bucket_of(b, bbits);
+        b1[i] = a;
+        b2[i] = b;
+        atomicAdd(counts + a, 1u);
+        if (a != b) atomicAdd(counts + b, 1u);
+      }
+    }
+    __syncthreads();
   }
   if (bad && lane == 0) atomicOr(err, starts ? ERR_LINE : ERR_LAYOUT);
 }
@@ -944,9 +992,9 @@ static int grid_for(const Env& e, uint64_t work, int block) {
   return int(std::max<uint64_t>(1, std::min(want, cap)));
 }
 
-#define UC_CK(call)                                                            \
-  do {                                                                         \
-    cudaError_t _e = (call);                                                   \
+#define UC_CK(call)                                                                                  \
+  do {                                                                                               \
+    cudaError_t _e = (call);                                                                         \
     if (_e != cudaSuccess) return e.fail(UC_ECUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
@@ -955,30 +1003,35 @@ int Env::fail(int code, const std::string& msg) {
   return code;
 }
 
-void* Env::take(size_t bytes) {
-  const size_t a = (used + 255) & ~size_t(255);
-  if (a + bytes > cap) return nullptr;
-  used = a + bytes;
-  return arena + a;
+void* Env::take(int w, size_t bytes) {
+  Arena& a = ar[w];
+  const size_t o = (a.used + 255) & ~size_t(255);
+  if (o + bytes > a.cap) return nullptr;
+  a.used = o + bytes;
+  return a.base + o;
 }
 
-int Env::reserve(size_t bytes) {
-  bytes = (bytes + (size_t(64) << 20));
-  if (bytes <= cap) return UC_OK;
-  if (bytes > budget) return fail(UC_EBUDGET, "job needs " + std::to_string(bytes >> 20) + " MiB, budget " +
-                                                  std::to_string(budget >> 20) + " MiB");
-  if (arena) {
+int Env::reserve(int w, size_t bytes) {
+  Arena& a = ar[w];
+  bytes += size_t(16) << 20;
+  if (bytes <= a.cap) return UC_OK;
+  if (a.used) return fail(UC_EINTERNAL, "arena grown while in use");
+  const size_t other = ar[1 - w].cap;
+  if (bytes + other > budget)
+    return fail(UC_EBUDGET, "job needs " + std::to_string((bytes + other) >> 20) + " MiB of scratch, budget " +
+                                std::to_string(budget >> 20) + " MiB");
+  if (a.base) {
     cudaStreamSynchronize(stream);
-    cudaFree(arena);
-    arena = nullptr;
-    cap = 0;
+    cudaFree(a.base);
+    a.base = nullptr;
+    a.cap = 0;
   }
-  if (cudaMalloc(&arena, bytes) != cudaSuccess) {
+  if (cudaMalloc(&a.base, bytes) != cudaSuccess) {
     cudaGetLastError();
-    arena = nullptr;
+    a.base = nullptr;
     return fail(UC_ENOMEM, "cudaMalloc of " + std::to_string(bytes >> 20) + " MiB failed");
   }
-  cap = bytes;
+  a.cap = bytes;
   return UC_OK;
 }
 
@@ -992,6 +1045,13 @@ int Env::check_err(const Counters* h) {
   return fail(UC_EINTERNAL, "internal invariant failed (flags " + std::to_string(f) + ")");
 }
 
+int Env::read_ctr() {
+  Env& e = *this;
+  UC_CK(cudaMemcpyAsync(h_ctr, ctr, sizeof(Counters), cudaMemcpyDeviceToHost, stream));
+  UC_CK(cudaStreamSynchronize(stream));
+  return UC_OK;
+}
+
 // Parse the count line: reads the first bytes back to the host.
 int parse_header(Env& e, const char* d_text, size_t bytes, uint64_t& n, uint64_t& body) {
   std::vector<char> h;
@@ -1003,7 +1063,10 @@ int parse_header(Env& e, const char* d_text, size_t bytes, uint64_t& n, uint64_t
     size_t p = 0;
     while (p < want && (h[p] == ' ' || h[p] == '\t' || h[p] == '\r')) ++p;
     if (p >= want || h[p] < '0' || h[p] > '9') {
-      if (want < bytes && p >= want) { want = std::min(bytes, want * 4); continue; }
+      if (want < bytes && p >= want) {
+        want = std::min(bytes, want * 4);
+        continue;
+      }
       return e.fail(UC_EINPUT, "missing k-mer count header");
     }
     uint64_t v = 0;
@@ -1013,17 +1076,14 @@ int parse_header(Env& e, const char* d_text, size_t bytes, uint64_t& n, uint64_t
       ++p;
     }
     while (p < want && h[p] != '\n') ++p;
-    if (p >= want && want < bytes) { want = std::min(bytes, want * 4); continue; }
+    if (p >= want && want < bytes) {
+      want = std::min(bytes, want * 4);
+      continue;
+    }
     n = v;
     body = (p < want) ? p + 1 : want;
     return UC_OK;
   }
-}
-
-// Scratch of the general-layout line index.
-static size_t line_index_bytes(size_t bytes, uint64_t n) {
-  const uint64_t nchunks = bytes / (1 << 16) + 2;
-  return nchunks * 4 + (nchunks + 1) * 8 + scan_tmp_elems(nchunks) * 8 + (n + 1) * 8 + 8 * 256;
 }
 
 // End of the k-mer lines: trailing '\n' / '\r' bytes are not a line.
@@ -1042,7 +1102,38 @@ static int text_end(Env& e, const char* d_text, size_t bytes, uint64_t body, uin
   return UC_OK;
 }
 
-int pack(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t& n_out) {
+static size_t line_index_bytes(size_t bytes, uint64_t n) {
+  const uint64_t nchunks = bytes / (1 << 16) + 2;
+  return nchunks * 4 + (nchunks + 1) * 8 + scan_tmp_elems(nchunks) * 8 + (n + 1) * 8 + 8 * 256;
+}
+
+struct FuseArgs {
+  int l = 0;
+  uint64_t seed = 0;
+  uint32_t bbits = 0;
+  uint32_t *b1 = nullptr, *b2 = nullptr, *counts = nullptr;
+  uint64_t M = 0;
+};
+
+template <int NW>
+static void launch_pack(Env& e, const uint8_t* text, size_t bytes, uint64_t body, uint64_t end,
+                        const unsigned long long* starts, uint32_t stride, uint64_t n, int k, uint64_t* keys,
+                        const FuseArgs* fz) {
+  const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>((n + PACK_LINES - 1) / PACK_LINES,
+                                                                 uint64_t(e.sm_count) * 8)));
+  ++e.launches;
+  if (fz)
+    k_pack<NW, true><<<grid, 256, 0, e.stream>>>(text, bytes, body, end, starts, stride, n, k, keys, &e.ctr->err,
+                                                 fz->l, fz->seed, fz->bbits, fz->b1, fz->b2, fz->counts);
+  else
+    k_pack<NW, false><<<grid, 256, 0, e.stream>>>(text, bytes, body, end, starts, stride, n, k, keys, &e.ctr->err,
+                                                  0, 0, 0, nullptr, nullptr, nullptr);
+}
+
+// Text -> keys (and, with fz, minimizer buckets + counts).  The general line
+// layout uses the back arena for its line index; it must be empty.
+static int pack_impl(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t& n_out,
+                     const FuseArgs* fz) {
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
   uint64_t n = 0, body = 0, end = 0;
   int st = parse_header(e, d_text, bytes, n, body);
@@ -1051,7 +1142,7 @@ int pack(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint
   if (st) return st;
   n_out = n;
   const uint8_t* text = reinterpret_cast<const uint8_t*>(d_text);
-  UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+  UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
   if (n == 0) {
     if (end > body) return e.fail(UC_EINPUT, "header count differs from the number of lines");
     return UC_OK;
@@ -1059,51 +1150,56 @@ int pack(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint
   const int nw = (k <= 31) ? 1 : 2;
   const uint32_t stride = uint32_t(k) + 1;
   bool fixed = (end - body) == n * stride - 1;
-  const int block = 256;
-  const int grid = grid_for(e, (n + 7) / 8 * 32, block);
   if (fixed) {
-    if (nw == 1) k_pack<1><<<grid, block, 0, e.stream>>>(text, body, end, nullptr, stride, n, k, d_keys, &e.ctr->err);
-    else k_pack<2><<<grid, block, 0, e.stream>>>(text, body, end, nullptr, stride, n, k, d_keys, &e.ctr->err);
+    if (nw == 1) launch_pack<1>(e, text, bytes, body, end, nullptr, stride, n, k, d_keys, fz);
+    else launch_pack<2>(e, text, bytes, body, end, nullptr, stride, n, k, d_keys, fz);
     UC_CK(cudaGetLastError());
-    UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
-    UC_CK(cudaStreamSynchronize(e.stream));
+    st = e.read_ctr();
+    if (st) return st;
     if (e.h_ctr->err & ERR_LAYOUT) {
       fixed = false;
-      UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+      UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
+      if (fz) UC_CK(cudaMemsetAsync(fz->counts, 0, fz->M * 4, e.stream));
     } else if (e.h_ctr->err) {
       return e.check_err(e.h_ctr);
     }
   }
   if (!fixed) {
-    // general layout: index the line starts
     const uint32_t chunk = 1 << 16;
     const uint64_t nchunks = std::max<uint64_t>(1, (end - body + chunk - 1) / chunk);
-    if (e.used == 0) {
-      const int r = e.reserve(line_index_bytes(bytes, n));
-      if (r) return r;
-    }
-    const size_t mark = e.used;
-    uint32_t* cnt = static_cast<uint32_t*>(e.take(nchunks * 4));
-    unsigned long long* off = static_cast<unsigned long long*>(e.take((nchunks + 1) * 8));
-    unsigned long long* tmp = static_cast<unsigned long long*>(e.take(scan_tmp_elems(nchunks) * 8));
-    unsigned long long* starts = static_cast<unsigned long long*>(e.take((n + 1) * 8));
+    st = e.reserve(1, line_index_bytes(bytes, n));
+    if (st) return st;
+    uint32_t* cnt = static_cast<uint32_t*>(e.take(1, nchunks * 4));
+    unsigned long long* off = static_cast<unsigned long long*>(e.take(1, (nchunks + 1) * 8));
+    unsigned long long* tmp = static_cast<unsigned long long*>(e.take(1, scan_tmp_elems(nchunks) * 8));
+    unsigned long long* starts = static_cast<unsigned long long*>(e.take(1, (n + 1) * 8));
     if (!cnt || !off || !tmp || !starts) return e.fail(UC_EBUDGET, "scratch for the line index");
+    ++e.launches;
     k_count_nl<<<unsigned(nchunks), 256, 0, e.stream>>>(text, body, end, cnt, chunk);
+    e.launches += 2 * 3;
     scan_excl<uint32_t, unsigned long long>(cnt, nchunks, off, tmp, e.stream);
     unsigned long long lines_m1 = 0;
     UC_CK(cudaMemcpyAsync(&lines_m1, off + nchunks, 8, cudaMemcpyDeviceToHost, e.stream));
     UC_CK(cudaStreamSynchronize(e.stream));
     if (lines_m1 + 1 != n) return e.fail(UC_EINPUT, "header count differs from the number of lines");
+    ++e.launches;
     k_write_starts<<<unsigned(nchunks), 256, 0, e.stream>>>(text, body, end, off, chunk, starts, n);
-    if (nw == 1) k_pack<1><<<grid, block, 0, e.stream>>>(text, body, end, starts, stride, n, k, d_keys, &e.ctr->err);
-    else k_pack<2><<<grid, block, 0, e.stream>>>(text, body, end, starts, stride, n, k, d_keys, &e.ctr->err);
+    if (nw == 1) launch_pack<1>(e, text, bytes, body, end, starts, stride, n, k, d_keys, fz);
+    else launch_pack<2>(e, text, bytes, body, end, starts, stride, n, k, d_keys, fz);
     UC_CK(cudaGetLastError());
-    UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
-    UC_CK(cudaStreamSynchronize(e.stream));
-    e.used = mark;
+    st = e.read_ctr();
+    e.ar[1].used = 0;
+    if (st) return st;
     if (e.h_ctr->err) return e.check_err(e.h_ctr);
   }
   return UC_OK;
+}
+
+int pack(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t& n_out) {
+  e.reset();
+  const int r = pack_impl(e, d_text, bytes, k, d_keys, n_out, nullptr);
+  e.reset();
+  return r;
 }
 
 int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed,
@@ -1112,153 +1208,148 @@ int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
   if (n == 0) return UC_OK;
   const int grid = grid_for(e, n, 256);
+  ++e.launches;
   if (k <= 31) k_lmin<1><<<grid, 256, 0, e.stream>>>(d_keys, n, k, l, seed, d_table, l1, l2);
   else k_lmin<2><<<grid, 256, 0, e.stream>>>(d_keys, n, k, l, seed, d_table, l1, l2);
   UC_CK(cudaGetLastError());
   return UC_OK;
 }
 
-// Bucket plan for n k-mers: bucket bits and the minimizer length actually used.
-void plan_buckets(const Env& e, uint64_t n, int k, int l, uint32_t& bbits, int& l_used, uint32_t& cap,
-                  uint32_t& win, uint32_t& small) {
-  cap = e.tune.tile_capacity ? e.tune.tile_capacity : 4096;
-  // the tile (copies + hash slots) must fit one block's shared memory
+// Bucket plan for n k-mers.
+struct Plan {
+  uint32_t bbits, cap, win, small, tslots;
+  int l_used;
+  uint64_t M;
+};
+
+static Plan plan_buckets(const Env& e, uint64_t n, int k, int l) {
+  Plan P{};
   const int nw = (k <= 31) ? 1 : 2;
+  uint32_t cap = e.tune.tile_capacity ? e.tune.tile_capacity : 4096;
   while (cap > 256 && tile_bytes(nw, cap, pow2_at_least(2ull * cap)) > size_t(e.smem_optin)) cap -= 256;
   const uint64_t copies = n + n / 8 + 1;
+  uint32_t bbits = 0;
   if (e.tune.bucket_bits) {
     bbits = e.tune.bucket_bits;
   } else {
-    // ~cap/8 copies per bucket on average
-    bbits = 0;
-    while ((copies >> bbits) > cap / 8 && bbits < 24) ++bbits;
+    while ((copies >> bbits) > cap / 8 && bbits < 24) ++bbits;  // ~cap/8 copies per bucket
   }
   // enough l-mers that each bucket gathers several of them
-  int lmin = int((bbits + 2 + 1) / 2);
-  l_used = std::max(l, lmin);
-  l_used = std::min(l_used, std::min(16, k - 1));
-  win = cap - cap / 4;
-  small = cap / 4;
+  const int lmin = int((bbits + 2 + 1) / 2);
+  int lu = std::max(l, lmin);
+  lu = std::min(lu, std::min(16, k - 1));
+  uint32_t ts = pow2_at_least(uint64_t(cap) * std::max<uint32_t>(200, e.tune.load_factor_pct) / 100);
+  if (ts < 2 * cap) ts = pow2_at_least(2ull * cap);
+  while (ts > pow2_at_least(2ull * cap) && tile_bytes(nw, cap, ts) > size_t(e.smem_optin)) ts >>= 1;
+  P.bbits = bbits;
+  P.cap = cap;
+  P.win = cap - cap / 4;
+  P.small = cap / 4;
+  P.tslots = ts;
+  P.l_used = lu;
+  P.M = 1ull << bbits;
+  return P;
 }
 
-struct Fused {
+struct Front {
   uint64_t* keys;
   uint32_t *b1, *b2, *counts;
   unsigned long long *boff, *cursor, *tile_begin, *scan_tmp;
   uint32_t *flag, *fidx, *big_list;
   unsigned long long* big_size;
-  uint64_t* pkeys;
-  uint32_t* plink;
 };
 
-// Shared front half: pack, minimizers, counts, scan, tile plan, scatter.
-static int front(Env& e, const char* d_text, size_t bytes, int k, int l, int ids_mode,
-                 const uint64_t* given_keys, uint64_t given_n, uint64_t seed, Fused& f,
-                 uint64_t& n, uint32_t& cap, uint32_t& tslots, uc_stats* st, int& l_used,
-                 uint32_t& bbits) {
-  const int nw = (k <= 31) ? 1 : 2;
-  if (given_keys) {
-    n = given_n;
-  } else {
-    uint64_t body = 0;
-    int r = parse_header(e, d_text, bytes, n, body);
-    if (r) return r;
-  }
-  uint32_t win, small;
-  plan_buckets(e, n, k, l, bbits, l_used, cap, win, small);
-  const uint64_t M = 1ull << bbits;
-  tslots = pow2_at_least(uint64_t(cap) * std::max<uint32_t>(200, e.tune.load_factor_pct) / 100);
-  if (tslots < 2 * cap) tslots = pow2_at_least(2ull * cap);
-  while (tslots > pow2_at_least(2ull * cap) && tile_bytes(nw, cap, tslots) > size_t(e.smem_optin)) tslots >>= 1;
-  // allocations (upper bounds from n)
-  const uint64_t ncp = 2 * n + 1;
+static size_t front_bytes(uint64_t n, int nw, uint64_t M, bool own_keys) {
   size_t need = 0;
   auto add = [&](size_t b) { need += (b + 255) & ~size_t(255); };
-  if (!given_keys) {
-    add(n * 8 * nw);
-    add(line_index_bytes(bytes, n));
-  }
+  if (own_keys) add(n * 8 * nw);
   add(n * 4); add(n * 4); add(M * 4); add((M + 1) * 8); add(M * 8); add((M + 2) * 8);
   add(scan_tmp_elems(M) * 8); add(M * 4); add((M + 1) * 4); add(M * 4); add(M * 8);
-  add(ncp * 8 * nw); add(ncp * 4);
-  int r = e.reserve(e.used + need + e.extra_need);
-  if (r) return r;
-  f.keys = given_keys ? const_cast<uint64_t*>(given_keys) : static_cast<uint64_t*>(e.take(n * 8 * nw));
-  f.b1 = static_cast<uint32_t*>(e.take(n * 4));
-  f.b2 = static_cast<uint32_t*>(e.take(n * 4));
-  f.counts = static_cast<uint32_t*>(e.take(M * 4));
-  f.boff = static_cast<unsigned long long*>(e.take((M + 1) * 8));
-  f.cursor = static_cast<unsigned long long*>(e.take(M * 8));
-  f.tile_begin = static_cast<unsigned long long*>(e.take((M + 2) * 8));
-  f.scan_tmp = static_cast<unsigned long long*>(e.take(scan_tmp_elems(M) * 8));
-  f.flag = static_cast<uint32_t*>(e.take(M * 4));
-  f.fidx = static_cast<uint32_t*>(e.take((M + 1) * 4));
-  f.big_list = static_cast<uint32_t*>(e.take(M * 4));
-  f.big_size = static_cast<unsigned long long*>(e.take(M * 8));
-  f.pkeys = static_cast<uint64_t*>(e.take(ncp * 8 * nw));
-  f.plink = static_cast<uint32_t*>(e.take(ncp * 4));
-  if (!f.plink) return e.fail(UC_EBUDGET, "arena overflow");
-  if (!given_keys) {
-    uint64_t n2 = 0;
-    cudaEventRecord(e.ev[0], e.stream);
-    r = pack(e, d_text, bytes, k, f.keys, n2);
-    if (r) return r;
-  } else {
-    UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
-    cudaEventRecord(e.ev[0], e.stream);
-  }
-  cudaEventRecord(e.ev[1], e.stream);
-  UC_CK(cudaMemsetAsync(f.counts, 0, M * 4, e.stream));
-  if (n > 0) {
-    const int grid = grid_for(e, n, 256);
-    if (nw == 1) k_lmin_count<1><<<grid, 256, 0, e.stream>>>(f.keys, n, k, l_used, seed, bbits, f.b1, f.b2, f.counts);
-    else k_lmin_count<2><<<grid, 256, 0, e.stream>>>(f.keys, n, k, l_used, seed, bbits, f.b1, f.b2, f.counts);
-    UC_CK(cudaGetLastError());
-  }
+  return need;
+}
+
+static int take_front(Env& e, uint64_t n, int nw, uint64_t M, bool own_keys, Front& f) {
+  f.keys = own_keys ? static_cast<uint64_t*>(e.take(0, n * 8 * nw)) : nullptr;
+  f.b1 = static_cast<uint32_t*>(e.take(0, n * 4));
+  f.b2 = static_cast<uint32_t*>(e.take(0, n * 4));
+  f.counts = static_cast<uint32_t*>(e.take(0, M * 4));
+  f.boff = static_cast<unsigned long long*>(e.take(0, (M + 1) * 8));
+  f.cursor = static_cast<unsigned long long*>(e.take(0, M * 8));
+  f.tile_begin = static_cast<unsigned long long*>(e.take(0, (M + 2) * 8));
+  f.scan_tmp = static_cast<unsigned long long*>(e.take(0, scan_tmp_elems(M) * 8));
+  f.flag = static_cast<uint32_t*>(e.take(0, M * 4));
+  f.fidx = static_cast<uint32_t*>(e.take(0, (M + 1) * 4));
+  f.big_list = static_cast<uint32_t*>(e.take(0, M * 4));
+  f.big_size = static_cast<unsigned long long*>(e.take(0, M * 8));
+  if (!f.big_size) return e.fail(UC_EBUDGET, "front arena overflow");
+  return UC_OK;
+}
+
+// counts -> bucket offsets; returns the total number of copies (host sync).
+static int bucket_offsets(Env& e, const Front& f, uint64_t M, uint64_t& copies) {
+  e.launches += 6;
   scan_excl<uint32_t, unsigned long long>(f.counts, M, f.boff, f.scan_tmp, e.stream);
+  unsigned long long tot = 0;
+  UC_CK(cudaMemcpyAsync(&tot, f.boff + M, 8, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  copies = tot;
+  return UC_OK;
+}
+
+// tile plan + scatter of every k-mer into its bucket(s).
+static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, int nw, int ids_mode,
+                            uint64_t* pkeys, uint32_t* plink) {
+  const uint64_t M = P.M;
   UC_CK(cudaMemcpyAsync(f.cursor, f.boff, M * 8, cudaMemcpyDeviceToDevice, e.stream));
   const int gm = grid_for(e, M, 256);
-  k_tile_flags<<<gm, 256, 0, e.stream>>>(f.counts, f.boff, uint32_t(M), win, small, f.flag);
+  e.launches += 2 + 6;
+  k_tile_flags<<<gm, 256, 0, e.stream>>>(f.counts, f.boff, uint32_t(M), P.win, P.small, f.flag);
   scan_excl<uint32_t, uint32_t>(f.flag, M, f.fidx, reinterpret_cast<uint32_t*>(f.scan_tmp), e.stream);
   k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), f.tile_begin, e.ctr);
-  UC_CK(cudaMemsetAsync(&e.ctr->seg_count, 0, 8, e.stream));  // seg_count + cross_count reused as cross cursor
+  UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
   if (n > 0) {
     const int grid = grid_for(e, n, 256);
-    if (nw == 1) k_scatter<1><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, f.pkeys, f.plink, ids_mode, e.ctr);
-    else k_scatter<2><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, f.pkeys, f.plink, ids_mode, e.ctr);
+    ++e.launches;
+    if (nw == 1) k_scatter<1><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, pkeys, plink, ids_mode, e.ctr);
+    else k_scatter<2><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, pkeys, plink, ids_mode, e.ctr);
     UC_CK(cudaGetLastError());
   }
-  k_find_big<<<grid_for(e, M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, cap, f.big_list, f.big_size, nw);
-  cudaEventRecord(e.ev[2], e.stream);
-  if (st) {
-    st->l_used = uint32_t(l_used);
-    st->bucket_bits = bbits;
-    st->tile_capacity = cap;
-  }
+  ++e.launches;
+  k_find_big<<<grid_for(e, M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, P.cap, f.big_list, f.big_size, nw);
+  UC_CK(cudaGetLastError());
   return UC_OK;
 }
 
 template <int NW>
-static int run_tiles(Env& e, TileParams& tp, const Fused& f, uint32_t threads) {
+static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
   const size_t smem = tile_bytes(NW, tp.cap, tp.tslots);
   UC_CK(cudaFuncSetAttribute(k_tile<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   int occ = 0;
   UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<NW>, int(threads), smem));
   if (occ < 1) return e.fail(UC_EINTERNAL, "tile kernel does not fit an SM");
+  ++e.launches;
   k_tile<NW><<<e.sm_count * occ, threads, smem, e.stream>>>(tp);
   UC_CK(cudaGetLastError());
   // oversized tiles: one CTA each in global scratch
-  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
-  UC_CK(cudaStreamSynchronize(e.stream));
+  int st = e.read_ctr();
+  if (st) return st;
+  if (e.h_ctr->err) return e.check_err(e.h_ctr);
   const uint32_t nbig = e.h_ctr->nbig;
   if (nbig) {
     std::vector<unsigned long long> sz(nbig), off(nbig);
-    UC_CK(cudaMemcpy(sz.data(), f.big_size, nbig * 8, cudaMemcpyDeviceToHost));
+    UC_CK(cudaMemcpyAsync(sz.data(), f.big_size, nbig * 8, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
     unsigned long long tot = 0;
-    for (uint32_t i = 0; i < nbig; ++i) { off[i] = tot; tot += sz[i]; }
+    for (uint32_t i = 0; i < nbig; ++i) {
+      off[i] = tot;
+      tot += sz[i];
+    }
     const size_t want = size_t(tot) + size_t(nbig) * 8 + 4096;
     if (want > e.big_cap) {
-      if (e.big_buf) cudaFree(e.big_buf);
+      if (e.big_buf) {
+        cudaStreamSynchronize(e.stream);
+        cudaFree(e.big_buf);
+      }
       e.big_buf = nullptr;
       e.big_cap = 0;
       if (want > e.budget) return e.fail(UC_EBUDGET, "scratch for oversized buckets");
@@ -1275,6 +1366,7 @@ static int run_tiles(Env& e, TileParams& tp, const Fused& f, uint32_t threads) {
     tp.big_list = f.big_list;
     tp.big_scratch = scratch;
     tp.big_off = d_off;
+    ++e.launches;
     k_tile_big<NW><<<nbig, 1024, 0, e.stream>>>(tp);
     UC_CK(cudaGetLastError());
     UC_CK(cudaStreamSynchronize(e.stream));
@@ -1286,65 +1378,73 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
                uint32_t* pred) {
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
   if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
-  if (n >= 0xFFFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 32-bit ids");
-  const size_t mark = e.used;
-  Fused f{};
-  uint32_t cap, tslots, bbits;
-  int l_used;
-  uint64_t nn = n;
-  e.extra_need = 0;
-  int r = front(e, nullptr, 0, k, l, 1, d_keys, n, seed, f, nn, cap, tslots, nullptr, l_used, bbits);
+  if (n >= 0x7FFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 31-bit ids");
+  if (n == 0) return UC_OK;
+  e.reset();
+  const int nw = (k <= 31) ? 1 : 2;
+  const Plan P = plan_buckets(e, n, k, l);
+  int r = e.reserve(0, front_bytes(n, nw, P.M, false));
+  if (r) return r;
+  Front f{};
+  r = take_front(e, n, nw, P.M, false, f);
+  if (r) return r;
+  f.keys = const_cast<uint64_t*>(d_keys);
+  UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+  UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
+  ++e.launches;
+  if (nw == 1) k_lmin_count<1><<<grid_for(e, n, 256), 256, 0, e.stream>>>(d_keys, n, k, P.l_used, seed, P.bbits, f.b1, f.b2, f.counts);
+  else k_lmin_count<2><<<grid_for(e, n, 256), 256, 0, e.stream>>>(d_keys, n, k, P.l_used, seed, P.bbits, f.b1, f.b2, f.counts);
+  uint64_t copies = 0;
+  r = bucket_offsets(e, f, P.M, copies);
+  if (r) return r;
+  r = e.reserve(1, copies * (8 * nw + 4) + 1024);
+  if (r) return r;
+  uint64_t* pkeys = static_cast<uint64_t*>(e.take(1, copies * 8 * nw));
+  uint32_t* plink = static_cast<uint32_t*>(e.take(1, copies * 4));
+  if (!plink) return e.fail(UC_EBUDGET, "back arena overflow");
+  r = plan_and_scatter(e, f, P, n, nw, 1, pkeys, plink);
   if (r) return r;
   TileParams tp{};
-  tp.pkeys = f.pkeys;
-  tp.plink = f.plink;
+  tp.pkeys = pkeys;
+  tp.plink = plink;
   tp.tile_begin = f.tile_begin;
   tp.ctr = e.ctr;
   tp.k = k;
-  tp.cap = cap;
-  tp.tslots = tslots;
+  tp.cap = P.cap;
+  tp.tslots = P.tslots;
   tp.mode = 0;
   tp.succ = succ;
   tp.pred = pred;
-  r = (k <= 31) ? run_tiles<1>(e, tp, f, 512) : run_tiles<2>(e, tp, f, 512);
+  r = (nw == 1) ? run_tiles<1>(e, tp, f, 512) : run_tiles<2>(e, tp, f, 512);
   if (r) return r;
-  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
-  UC_CK(cudaStreamSynchronize(e.stream));
-  e.used = mark;
+  r = e.read_ctr();
+  e.reset();
+  if (r) return r;
   return e.check_err(e.h_ctr);
 }
 
-// Weighted list ranking over `prev` by asynchronous pointer jumping.
-// Returns the number of entries left on cycles (in act[0..left)).
-static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t n, bool count_on_device,
-                      unsigned long long* X, uint32_t* act0, uint32_t* act1, uint32_t& left,
-                      uint32_t& rounds_used, uint32_t*& act_final) {
-  uint32_t* cnt = &e.ctr->active;
-  uint32_t* cnt2 = &e.ctr->active_next;
-  UC_CK(cudaMemsetAsync(cnt, 0, 8, e.stream));
-  const int grid = grid_for(e, n ? n : 1, 256);
-  k_rank_init<<<grid, 256, 0, e.stream>>>(prev, w, n, count_on_device ? e.ctr : nullptr, X, act0, cnt);
-  uint32_t* a = act0;
-  uint32_t* b = act1;
-  uint32_t maxr = 2;
-  for (uint64_t t = 1; t < n; t <<= 1) ++maxr;
-  uint32_t h = 0;
-  rounds_used = 0;
-  for (uint32_t r = 0; r < maxr + 2; ++r) {
-    UC_CK(cudaMemcpyAsync(&e.h_ctr->active, cnt, 4, cudaMemcpyDeviceToHost, e.stream));
-    UC_CK(cudaStreamSynchronize(e.stream));
-    h = e.h_ctr->active;
-    if (h == 0) break;
-    UC_CK(cudaMemsetAsync(cnt2, 0, 4, e.stream));
-    k_rank_round<<<grid_for(e, h, 256), 256, 0, e.stream>>>(X, a, cnt, b, cnt2);
-    UC_CK(cudaMemcpyAsync(cnt, cnt2, 4, cudaMemcpyDeviceToDevice, e.stream));
-    std::swap(a, b);
-    ++rounds_used;
+// Weighted list ranking over `prev` by asynchronous pointer jumping, all
+// rounds enqueued without host round trips: round r reads list r%2 with its
+// count in cnt[r] and appends survivors to the other list, count cnt[r+1].
+// A round whose count is 0 returns at once.  The last list holds the
+// entries left on cycles, its count in cnt[rounds].
+static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t nmax, bool count_on_device,
+                      unsigned long long* X, uint32_t* act0, uint32_t* act1, uint32_t* cnt, uint32_t& rounds,
+                      uint32_t*& act_final, uint32_t*& cnt_final) {
+  rounds = 2;
+  for (uint64_t t = 1; t < nmax; t <<= 1) ++rounds;
+  UC_CK(cudaMemsetAsync(cnt, 0, (rounds + 1) * 4, e.stream));
+  const int grid = grid_for(e, nmax ? nmax : 1, 256);
+  ++e.launches;
+  k_rank_init<<<grid, 256, 0, e.stream>>>(prev, w, nmax, count_on_device ? e.ctr : nullptr, X, act0, cnt);
+  uint32_t* lists[2] = {act0, act1};
+  for (uint32_t r = 0; r < rounds; ++r) {
+    ++e.launches;
+    k_rank_round<<<grid, 256, 0, e.stream>>>(X, lists[r & 1], cnt + r, lists[(r + 1) & 1], cnt + r + 1);
   }
-  UC_CK(cudaMemcpyAsync(&e.h_ctr->active, cnt, 4, cudaMemcpyDeviceToHost, e.stream));
-  UC_CK(cudaStreamSynchronize(e.stream));
-  left = e.h_ctr->active;
-  act_final = a;
+  UC_CK(cudaGetLastError());
+  act_final = lists[rounds & 1];
+  cnt_final = cnt + rounds;
   return UC_OK;
 }
 
@@ -1352,34 +1452,40 @@ int contract(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_
              int method, uint32_t* head, uint32_t* rank, uint64_t& ncyc) {
   (void)method;
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  if (n >= 0x7FFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 31-bit ids");
   ncyc = 0;
   if (n == 0) return UC_OK;
-  const size_t mark = e.used;
-  int r = e.reserve(e.used + n * (8 + 4 + 4 + 1) + (size_t(1) << 20));
+  e.reset();
+  int r = e.reserve(1, n * (8 + 4 + 4 + 1) + 64 * 8 + 4096);
   if (r) return r;
-  unsigned long long* X = static_cast<unsigned long long*>(e.take(n * 8));
-  uint32_t* a0 = static_cast<uint32_t*>(e.take(n * 4));
-  uint32_t* a1 = static_cast<uint32_t*>(e.take(n * 4));
-  uint8_t* seen = static_cast<uint8_t*>(e.take(n));
-  unsigned long long* dcyc = static_cast<unsigned long long*>(e.take(8));
+  unsigned long long* X = static_cast<unsigned long long*>(e.take(1, n * 8));
+  uint32_t* a0 = static_cast<uint32_t*>(e.take(1, n * 4));
+  uint32_t* a1 = static_cast<uint32_t*>(e.take(1, n * 4));
+  uint8_t* seen = static_cast<uint8_t*>(e.take(1, n));
+  uint32_t* cnt = static_cast<uint32_t*>(e.take(1, 64 * 4));
+  unsigned long long* dcyc = static_cast<unsigned long long*>(e.take(1, 8));
   if (!dcyc) return e.fail(UC_EBUDGET, "arena overflow");
-  uint32_t left = 0, rounds = 0;
-  uint32_t* act = nullptr;
-  r = rank_lists(e, pred, nullptr, n, false, X, a0, a1, left, rounds, act);
+  uint32_t rounds = 0;
+  uint32_t *act = nullptr, *left = nullptr;
+  r = rank_lists(e, pred, nullptr, n, false, X, a0, a1, cnt, rounds, act, left);
   if (r) return r;
+  ++e.launches;
   k_head_rank<<<grid_for(e, n, 256), 256, 0, e.stream>>>(X, n, head, rank);
-  if (left) {
+  uint32_t hleft = 0;
+  UC_CK(cudaMemcpyAsync(&hleft, left, 4, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  if (hleft) {
     UC_CK(cudaMemsetAsync(seen, 0, n, e.stream));
     UC_CK(cudaMemsetAsync(dcyc, 0, 8, e.stream));
-    if (k <= 31) k_vertex_cycles<1><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, n, head, rank, seen, dcyc);
-    else k_vertex_cycles<2><<<1, 1, 0, e.stream>>>(act, left, succ, d_keys, n, head, rank, seen, dcyc);
+    ++e.launches;
+    if (k <= 31) k_vertex_cycles<1><<<1, 1, 0, e.stream>>>(act, hleft, succ, d_keys, n, head, rank, seen, dcyc);
+    else k_vertex_cycles<2><<<1, 1, 0, e.stream>>>(act, hleft, succ, d_keys, n, head, rank, seen, dcyc);
     unsigned long long hc = 0;
     UC_CK(cudaMemcpyAsync(&hc, dcyc, 8, cudaMemcpyDeviceToHost, e.stream));
     UC_CK(cudaStreamSynchronize(e.stream));
     ncyc = hc;
   }
-  UC_CK(cudaStreamSynchronize(e.stream));
-  e.used = mark;
+  e.reset();
   return UC_OK;
 }
 
@@ -1389,16 +1495,17 @@ int emit(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* h
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
   out_bytes = 0;
   if (n == 0) return UC_OK;
-  const size_t mark = e.used;
-  int r = e.reserve(e.used + n * 16 + scan_tmp_elems(n) * 8 + (size_t(1) << 20));
+  e.reset();
+  int r = e.reserve(1, n * 16 + scan_tmp_elems(n) * 8 + 4096);
   if (r) return r;
-  uint32_t* cnt = static_cast<uint32_t*>(e.take(n * 4));
-  uint32_t* len = static_cast<uint32_t*>(e.take(n * 4));
-  unsigned long long* loff = static_cast<unsigned long long*>(e.take((n + 1) * 8));
-  unsigned long long* tmp = static_cast<unsigned long long*>(e.take(scan_tmp_elems(n) * 8));
+  uint32_t* cnt = static_cast<uint32_t*>(e.take(1, n * 4));
+  uint32_t* len = static_cast<uint32_t*>(e.take(1, n * 4));
+  unsigned long long* loff = static_cast<unsigned long long*>(e.take(1, (n + 1) * 8));
+  unsigned long long* tmp = static_cast<unsigned long long*>(e.take(1, scan_tmp_elems(n) * 8));
   if (!tmp) return e.fail(UC_EBUDGET, "arena overflow");
   UC_CK(cudaMemsetAsync(cnt, 0, n * 4, e.stream));
   const int grid = grid_for(e, n, 256);
+  e.launches += 2 + 6;
   k_count_members<<<grid, 256, 0, e.stream>>>(head, n, cnt);
   k_line_len<<<grid, 256, 0, e.stream>>>(head, cnt, n, k, len);
   scan_excl<uint32_t, unsigned long long>(len, n, loff, tmp, e.stream);
@@ -1408,12 +1515,13 @@ int emit(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* h
   out_bytes = total;
   if (out) {
     if (total > cap) return e.fail(UC_EINPUT, "output buffer too small");
+    ++e.launches;
     if (k <= 31) k_spell<1><<<grid, 256, 0, e.stream>>>(d_keys, head, rank, cnt, loff, n, k, out);
     else k_spell<2><<<grid, 256, 0, e.stream>>>(d_keys, head, rank, cnt, loff, n, k, out);
     UC_CK(cudaGetLastError());
     UC_CK(cudaStreamSynchronize(e.stream));
   }
-  e.used = mark;
+  e.reset();
   return UC_OK;
 }
 
@@ -1422,119 +1530,166 @@ uint64_t output_bound(size_t text_bytes, int k) {
   return uint64_t(text_bytes) + 64;
 }
 
+// The fused path.  Device memory: the front arena holds per-k-mer arrays
+// (keys, bucket ids) and per-bucket arrays; the back arena, sized once the
+// cross k-mers X are counted, holds the n+X bucketed copies and the segment
+// arrays (at most 2X open segments: each holds an S-only start or a P-only
+// end, one of each per cross k-mer).
 int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char* out, uint64_t cap,
                    uint64_t& out_bytes, uc_stats* st) {
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
   if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
   const int nw = (k <= 31) ? 1 : 2;
-  e.used = 0;
+  e.reset();
+  e.launches = 0;
   uint64_t n = 0, body = 0;
   int r = parse_header(e, d_text, bytes, n, body);
   if (r) return r;
-  if (n >= 0xFFFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 32-bit ids");
-  // Segment bounds.  Every open segment holds a P-only end or an S-only
-  // start, so there are at most 2 * cross + closed-free segments <= copies;
-  // its chars are k-1+m <= k per copy.
-  const uint64_t ncp = 2 * n + 1;
-  const uint64_t segchars = ncp * uint64_t(k) + 64;
-  e.extra_need = ncp * (8 + 4 + 4 + 4 + 4 + 4 + 4 + 4 + 4 + 8 + 8 + 1 + 4) + segchars +
-                 scan_tmp_elems(ncp) * 8 + 2 * (n + 1) * 4 + (size_t(8) << 20);
-  Fused f{};
-  uint32_t tcap, tslots, bbits;
-  int l_used;
-  r = front(e, d_text, bytes, k, l, 0, nullptr, 0, e.seed, f, n, tcap, tslots, st, l_used, bbits);
+  if (n >= 0x7FFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 31-bit ids");
+  const Plan P = plan_buckets(e, n, k, l);
+  r = e.reserve(0, front_bytes(n, nw, P.M, true));
   if (r) return r;
-  auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(c * 8)); };
-  auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(c * 4)); };
-  unsigned long long* seg_off = T64(ncp);
-  uint32_t* seg_len = T32(ncp);
-  uint32_t* seg_sx = T32(ncp);
-  uint32_t* seg_ex = T32(ncp);
-  uint32_t* start_seg = T32(n + 1);
-  uint32_t* end_seg = T32(n + 1);
-  char* segc = static_cast<char*>(e.take(segchars));
-  uint32_t* next = T32(ncp);
-  uint32_t* prev = T32(ncp);
-  uint32_t* wgt = T32(ncp);
-  uint32_t* act0 = T32(ncp);
-  uint32_t* act1 = T32(ncp);
-  uint32_t* llen = T32(ncp);
-  uint32_t* hlen = T32(ncp);
-  unsigned long long* X = T64(ncp);
-  unsigned long long* loff = T64(ncp + 1);
-  uint8_t* oncyc = static_cast<uint8_t*>(e.take(ncp));
-  unsigned long long* stmp = T64(scan_tmp_elems(ncp));
+  Front f{};
+  r = take_front(e, n, nw, P.M, true, f);
+  if (r) return r;
+  UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+  UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
+  cudaEventRecord(e.ev[0], e.stream);
+  FuseArgs fz;
+  fz.l = P.l_used;
+  fz.seed = e.seed;
+  fz.bbits = P.bbits;
+  fz.b1 = f.b1;
+  fz.b2 = f.b2;
+  fz.counts = f.counts;
+  fz.M = P.M;
+  uint64_t n2 = 0;
+  r = pack_impl(e, d_text, bytes, k, f.keys, n2, &fz);
+  if (r) return r;
+  cudaEventRecord(e.ev[1], e.stream);
+  uint64_t copies = 0;
+  r = bucket_offsets(e, f, P.M, copies);
+  if (r) return r;
+  const uint64_t X = copies - n;
+  const uint64_t S = 2 * X + 1;
+  const uint64_t segchars = S * uint64_t(k) + copies + 64;
+  const uint32_t R = 64;
+  size_t back = 0;
+  auto add = [&](size_t b) { back += (b + 255) & ~size_t(255); };
+  add(copies * 8 * nw); add(copies * 4);                       // copies
+  add(S * 8); add(S * 4); add(S * 4); add(S * 4);              // seg_off, len, sx, ex
+  add((X + 1) * 4); add((X + 1) * 4);                          // start_seg, end_seg
+  add(segchars);
+  add(S * 4); add(S * 4); add(S * 4); add(S * 4); add(S * 4);  // next, prev, w, act0, act1
+  add(S * 4); add(S * 4); add(S * 8); add((S + 1) * 8); add(S); // llen, hlen, X, loff, oncyc
+  add(scan_tmp_elems(S) * 8); add(8); add(R * 4);
+  r = e.reserve(1, back);
+  if (r) return r;
+  auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
+  auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(1, c * 4)); };
+  uint64_t* pkeys = reinterpret_cast<uint64_t*>(T64(copies * nw));
+  uint32_t* plink = T32(copies);
+  unsigned long long* seg_off = T64(S);
+  uint32_t* seg_len = T32(S);
+  uint32_t* seg_sx = T32(S);
+  uint32_t* seg_ex = T32(S);
+  uint32_t* start_seg = T32(X + 1);
+  uint32_t* end_seg = T32(X + 1);
+  char* segc = static_cast<char*>(e.take(1, segchars));
+  uint32_t* next = T32(S);
+  uint32_t* prev = T32(S);
+  uint32_t* wgt = T32(S);
+  uint32_t* act0 = T32(S);
+  uint32_t* act1 = T32(S);
+  uint32_t* llen = T32(S);
+  uint32_t* hlen = T32(S);
+  unsigned long long* Xr = T64(S);
+  unsigned long long* loff = T64(S + 1);
+  uint8_t* oncyc = static_cast<uint8_t*>(e.take(1, S));
+  unsigned long long* stmp = T64(scan_tmp_elems(S));
   unsigned long long* dtotal = T64(1);
-  if (!dtotal) return e.fail(UC_EBUDGET, "arena overflow");
+  uint32_t* rcnt = T32(R);
+  if (!rcnt) return e.fail(UC_EBUDGET, "back arena overflow");
+  r = plan_and_scatter(e, f, P, n, nw, 0, pkeys, plink);
+  if (r) return r;
+  cudaEventRecord(e.ev[2], e.stream);
 
   TileParams tp{};
-  tp.pkeys = f.pkeys;
-  tp.plink = f.plink;
+  tp.pkeys = pkeys;
+  tp.plink = plink;
   tp.tile_begin = f.tile_begin;
   tp.ctr = e.ctr;
   tp.k = k;
-  tp.cap = tcap;
-  tp.tslots = tslots;
+  tp.cap = P.cap;
+  tp.tslots = P.tslots;
   tp.mode = 1;
   tp.out = out;
   tp.out_cap = cap;
   tp.segchars = segc;
   tp.segchars_cap = segchars;
-  tp.seg_cap = uint32_t(std::min<uint64_t>(ncp, 0xFFFFFFFEull));
+  tp.seg_cap = uint32_t(S);
   tp.seg_off = seg_off;
   tp.seg_len = seg_len;
   tp.seg_sx = seg_sx;
   tp.seg_ex = seg_ex;
   tp.start_seg = start_seg;
   tp.end_seg = end_seg;
-  // seg_count served as nothing before; cross_count now holds the cross k-mers
-  UC_CK(cudaMemsetAsync(&e.ctr->seg_count, 0, 4, e.stream));
   const uint32_t threads = e.tune.tile_threads ? e.tune.tile_threads : 512;
   r = (nw == 1) ? run_tiles<1>(e, tp, f, threads) : run_tiles<2>(e, tp, f, threads);
   if (r) return r;
   cudaEventRecord(e.ev[3], e.stream);
-  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
-  UC_CK(cudaStreamSynchronize(e.stream));
+  r = e.read_ctr();
+  if (r) return r;
   if (e.h_ctr->err) return e.check_err(e.h_ctr);
-  const uint32_t S = e.h_ctr->seg_count;
+  const uint32_t nseg = e.h_ctr->seg_count;
   const unsigned long long closed_bytes = e.h_ctr->out_cursor;
-  uint32_t rounds = 0, left = 0;
-  if (S) {
-    const int gs = grid_for(e, S, 256);
+  uint32_t rounds = 0;
+  if (nseg) {
+    const int gs = grid_for(e, nseg, 256);
+    e.launches += 1;
     k_seg_link<<<gs, 256, 0, e.stream>>>(e.ctr, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k);
-    uint32_t* act = nullptr;
-    r = rank_lists(e, prev, wgt, S, true, X, act0, act1, left, rounds, act);
+    uint32_t *act = nullptr, *left = nullptr;
+    r = rank_lists(e, prev, wgt, nseg, true, Xr, act0, act1, rcnt, rounds, act, left);
     if (r) return r;
-    UC_CK(cudaMemsetAsync(oncyc, 0, S, e.stream));
-    if (left) k_mark_cycle<<<grid_for(e, left, 256), 256, 0, e.stream>>>(act, &e.ctr->active, oncyc);
-    k_chain_len<<<gs, 256, 0, e.stream>>>(e.ctr, X, next, wgt, oncyc, llen);
+    UC_CK(cudaMemsetAsync(oncyc, 0, nseg, e.stream));
+    e.launches += 3 + 6 + 2;
+    k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
+    k_chain_len<<<gs, 256, 0, e.stream>>>(e.ctr, Xr, next, wgt, oncyc, llen);
     k_head_len<<<gs, 256, 0, e.stream>>>(e.ctr, prev, llen, hlen);
-    scan_excl<uint32_t, unsigned long long>(hlen, S, loff, stmp, e.stream, dtotal);
-    k_seg_copy<<<grid_for(e, uint64_t(S) * 32, 256), 256, 0, e.stream>>>(e.ctr, X, next, prev, wgt, oncyc, seg_off,
-                                                                          loff, segc, out, closed_bytes, k);
+    scan_excl<uint32_t, unsigned long long>(hlen, nseg, loff, stmp, e.stream, dtotal);
+    k_seg_copy<<<grid_for(e, uint64_t(nseg) * 32, 256), 256, 0, e.stream>>>(e.ctr, Xr, next, prev, wgt, oncyc,
+                                                                             seg_off, loff, segc, out, closed_bytes, k);
     k_add_cursor<<<1, 1, 0, e.stream>>>(e.ctr, dtotal);
-    if (left) {
-      if (nw == 1) k_seg_cycles<1><<<1, 1, 0, e.stream>>>(e.ctr, act, left, oncyc, next, seg_len, seg_off, segc, out, cap, k);
-      else k_seg_cycles<2><<<1, 1, 0, e.stream>>>(e.ctr, act, left, oncyc, next, seg_len, seg_off, segc, out, cap, k);
+    uint32_t hleft = 0;
+    UC_CK(cudaMemcpyAsync(&hleft, left, 4, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    if (hleft) {
+      ++e.launches;
+      if (nw == 1) k_seg_cycles<1><<<1, 1, 0, e.stream>>>(e.ctr, act, hleft, oncyc, next, seg_len, seg_off, segc, out, cap, k);
+      else k_seg_cycles<2><<<1, 1, 0, e.stream>>>(e.ctr, act, hleft, oncyc, next, seg_len, seg_off, segc, out, cap, k);
     }
     UC_CK(cudaGetLastError());
   }
   cudaEventRecord(e.ev[4], e.stream);
-  UC_CK(cudaMemcpyAsync(e.h_ctr, e.ctr, sizeof(Counters), cudaMemcpyDeviceToHost, e.stream));
-  UC_CK(cudaStreamSynchronize(e.stream));
+  r = e.read_ctr();
+  if (r) return r;
   if (e.h_ctr->err) return e.check_err(e.h_ctr);
   out_bytes = e.h_ctr->out_cursor;
   if (out_bytes > cap) return e.fail(UC_EINTERNAL, "output bound exceeded");
   if (st) {
     st->n_kmers = n;
-    st->n_copies = n + e.h_ctr->cross_count;
-    st->n_cross = e.h_ctr->cross_count;
+    st->n_copies = copies;
+    st->n_cross = X;
     st->n_tiles = e.h_ctr->ntiles;
     st->n_big_tiles = e.h_ctr->nbig;
-    st->n_segments = S;
+    st->n_segments = nseg;
     st->n_cycles = e.h_ctr->cycles;
     st->out_bytes = out_bytes;
     st->stitch_rounds = rounds;
+    st->l_used = uint32_t(P.l_used);
+    st->bucket_bits = P.bbits;
+    st->tile_capacity = P.cap;
+    st->launches = e.launches;
     float a = 0, b = 0, c = 0, d = 0;
     cudaEventElapsedTime(&a, e.ev[0], e.ev[1]);
     cudaEventElapsedTime(&b, e.ev[1], e.ev[2]);
@@ -1546,7 +1701,7 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
     st->ms_stitch = d;
     st->ms_total = a + b + c + d;
   }
-  e.used = 0;
+  e.reset();
   return UC_OK;
 }
 

@@ -10,31 +10,38 @@
 
 namespace uc {
 
-// Per-context state: stream, device scratch arena, counters, tuning.
+// Grow-only device scratch region.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0;
+  size_t used = 0;
+};
+
+// Per-context state: stream, device scratch arenas, counters, tuning.
 struct Env {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int sm_count = 148;
+  int smem_optin = 232448;  // max dynamic shared memory per block
   size_t budget = 0;
-  char* arena = nullptr;
-  size_t cap = 0;
-  size_t used = 0;
-  size_t extra_need = 0;
+  Arena ar[2];              // 0: per-k-mer arrays, 1: copies/segments/scratch
+  char* big_buf = nullptr;  // scratch of oversized tiles (grow only)
+  size_t big_cap = 0;
   Counters* ctr = nullptr;    // device
   Counters* h_ctr = nullptr;  // pinned host mirror
   cudaEvent_t ev[8] = {};
   uc_tuning tune{};
   uint64_t seed = 0x00C0FFEE5EEDull;
-  int smem_optin = 232448;     // max dynamic shared memory per block
-  char* big_buf = nullptr;     // scratch of oversized tiles (grow only)
-  size_t big_cap = 0;
+  uint32_t launches = 0;    // kernels launched by the last call
   std::string err;
 
   int fail(int code, const std::string& msg);
-  void* take(size_t bytes);
-  // Make the arena hold `bytes`; only valid while nothing is taken (used == 0).
-  int reserve(size_t bytes);
+  void* take(int arena, size_t bytes);
+  // Make an arena hold `bytes`; only while nothing is taken from it.
+  int reserve(int arena, size_t bytes);
+  void reset() { ar[0].used = ar[1].used = 0; }
+  int read_ctr();
   int check_err(const Counters* h);
 };
 
