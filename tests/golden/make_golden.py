@@ -21,15 +21,45 @@ sys.path.insert(0, ROOT)
 
 REF = os.path.join(ROOT, "oracle", "_ref", "uc_ref_serial")
 
-# name -> (genome spec factory, k, l)
+# Full fixtures (input and sorted reference lines, gzipped):
+# name -> (synth factory, kwargs, k, l)
 CASES = {
-    "small_plain_k31": (lambda s: s.small_plain(length=20_000, seed=21), 31, 8),
-    "scale_like_k31": (lambda s: s.scale_plain(length=30_000, seed=22), 31, 8),
-    "batched_job_k31": (lambda s: s.batched_job(7, scale=0.006), 31, 6),
-    "wide_tandem_k63": (lambda s: s.wide_k(length=20_000, seed=23), 63, 8),
-    "k15_gc30": (lambda s: s.GenomeSpec(length=8_000, gc=0.3, seed=24, snp_rate=0.003), 15, 5),
-    "k47_tandem": (lambda s: s.GenomeSpec(length=15_000, gc=0.6, seed=25, snp_rate=0.002, tandem_frac=0.05), 47, 9),
+    "small_plain_k31": ("small_plain", {"length": 20_000, "seed": 21}, 31, 8),
+    "scale_like_k31": ("scale_plain", {"length": 30_000, "seed": 22}, 31, 8),
+    "batched_job_k31": ("batched_job", {"job": 7, "scale": 0.006}, 31, 6),
+    "k15_gc30": ("GenomeSpec", {"length": 30_000, "gc": 0.3, "seed": 24, "snp_rate": 0.003}, 15, 5),
 }
+# Checksum goldens (the input is regenerated from the seeded spec; the
+# reference's sorted lines are pinned by count, bytes and sha256), for sizes
+# too large to commit as text.  The reference reads out of bounds on small
+# cross-bucket outputs (driver.cpp:632-633), so these stay above that size.
+CHECKSUMS = {
+    "small_plain_full_k31": ("small_plain", {}, 31, 8),
+    "wide_tandem_k63": ("wide_k", {"length": 300_000, "seed": 24}, 63, 8),
+    "k47_tandem": ("GenomeSpec", {"length": 120_000, "gc": 0.6, "seed": 26, "snp_rate": 0.002,
+                                  "tandem_frac": 0.05}, 47, 9),
+    "scale_like_k31": ("scale_plain", {"length": 2_000_000, "seed": 27}, 31, 8),
+    "batched_job_k31": ("batched_job", {"job": 11, "scale": 0.3}, 31, 8),
+}
+
+
+def spec_of(fn: str, kw: dict):
+    from unitigcoarsening_b200 import synth
+    return getattr(synth, fn)(**kw)
+
+
+def text_of(fn: str, kw: dict, k: int) -> bytes:
+    from unitigcoarsening_b200 import synth
+    return synth.make_text(spec_of(fn, kw), k).numpy().tobytes()
+
+
+def digest(lines) -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for x in lines:
+        h.update(x)
+        h.update(b"\n")
+    return h.hexdigest()
 
 
 def run_reference(text: bytes, k: int, l: int) -> bytes:
@@ -44,9 +74,9 @@ def run_reference(text: bytes, k: int, l: int) -> bytes:
 
 
 def main():
-    from unitigcoarsening_b200 import synth
-    for name, (mk, k, l) in CASES.items():
-        text = synth.make_text(mk(synth), k).numpy().tobytes()
+    import json
+    for name, (fn, kw, k, l) in CASES.items():
+        text = text_of(fn, kw, k)
         out = run_reference(text, k, l)
         lines = sorted(out.split(b"\n")[:-1])
         with open(os.path.join(HERE, f"{name}.in.txt.gz"), "wb") as f:
@@ -54,6 +84,16 @@ def main():
         with open(os.path.join(HERE, f"{name}.ref.txt.gz"), "wb") as f:
             f.write(gzip.compress(b"".join(x + b"\n" for x in lines), compresslevel=9, mtime=0))
         print(name, "k", k, "l", l, "kmers", text.split(b"\n", 1)[0].decode(), "lines", len(lines))
+    sums = {}
+    for name, (fn, kw, k, l) in CHECKSUMS.items():
+        text = text_of(fn, kw, k)
+        out = run_reference(text, k, l)
+        lines = sorted(out.split(b"\n")[:-1])
+        sums[name] = {"fn": fn, "kwargs": kw, "k": k, "l": l, "n_kmers": int(text.split(b"\n", 1)[0]),
+                      "n_lines": len(lines), "bytes": len(out), "sha256_sorted_lines": digest(lines)}
+        print(name, sums[name])
+    with open(os.path.join(HERE, "checksums.json"), "w") as f:
+        json.dump(sums, f, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":

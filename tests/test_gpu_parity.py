@@ -170,3 +170,24 @@ def test_host_path_and_file(comp, oracle, texts, tmp_path):
     data = outp.read_bytes()
     assert len(data) == 2 * len(want)
     assert sorted_lines(data) == sorted(sorted_lines(want) * 2)
+
+
+def _golden():
+    from tests.test_oracle import _checksum_cases, _golden_cases
+    return _golden_cases(), _checksum_cases()
+
+
+@pytest.mark.parametrize("case", _golden()[0])
+def test_fused_matches_reference_fixture(comp, case):
+    from tests.test_oracle import load_golden
+    text, want, k = load_golden(case)
+    assert fused_lines(comp, text, k, 8 if k > 8 else k - 1) == sorted_lines(want)
+
+
+@pytest.mark.parametrize("name,entry", _golden()[1], ids=[c[0] for c in _golden()[1]])
+def test_fused_matches_reference_checksum(comp, name, entry):
+    from tests.test_oracle import digest, regen_text
+    text = regen_text(entry)
+    lines = fused_lines(comp, text, entry["k"], entry["l"])
+    assert len(lines) == entry["n_lines"]
+    assert digest(lines) == entry["sha256_sorted_lines"]

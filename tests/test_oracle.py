@@ -77,17 +77,73 @@ def test_edges_are_exactly_the_unique_overlaps(oracle):
 
 
 def _golden_cases():
-    if not os.path.isdir(GOLDEN):
-        return []
-    return sorted(f[:-len(".in.txt")] for f in os.listdir(GOLDEN) if f.endswith(".in.txt"))
+    return sorted(f[:-len(".in.txt.gz")] for f in os.listdir(GOLDEN) if f.endswith(".in.txt.gz"))
+
+
+def load_golden(case):
+    import gzip
+    with open(os.path.join(GOLDEN, case + ".in.txt.gz"), "rb") as f:
+        text = gzip.decompress(f.read())
+    with open(os.path.join(GOLDEN, case + ".ref.txt.gz"), "rb") as f:
+        want = gzip.decompress(f.read())
+    import re
+    k = int(re.search(r"(?:^|_)k(\d+)", case).group(1))
+    return text, want, k
+
+
+def _checksum_cases():
+    import json
+    with open(os.path.join(GOLDEN, "checksums.json")) as f:
+        return sorted(json.load(f).items())
+
+
+def digest(lines):
+    import hashlib
+    h = hashlib.sha256()
+    for x in lines:
+        h.update(x)
+        h.update(b"\n")
+    return h.hexdigest()
+
+
+def regen_text(entry):
+    from unitigcoarsening_b200 import synth
+    return synth.make_text(getattr(synth, entry["fn"])(**entry["kwargs"]), entry["k"]).numpy().tobytes()
 
 
 @pytest.mark.parametrize("case", _golden_cases())
-def test_oracle_matches_golden(oracle, case):
-    with open(os.path.join(GOLDEN, case + ".in.txt"), "rb") as f:
-        text = f.read()
-    with open(os.path.join(GOLDEN, case + ".out.txt"), "rb") as f:
-        want = f.read()
-    k = int(case.split("_k")[1].split("_")[0])
+def test_oracle_matches_reference_fixture(oracle, case):
+    """Golden vectors printed by the reference itself (compiled unmodified)."""
+    text, want, k = load_golden(case)
     out, _, _ = oracle.compact(text, k)
     assert sorted_lines(out) == sorted_lines(want)
+
+
+@pytest.mark.parametrize("name,entry", _checksum_cases(), ids=[c[0] for c in _checksum_cases()])
+def test_oracle_matches_reference_checksum(oracle, name, entry):
+    text = regen_text(entry)
+    assert int(text.split(b"\n", 1)[0]) == entry["n_kmers"]
+    out, _, _ = oracle.compact(text, entry["k"])
+    lines = sorted_lines(out)
+    assert len(lines) == entry["n_lines"] and len(out) == entry["bytes"]
+    assert digest(lines) == entry["sha256_sorted_lines"]
+
+
+REF_BIN = os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "uc_ref_serial")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_BIN), reason="reference not compiled here")
+@pytest.mark.parametrize("seed,k", [(101, 31), (102, 63), (103, 47), (104, 15)])
+def test_oracle_matches_live_reference(oracle, tmp_path, seed, k):
+    """The reference binary (its own sources against the Kokkos-API shim) on
+    fresh seeded inputs, sized above its small-input read overrun."""
+    import subprocess
+    from unitigcoarsening_b200 import synth
+    length = {31: 150_000, 63: 300_000, 47: 200_000, 15: 60_000}[k]
+    text = synth.make_text(synth.GenomeSpec(length=length, gc=0.45, seed=seed, snp_rate=0.002,
+                                            repeat_frac=0.03, repeat_copies=(2, 8)), k).numpy().tobytes()
+    inp, outp = tmp_path / "in.txt", tmp_path / "out.txt"
+    inp.write_bytes(text)
+    subprocess.run([REF_BIN, str(inp), str(k), "8", str(outp)], check=True, capture_output=True, timeout=300)
+    out, _, _ = oracle.compact(text, k)
+    assert sorted_lines(outp.read_bytes()) == sorted_lines(out)

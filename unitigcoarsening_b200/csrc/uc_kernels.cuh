@@ -52,8 +52,10 @@ struct TileParams {
   uint32_t* end_seg;
 };
 
+// Shared memory of one tile: keys plus four 16-bit arrays per copy, and
+// 16-bit hash slots.
 __host__ __device__ inline size_t tile_bytes(int nw, uint32_t cap, uint32_t tslots) {
-  return size_t(cap) * (8u * nw + 4u + 16u) + size_t(tslots) * 4u;
+  return size_t(cap) * (8u * nw + 8u) + size_t(tslots) * 2u;
 }
 
 // Smallest power of two >= x, for x <= 2^31 (callers bound x first); larger

@@ -16,6 +16,8 @@
 #include "uc_kernels.cuh"
 #include "uc_pipeline.h"
 
+#include <cuda_pipeline.h>
+
 namespace uc {
 
 // ===================================================================== scan
@@ -307,7 +309,8 @@ __global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Co
   const uint32_t nt = ctr->ntiles;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     const uint64_t c = tile_begin[t + 1] - tile_begin[t];
-    if (tile_begin[t + 1] < tile_begin[t] || c > (1ull << 30)) {
+    // (a tile's line bytes must fit 32-bit offsets: c * 64 < 2^32)
+    if (tile_begin[t + 1] < tile_begin[t] || c > (1ull << 26)) {
       atomicOr(&ctr->err, ERR_INTERNAL);
       continue;
     }
@@ -315,7 +318,7 @@ __global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Co
       const uint32_t i = atomicAdd(&ctr->nbig, 1u);
       big_list[i] = t;
       const uint64_t ts = uint64_t(pow2_at_least(2 * c));
-      big_size[i] = (c * (8ull * nw + 20ull) + ts * 4ull + 255ull) & ~255ull;
+      big_size[i] = (c * (8ull * nw + 16ull) + ts * 4ull + 255ull) & ~255ull;
     }
   }
 }
@@ -378,27 +381,62 @@ __global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ ke
 
 // ==================================================================== tiles
 
-constexpr uint32_t DUP = 0x80000000u;
-constexpr uint32_t CAND_NONE = 0x7FFFFFFFu;
+// In-tile indices: 16-bit for shared-memory tiles (capacity <= 32766), 32-bit
+// for oversized tiles worked in global scratch.  The top bit of A marks a
+// shared prefix ("nullified", assembler.h:138-144) during the edge passes and
+// a cycle copy during the cycle cut.
+template <typename IT>
+struct Ix;
+template <>
+struct Ix<uint16_t> {
+  static constexpr uint32_t NONE = 0xFFFFu, DUP = 0x8000u, CNONE = 0x7FFFu;
+};
+template <>
+struct Ix<uint32_t> {
+  static constexpr uint32_t NONE = 0xFFFFFFFFu, DUP = 0x80000000u, CNONE = 0x7FFFFFFFu;
+};
 
-template <int NW>
+// 32-bit atomics on the word holding a 16-bit element; counters stay below
+// 2^15 so no carry reaches the neighbouring element.
+__device__ __forceinline__ uint32_t* word_of(uint16_t* p, uint32_t& sh) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  sh = uint32_t(a & 2u) * 8u;
+  return reinterpret_cast<uint32_t*>(a & ~uintptr_t(3));
+}
+__device__ __forceinline__ void at_or(uint16_t* p, uint32_t v) {
+  uint32_t sh;
+  uint32_t* w = word_of(p, sh);
+  atomicOr(w, v << sh);
+}
+__device__ __forceinline__ void at_or(uint32_t* p, uint32_t v) { atomicOr(p, v); }
+__device__ __forceinline__ void at_inc(uint16_t* p) {
+  uint32_t sh;
+  uint32_t* w = word_of(p, sh);
+  atomicAdd(w, 1u << sh);
+}
+__device__ __forceinline__ void at_inc(uint32_t* p) { atomicAdd(p, 1u); }
+__device__ __forceinline__ uint32_t at_cas(uint16_t* p, uint32_t cmp, uint32_t val) {
+  return atomicCAS(reinterpret_cast<unsigned short*>(p), static_cast<unsigned short>(cmp),
+                   static_cast<unsigned short>(val));
+}
+__device__ __forceinline__ uint32_t at_cas(uint32_t* p, uint32_t cmp, uint32_t val) { return atomicCAS(p, cmp, val); }
+
+template <int NW, typename IT>
 struct TileMem {
-  uint64_t* key;   // [cap * NW]
-  uint32_t* link;  // [cap]
-  uint32_t* A;     // cand | DUP -> local successor
-  uint32_t* B;     // in-count -> rank
-  uint32_t* P;     // who -> local predecessor
-  uint32_t* Q;     // rank pointer
-  uint32_t* T;     // hash slots [ts] (>= 2*cap), later scratch
+  uint64_t* key;  // [cap * NW], role bits in the last word
+  IT* A;          // suffix-lookup candidate | DUP  -> local successor
+  IT* B;          // in-count                       -> scratch
+  IT* P;          // who                            -> local predecessor -> segment id
+  IT* Q;          // rank pointer / scratch
+  IT* T;          // hash slots [ts >= 2*cap]       -> ranks / scratch
   uint32_t ts;
 };
 
-template <int NW>
-__device__ __forceinline__ TileMem<NW> carve(char* base, uint32_t cap, uint32_t ts) {
-  TileMem<NW> m;
+template <int NW, typename IT>
+__device__ __forceinline__ TileMem<NW, IT> carve(char* base, uint32_t cap, uint32_t ts) {
+  TileMem<NW, IT> m;
   m.key = reinterpret_cast<uint64_t*>(base);
-  m.link = reinterpret_cast<uint32_t*>(m.key + size_t(cap) * NW);
-  m.A = m.link + cap;
+  m.A = reinterpret_cast<IT*>(m.key + size_t(cap) * NW);
   m.B = m.A + cap;
   m.P = m.B + cap;
   m.Q = m.P + cap;
@@ -407,81 +445,115 @@ __device__ __forceinline__ TileMem<NW> carve(char* base, uint32_t cap, uint32_t 
   return m;
 }
 
-template <int NW>
-__device__ __forceinline__ Key<NW> skey(const TileMem<NW>& m, uint32_t i) {
+template <int NW, typename IT>
+__device__ __forceinline__ Key<NW> skey(const TileMem<NW, IT>& m, uint32_t i) {
   Key<NW> k;
 #pragma unroll
   for (int w = 0; w < NW; ++w) k.w[w] = m.key[size_t(i) * NW + w];
   return k;
 }
 
-// Pointer jumping over the local predecessor links: Q[i] -> segment start,
-// B[i] -> distance from it.  Uses T[0..2c) as the second buffer and leaves
-// the result in (Q, B).
-template <int NW>
-__device__ void tile_rank(const TileMem<NW>& m, uint32_t c) {
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-    const uint32_t p = m.P[i];
-    m.Q[i] = (p == NONE) ? i : p;
-    m.B[i] = (p == NONE) ? 0u : 1u;
-  }
-  __syncthreads();
-  uint32_t *px = m.Q, *rx = m.B, *py = m.T, *ry = m.T + c;
-  uint32_t rounds = 0;
-  for (uint32_t lim = 2; lim < 2 * c + 2; lim <<= 1) ++rounds;
-  rounds += 1;
+// Pointer-jumping rounds over (px, rx) with second buffers (py, ry); the
+// result lands in (ptr, rnk).  Starts point at themselves with rank 0.
+template <typename IT>
+__device__ void jump_rounds(uint32_t c, IT* px, IT* rx, IT* py, IT* ry, IT*& ptr, IT*& rnk) {
+  uint32_t rounds = 1;
+  for (uint32_t lim = 1; lim < c; lim <<= 1) ++rounds;
   for (uint32_t r = 0; r < rounds; ++r) {
     int changed = 0;
     for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
       const uint32_t p = px[i];
       const uint32_t np = px[p];
-      py[i] = np;
-      ry[i] = rx[i] + rx[p];
+      py[i] = IT(np);
+      ry[i] = IT(uint32_t(rx[i]) + uint32_t(rx[p]));
       changed |= (np != p);
     }
-    uint32_t* t = px; px = py; py = t;
+    IT* t = px; px = py; py = t;
     t = rx; rx = ry; ry = t;
     if (!__syncthreads_or(changed)) break;
   }
-  if (px != m.Q) {
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-      m.Q[i] = px[i];
-      m.B[i] = rx[i];
-    }
-  }
-  __syncthreads();
+  ptr = px;
+  rnk = rx;
 }
 
-template <int NW>
-__device__ void process_tile(const TileParams& p, const TileMem<NW>& m, uint64_t beg, uint32_t c) {
+struct U3 {
+  unsigned long long a, b, c;
+};
+__device__ __forceinline__ U3 u3_add(U3 x, U3 y) { return U3{x.a + y.a, x.b + y.b, x.c + y.c}; }
+__device__ __forceinline__ U3 u3_shfl_up(U3 v, int o) {
+  return U3{__shfl_up_sync(0xFFFFFFFFu, v.a, o), __shfl_up_sync(0xFFFFFFFFu, v.b, o),
+            __shfl_up_sync(0xFFFFFFFFu, v.c, o)};
+}
+// Exclusive block scan of three counters at once.
+__device__ __forceinline__ U3 block_excl_scan3(U3 v, U3* sc, U3* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  U3 inc = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const U3 t = u3_shfl_up(inc, o);
+    if (lane >= o) inc = u3_add(inc, t);
+  }
+  if (lane == 31) sc[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    U3 s = (lane < nw) ? sc[lane] : U3{0, 0, 0};
+    U3 si = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const U3 t = u3_shfl_up(si, o);
+      if (lane >= o) si = u3_add(si, t);
+    }
+    if (lane < nw) sc[lane] = U3{si.a - s.a, si.b - s.b, si.c - s.c};
+    if (lane == nw - 1) sc[32] = si;
+  }
+  __syncthreads();
+  const U3 base = sc[wid];
+  *total = sc[32];
+  const U3 r{base.a + inc.a - v.a, base.b + inc.b - v.b, base.c + inc.c - v.c};
+  __syncthreads();
+  return r;
+}
+
+template <int NW, typename IT>
+__device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint64_t beg, uint32_t c) {
+  constexpr uint32_t NONE_I = Ix<IT>::NONE, DUP_I = Ix<IT>::DUP, CNONE_I = Ix<IT>::CNONE;
   const PrefMask pm = pref_mask(p.k);
   const uint32_t tmask = m.ts - 1;
   const int k = p.k;
-  // ---- stage the tile's copies
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-    const Key<NW> x = ld_key<NW>(p.pkeys, beg + i);
+  // ---- stage the tile's keys (async copies), initialise the work arrays
+  if constexpr (sizeof(IT) == 2) {
+    // shared-memory tile: asynchronous copies overlap the initialisation
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x)
+      __pipeline_memcpy_async(m.key + size_t(i) * NW, p.pkeys + (beg + i) * NW, 8 * NW);
+    __pipeline_commit();
+  } else {
+    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      const Key<NW> x = ld_key<NW>(p.pkeys, beg + i);
 #pragma unroll
-    for (int w = 0; w < NW; ++w) m.key[size_t(i) * NW + w] = x.w[w];
-    m.link[i] = p.plink[beg + i];
-    m.A[i] = CAND_NONE;
-    m.B[i] = 0;
-    m.P[i] = NONE;
+      for (int w = 0; w < NW; ++w) m.key[size_t(i) * NW + w] = x.w[w];
+    }
   }
-  for (uint32_t i = threadIdx.x; i < m.ts; i += blockDim.x) m.T[i] = NONE;
+  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    m.A[i] = IT(CNONE_I);
+    m.B[i] = 0;
+    m.P[i] = IT(NONE_I);
+  }
+  for (uint32_t i = threadIdx.x; i < m.ts; i += blockDim.x) m.T[i] = IT(NONE_I);
+  if constexpr (sizeof(IT) == 2) __pipeline_wait_prior(0);
   __syncthreads();
   // ---- prefix table of the P copies (generate_hashmap, assembler.h:120-150):
-  // one slot per distinct (k-1)-prefix; a prefix shared by two copies marks
-  // the slot's copy DUP ("nullified")
+  // one slot per distinct (k-1)-prefix; a prefix held by two copies marks the
+  // slot's copy DUP ("nullified")
   for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
     const Key<NW> x = skey(m, i);
     if (!(roles(x) & ROLE_P)) continue;
     const Key<NW> pf = prefix_of(x, pm);
     uint32_t h = key_hash(pf) & tmask;
     for (uint32_t probe = 0; probe <= tmask; ++probe) {
-      const uint32_t cur = atomicCAS(m.T + h, NONE, i);
-      if (cur == NONE) break;
+      const uint32_t cur = at_cas(m.T + h, NONE_I, i);
+      if (cur == NONE_I) break;
       if (key_eq(prefix_of(skey(m, cur), pm), pf)) {
-        atomicOr(m.A + cur, DUP);
+        at_or(m.A + cur, DUP_I);
         break;
       }
       h = (h + 1) & tmask;
@@ -495,60 +567,63 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW>& m, uint64_t
     if (!(roles(x) & ROLE_S)) continue;
     const Key<NW> sf = suffix_of(x, pm);
     uint32_t h = key_hash(sf) & tmask;
-    uint32_t cand = CAND_NONE;
+    uint32_t cand = CNONE_I;
     for (uint32_t probe = 0; probe <= tmask; ++probe) {
       const uint32_t cur = m.T[h];
-      if (cur == NONE) break;
+      if (cur == NONE_I) break;
       if (key_eq(prefix_of(skey(m, cur), pm), sf)) {
-        if (!(m.A[cur] & DUP)) cand = cur;
+        if (!(uint32_t(m.A[cur]) & DUP_I)) cand = cur;
         break;
       }
       h = (h + 1) & tmask;
     }
-    if (cand != CAND_NONE) {
-      atomicAdd(m.B + cand, 1u);
-      m.P[cand] = i;
+    if (cand != CNONE_I) {
+      at_inc(m.B + cand);
+      m.P[cand] = IT(i);
     }
-    m.A[i] = (m.A[i] & DUP) | cand;
+    m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
   }
   __syncthreads();
   // ---- kept edges: u->v iff v is u's unique successor and u is v's only
-  // predecessor ("write edges", assembler.h:189-197)
+  // predecessor ("write edges", assembler.h:189-197); rank init alongside
   for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-    const uint32_t cand = m.A[i] & CAND_NONE;
-    const uint32_t s = (cand != CAND_NONE && m.B[cand] == 1u) ? cand : NONE;
-    const uint32_t q = (m.B[i] == 1u) ? m.P[i] : NONE;
-    m.A[i] = s;
-    m.P[i] = q;
+    const uint32_t cand = uint32_t(m.A[i]) & CNONE_I;
+    const uint32_t s = (cand != CNONE_I && m.B[cand] == 1u) ? cand : NONE_I;
+    const uint32_t q = (m.B[i] == 1u) ? uint32_t(m.P[i]) : NONE_I;
+    m.A[i] = IT(s);
+    m.P[i] = IT(q);
+    m.Q[i] = IT(q == NONE_I ? i : q);
+    m.T[i] = IT(q == NONE_I ? 0u : 1u);
   }
   __syncthreads();
   if (p.mode == 0) {
     for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
       const uint64_t r = roles(skey(m, i));
-      if (r & ROLE_S) p.succ[m.link[i]] = (m.A[i] == NONE) ? NONE : m.link[m.A[i]];
-      if (r & ROLE_P) p.pred[m.link[i]] = (m.P[i] == NONE) ? NONE : m.link[m.P[i]];
+      const uint32_t id = p.plink[beg + i];
+      if (r & ROLE_S) p.succ[id] = (m.A[i] == NONE_I) ? NONE : p.plink[beg + m.A[i]];
+      if (r & ROLE_P) p.pred[id] = (m.P[i] == NONE_I) ? NONE : p.plink[beg + m.P[i]];
     }
     return;
   }
   // ---- local segments: list ranking by pointer jumping
-  tile_rank(m, c);
+  IT *ptr, *rnk;
+  jump_rounds<IT>(c, m.Q, m.T, m.B, m.T + c, ptr, rnk);
   // ---- local cycles (every copy has a local predecessor): cut each at its
   // smallest key, then rank again
   int cyc = 0;
   for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-    // after ranking, a path copy points at its start (no predecessor); a
-    // cycle copy points at another cycle copy.  Flag cycle copies in A's top
-    // bit (A holds a local index < 2^31 or NONE; a cycle copy has a successor).
-    if (m.P[m.Q[i]] != NONE) {
-      m.A[i] |= DUP;
+    // a path copy points at its start (no predecessor); a cycle copy at
+    // another cycle copy.  Cycle copies have a successor, so A = index | DUP.
+    if (m.P[ptr[i]] != NONE_I) {
+      m.A[i] = IT(uint32_t(m.A[i]) | DUP_I);
       cyc = 1;
     }
   }
   if (__syncthreads_or(cyc)) {
-    uint32_t *lx = m.T, *jx = m.T + c, *ly = m.B, *jy = m.Q;  // B/Q recomputed below
+    IT *lx = m.T, *jx = m.T + c, *ly = m.B, *jy = m.Q;
     for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-      lx[i] = i;
-      jx[i] = (m.P[i] == NONE) ? i : m.P[i];
+      lx[i] = IT(i);
+      jx[i] = IT(m.P[i] == NONE_I ? i : uint32_t(m.P[i]));
     }
     __syncthreads();
     uint32_t rounds = 1;
@@ -557,69 +632,64 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW>& m, uint64_t
       for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
         const uint32_t j = jx[i];
         const uint32_t a = lx[i], b = lx[j];
-        ly[i] = key_lt(skey(m, b), skey(m, a)) ? b : a;
+        ly[i] = IT(key_lt(skey(m, b), skey(m, a)) ? b : a);
         jy[i] = jx[j];
       }
       __syncthreads();
-      uint32_t* t = lx; lx = ly; ly = t;
+      IT* t = lx; lx = ly; ly = t;
       t = jx; jx = jy; jy = t;
     }
-    // After ceil(log2 c)+1 rounds a cycle copy's label covers its whole
-    // cycle, so exactly one copy per cycle (the smallest key) is its own
-    // label.  Cut the edge into it; path copies are not touched.
-    int cut = 0;
-    // (a cycle copy always has a successor, so its A is index | DUP, never NONE)
-    auto on_cycle = [](uint32_t a) { return a != NONE && (a & DUP); };
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-      if (on_cycle(m.A[i]) && lx[i] == i) cut = 1;
-    }
-    (void)cut;
-    __syncthreads();
-    // the cycle minimum loses its in-edge: its predecessor becomes the end
+    // after ceil(log2 c)+1 rounds a cycle copy's label covers its whole cycle:
+    // exactly one copy per cycle (the smallest key) is its own label; the edge
+    // into it is cut, path copies are untouched
+    auto on_cycle = [](uint32_t a) { return a != NONE_I && (a & DUP_I); };
     for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
       if (on_cycle(m.A[i]) && lx[i] == i) {
         const uint32_t q = m.P[i];
-        m.A[q] = NONE;
-        m.P[i] = NONE;
+        m.A[q] = IT(NONE_I);
+        m.P[i] = IT(NONE_I);
       }
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
       const uint32_t a = m.A[i];
-      if (on_cycle(a)) m.A[i] = a & ~DUP;
+      if (on_cycle(a)) m.A[i] = IT(a & ~DUP_I);
+      const uint32_t q = m.P[i];
+      m.Q[i] = IT(q == NONE_I ? i : q);
+      m.T[i] = IT(q == NONE_I ? 0u : 1u);
     }
     __syncthreads();
-    tile_rank(m, c);
+    jump_rounds<IT>(c, m.Q, m.T, m.B, m.T + c, ptr, rnk);
   }
-  // every copy now reaches a segment start
-
+  // every copy now reaches a segment start.  Free arrays: the pair not
+  // holding (ptr, rnk) keeps each start's byte offset (lo/hi halves), P its
+  // local segment id.
+  IT* lo_a = (ptr == m.Q) ? m.B : m.Q;
+  IT* hi_a = (rnk == m.T) ? m.T + c : m.T;
   // ---- emission: closed segments (start has role P, end has role S) are
   // whole unitigs; the others are stitched across tiles
-  __shared__ unsigned long long sc64[33];
+  __shared__ U3 sc3[33];
   __shared__ unsigned long long s_base[3];
   __shared__ int s_skip;
   const uint32_t chunk = (c + blockDim.x - 1) / blockDim.x;
   const uint32_t lo = min(c, threadIdx.x * chunk), hi = min(c, lo + chunk);
-  unsigned long long cb = 0, ob = 0, oc = 0;
+  U3 mine{0, 0, 0};
   for (uint32_t i = lo; i < hi; ++i) {
-    if (m.A[i] != NONE) continue;
-    const uint32_t s = m.Q[i];
-    const uint32_t len = m.B[i] + 1;
+    if (m.A[i] != NONE_I) continue;
+    const uint32_t s = ptr[i];
+    const uint32_t len = uint32_t(rnk[i]) + 1;
     const bool closed = (roles(skey(m, s)) & ROLE_P) && (roles(skey(m, i)) & ROLE_S);
-    if (closed) cb += uint64_t(k) + len;
-    else { ob += uint64_t(k) - 1 + len; oc += 1; }
+    if (closed) mine.a += uint64_t(k) + len;
+    else { mine.b += uint64_t(k) - 1 + len; mine.c += 1; }
   }
-  unsigned long long tcb, tob, toc;
-  unsigned long long pcb = block_excl_scan(cb, sc64, &tcb);
-  unsigned long long pob = block_excl_scan(ob, sc64, &tob);
-  unsigned long long poc = block_excl_scan(oc, sc64, &toc);
+  U3 tot;
+  U3 pre = block_excl_scan3(mine, sc3, &tot);
   if (threadIdx.x == 0) {
     s_skip = 0;
-    s_base[0] = tcb ? atomicAdd(&p.ctr->out_cursor, tcb) : 0ull;
-    s_base[1] = tob ? atomicAdd(&p.ctr->seg_char_cursor, tob) : 0ull;
-    s_base[2] = toc ? atomicAdd(&p.ctr->seg_count, uint32_t(toc)) : 0u;
-    if (s_base[0] + tcb > p.out_cap || s_base[1] + tob > p.segchars_cap ||
-        s_base[2] + toc > p.seg_cap) {
+    s_base[0] = tot.a ? atomicAdd(&p.ctr->out_cursor, tot.a) : 0ull;
+    s_base[1] = tot.b ? atomicAdd(&p.ctr->seg_char_cursor, tot.b) : 0ull;
+    s_base[2] = tot.c ? atomicAdd(&p.ctr->seg_count, uint32_t(tot.c)) : 0u;
+    if (s_base[0] + tot.a > p.out_cap || s_base[1] + tot.b > p.segchars_cap || s_base[2] + tot.c > p.seg_cap) {
       atomicOr(&p.ctr->err, ERR_CAPACITY);
       s_skip = 1;
     }
@@ -627,39 +697,45 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW>& m, uint64_t
   __syncthreads();
   if (s_skip) return;
   const unsigned long long cbase = s_base[0], obase = s_base[1], sbase = s_base[2];
-  // per segment start: tile-local byte offset (T[s]) and local segment index
-  // (T[c + s], NONE for a closed segment)
   for (uint32_t i = lo; i < hi; ++i) {
-    if (m.A[i] != NONE) continue;
-    const uint32_t s = m.Q[i];
-    const uint32_t len = m.B[i] + 1;
+    if (m.A[i] != NONE_I) continue;
+    const uint32_t s = ptr[i];
+    const uint32_t len = uint32_t(rnk[i]) + 1;
     const bool closed = (roles(skey(m, s)) & ROLE_P) && (roles(skey(m, i)) & ROLE_S);
+    uint64_t loc;
     if (closed) {
-      m.T[s] = uint32_t(pcb);
-      m.T[c + s] = NONE;
-      pcb += uint64_t(k) + len;
+      loc = pre.a;
+      m.P[s] = IT(NONE_I);
+      pre.a += uint64_t(k) + len;
     } else {
-      m.T[s] = uint32_t(pob);
-      m.T[c + s] = uint32_t(poc);
-      pob += uint64_t(k) - 1 + len;
-      poc += 1;
+      loc = pre.b;
+      m.P[s] = IT(pre.c);
+      pre.b += uint64_t(k) - 1 + len;
+      pre.c += 1;
+    }
+    if constexpr (sizeof(IT) == 2) {
+      lo_a[s] = IT(loc & 0xFFFFu);
+      hi_a[s] = IT(loc >> 16);
+    } else {
+      lo_a[s] = IT(loc);
     }
   }
   __syncthreads();
   for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-    const uint32_t s = m.Q[i];
-    const uint32_t r = m.B[i];
-    const uint32_t loc = m.T[s];
-    const uint32_t sid = m.T[c + s];
+    const uint32_t s = ptr[i];
+    const uint32_t r = rnk[i];
+    uint64_t loc = lo_a[s];
+    if constexpr (sizeof(IT) == 2) loc |= uint64_t(hi_a[s]) << 16;
+    const uint32_t sid = m.P[s];
     const Key<NW> x = skey(m, i);
-    char* dst = (sid == NONE) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
+    char* dst = (sid == NONE_I) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
     if (r == 0) {
       for (int ch = 0; ch < k; ++ch) dst[ch] = acgt(key_char(x, ch));
     } else {
       dst[k - 1 + r] = acgt(key_char(x, k - 1));
     }
-    if (m.A[i] == NONE) {
-      if (sid == NONE) {
+    if (m.A[i] == NONE_I) {
+      if (sid == NONE_I) {
         dst[k + r] = '\n';
       } else {
         const uint32_t g = uint32_t(sbase) + sid;
@@ -667,10 +743,12 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW>& m, uint64_t
         const bool p_only = (roles(x) & ROLE_S) == 0;
         p.seg_off[g] = obase + loc;
         p.seg_len[g] = r + 1;
-        p.seg_sx[g] = s_only ? m.link[s] : NONE;
-        p.seg_ex[g] = p_only ? m.link[i] : NONE;
-        if (s_only) p.start_seg[m.link[s]] = g;
-        if (p_only) p.end_seg[m.link[i]] = g;
+        const uint32_t sx = s_only ? p.plink[beg + s] : NONE;
+        const uint32_t ex = p_only ? p.plink[beg + i] : NONE;
+        p.seg_sx[g] = sx;
+        p.seg_ex[g] = ex;
+        if (s_only) p.start_seg[sx] = g;
+        if (p_only) p.end_seg[ex] = g;
       }
     }
   }
@@ -683,7 +761,7 @@ template <int NW>
 __global__ void __launch_bounds__(512) k_tile(TileParams p) {
   extern __shared__ __align__(16) char smem[];
   __shared__ uint32_t s_t;
-  const TileMem<NW> m = carve<NW>(smem, p.cap, p.tslots);
+  const TileMem<NW, uint16_t> m = carve<NW, uint16_t>(smem, p.cap, p.tslots);
   const uint32_t nt = p.ctr->ntiles;
   for (;;) {
     if (threadIdx.x == 0) s_t = atomicAdd(&p.ctr->tile_next, 1u);
@@ -694,7 +772,7 @@ __global__ void __launch_bounds__(512) k_tile(TileParams p) {
     const uint64_t beg = p.tile_begin[t];
     const uint64_t c = p.tile_begin[t + 1] - beg;
     if (c == 0 || c > p.cap) continue;
-    process_tile<NW>(p, m, beg, uint32_t(c));
+    process_tile<NW, uint16_t>(p, m, beg, uint32_t(c));
     __syncthreads();
   }
 }
@@ -706,8 +784,8 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
   const uint64_t beg = p.tile_begin[t];
   const uint64_t c = p.tile_begin[t + 1] - beg;
   const uint32_t ts = pow2_at_least(2 * c);
-  const TileMem<NW> m = carve<NW>(p.big_scratch + p.big_off[blockIdx.x], uint32_t(c), ts);
-  process_tile<NW>(p, m, beg, uint32_t(c));
+  const TileMem<NW, uint32_t> m = carve<NW, uint32_t>(p.big_scratch + p.big_off[blockIdx.x], uint32_t(c), ts);
+  process_tile<NW, uint32_t>(p, m, beg, uint32_t(c));
 }
 
 // ================================================================= stitch
