@@ -144,18 +144,12 @@ __device__ __forceinline__ char acgt(uint32_t c) {
 
 // Seeded bijection of [0, 4^l): the l-mer priority.  The reference draws a
 // random permutation of the 4^l l-mers (generate_permutation,
-// driver.cpp:356-402); any permutation gives the same unitigs.
+// driver.cpp:356-402); any permutation gives the same unitigs.  An xor, an odd
+// multiplier and an addition modulo 4^l are each invertible.
 __host__ __device__ __forceinline__ uint32_t lmer_priority(uint32_t x, int l, uint64_t seed) {
   const uint32_t b = 2u * static_cast<uint32_t>(l);
   const uint32_t mask = (b >= 32u) ? 0xFFFFFFFFu : ((1u << b) - 1u);
-  const uint32_t sh = (b + 1u) / 2u;
-  x = (x ^ static_cast<uint32_t>(seed)) & mask;
-  x = (x * 0x9E3779B1u) & mask;
-  x ^= x >> sh;
-  x = (x * 0x85EBCA77u) & mask;
-  x ^= x >> sh;
-  x = (x + static_cast<uint32_t>(seed >> 32)) & mask;
-  return x;
+  return ((x ^ static_cast<uint32_t>(seed)) * 0x9E3779B1u + static_cast<uint32_t>(seed >> 32)) & mask;
 }
 
 // Bucket of a minimizer priority.  Any function of the minimizer keeps every
@@ -193,22 +187,18 @@ __device__ __forceinline__ void lmins(const Key<NW>& key, int k, int l, uint64_t
     hi = rev2(key.w[0]);
     lo = rev2(key.w[1] & ~ROLE_MASK);
   }
-  const int w = k - l + 1;
+  const int w = k - l + 1;  // l-mers in the k-mer (>= 2)
   const int sh = 64 - 2 * l;
-  uint32_t first = NONE, mid = NONE, last = NONE;
-  for (int p = 0; p < w; ++p) {
-    const uint32_t id = static_cast<uint32_t>(hi >> sh);
-    const uint32_t pr = table ? __ldg(table + id) : lmer_priority(id, l, seed);
-    if (p == 0) {
-      first = pr;
-    } else if (p == w - 1) {
-      last = pr;
-    } else {
-      mid = min(mid, pr);
-    }
+  auto pri = [&](uint32_t id) { return table ? __ldg(table + id) : lmer_priority(id, l, seed); };
+  const uint32_t first = pri(static_cast<uint32_t>(hi >> sh));
+  uint32_t mid = NONE;
+  for (int p = 1; p < w - 1; ++p) {
     hi = (hi << 2) | (lo >> 62);
     lo <<= 2;
+    mid = min(mid, pri(static_cast<uint32_t>(hi >> sh)));
   }
+  hi = (hi << 2) | (lo >> 62);
+  const uint32_t last = pri(static_cast<uint32_t>(hi >> sh));
   l1 = min(first, mid);
   l2 = min(mid, last);
 }

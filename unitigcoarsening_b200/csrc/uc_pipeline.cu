@@ -97,15 +97,38 @@ __device__ __forceinline__ uint32_t base_code(uint32_t c) {
   return (c == 'C') ? 1u : (c == 'G') ? 2u : (c == 'T') ? 3u : 0u;
 }
 
+// SWAR conversion of 4 text bytes (little-endian in x) to 2-bit codes.
+// A=0x41 C=0x43 G=0x47 T=0x54 give ((b>>1)^(b>>2))&3 = 0,1,2,3; a byte is
+// kept only if rebuilding its letter from that code gives the byte back, so
+// every other byte packs as A (the zeroed char_map of compact_kmers,
+// driver.cpp:228-232).  Returns the codes of the 4 bytes in bytes 0..3 of the
+// result (values 0..3); *nl gets 0x80 in each byte equal to '\n'.
+__device__ __forceinline__ uint32_t swar_codes(uint32_t x, uint32_t* nl) {
+  const uint32_t t = ((x >> 1) ^ (x >> 2)) & 0x03030303u;
+  const uint32_t f = (t << 1) + (((t >> 1) & 0x01010101u) << 1) + (t & (t >> 1) & 0x01010101u) * 11u;
+  const uint32_t eq = ~((0x41414141u + f) ^ x);
+  const uint32_t ok = ((eq & 0x7F7F7F7Fu) + 0x01010101u) & eq & 0x80808080u;  // 0x80 where byte matches
+  const uint32_t z = x ^ 0x0A0A0A0Au;
+  *nl = ~(((z & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | z) & 0x80808080u;
+  return t & ((ok >> 7) * 3u);
+}
+// 4 byte-wise codes -> one byte c0 | c1<<2 | c2<<4 | c3<<6
+__device__ __forceinline__ uint32_t gather_codes(uint32_t t) { return ((t * 0x41041u) >> 18) & 0xFFu; }
+
 // A block packs 256 consecutive lines per pass.  It first stages the text
-// span of those lines in shared memory with 16-byte loads issued by every
-// thread (so the block has the whole span in flight at once), then each warp
-// packs its 32 lines from shared memory: lane j takes chars j and j+32 of a
-// line and the 2-bit codes are gathered with warp OR-reductions; lane i keeps
-// line i's key.  With FUSE the prefix/suffix minimizer buckets of every key
-// are computed and counted in the same pass (lmin_buckets.h:299-318).
+// span of those lines in shared memory with 16-byte loads from every thread
+// (the whole span in flight at once), inserting a 4-byte gap after every 32
+// bytes so that lines 32 bytes apart fall in different banks.  Then each
+// thread packs one line, 4 chars per 32-bit SWAR step.  With FUSE the
+// prefix/suffix minimizer buckets of every key are computed and counted in the
+// same pass (lmin_buckets.h:299-318).
 constexpr int PACK_LINES = 256;
-constexpr int PACK_BUF = 20480;
+constexpr int PACK_SPAN = 18432;                    // staged text bytes per pass
+// + 32 words: a (short) line starting at the end of the span reads up to
+// k + 4 bytes past its start
+constexpr int PACK_WORDS = PACK_SPAN / 4 + PACK_SPAN / 32 + 32;
+
+__device__ __forceinline__ uint32_t pad_word(uint32_t byte_off) { return (byte_off >> 2) + (byte_off >> 5); }
 
 template <int NW, bool FUSE>
 __global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, uint64_t tbytes,
@@ -115,85 +138,111 @@ __global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, 
                                               uint64_t* __restrict__ keys, uint32_t* err, int l,
                                               uint64_t seed, uint32_t bbits, uint32_t* __restrict__ b1,
                                               uint32_t* __restrict__ b2, uint32_t* __restrict__ counts) {
-  __shared__ __align__(16) uint8_t buf[PACK_BUF];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const uint32_t sh = 2u * uint32_t(lane & 15);
+  __shared__ uint32_t buf[PACK_WORDS];
   const uintptr_t tb = reinterpret_cast<uintptr_t>(text);
   uint32_t bad = 0;
+  const uint64_t kmask_hi = (NW == 1) ? ((k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull))
+                                      : ((2 * k - 64 >= 64) ? ~0ull : ((1ull << (2 * k - 64)) - 1ull));
   for (uint64_t b0 = uint64_t(blockIdx.x) * PACK_LINES; b0 < n; b0 += uint64_t(gridDim.x) * PACK_LINES) {
     const uint32_t cnt = uint32_t((n - b0) < PACK_LINES ? (n - b0) : PACK_LINES);
     const uint64_t s0 = starts ? uint64_t(starts[b0]) : body + b0 * stride;
     const uint64_t s1 = (b0 + cnt < n) ? (starts ? uint64_t(starts[b0 + cnt]) : body + (b0 + cnt) * stride) : end;
     const uintptr_t A0 = (tb + s0) & ~uintptr_t(15);
     const uint64_t span = (tb + s1) - A0;
-    const bool staged = span + 16 <= PACK_BUF;
+    const bool staged = span + 16 <= PACK_SPAN;
     if (staged) {
       const uint32_t nch = uint32_t((span + 15) / 16);
       for (uint32_t c = threadIdx.x; c < nch; c += blockDim.x) {
         const uintptr_t a = A0 + 16u * c;
+        uint4 v;
         if (a >= tb && a + 16 <= tb + tbytes) {
-          *reinterpret_cast<uint4*>(buf + 16u * c) = __ldg(reinterpret_cast<const uint4*>(a));
+          v = __ldg(reinterpret_cast<const uint4*>(a));
         } else {
+          uint32_t w[4] = {0x0A0A0A0Au, 0x0A0A0A0Au, 0x0A0A0A0Au, 0x0A0A0A0Au};
           for (int q = 0; q < 16; ++q) {
             const uintptr_t x = a + q;
-            buf[16u * c + q] = (x >= tb && x < tb + tbytes) ? *reinterpret_cast<const uint8_t*>(x) : uint8_t('\n');
+            if (x >= tb && x < tb + tbytes) {
+              const uint32_t byte = *reinterpret_cast<const uint8_t*>(x);
+              w[q >> 2] = (w[q >> 2] & ~(0xFFu << (8 * (q & 3)))) | (byte << (8 * (q & 3)));
+            }
           }
+          v = make_uint4(w[0], w[1], w[2], w[3]);
         }
+        const uint32_t wi = pad_word(16u * c);  // 4 words, never split by a gap
+        buf[wi] = v.x;
+        buf[wi + 1] = v.y;
+        buf[wi + 2] = v.z;
+        buf[wi + 3] = v.w;
       }
     }
     __syncthreads();
-    const int wl0 = wid * 32;
-    const int wcnt = int(cnt) - wl0 < 0 ? 0 : (int(cnt) - wl0 > 32 ? 32 : int(cnt) - wl0);
-    Key<NW> mine;
-#pragma unroll
-    for (int w = 0; w < NW; ++w) mine.w[w] = 0;
-    for (int j = 0; j < wcnt; ++j) {
-      const uint64_t line = b0 + wl0 + j;
+    const uint32_t t = threadIdx.x;
+    if (t < cnt) {
+      const uint64_t line = b0 + t;
       const uint64_t s = starts ? uint64_t(starts[line]) : body + line * stride;
-      uint32_t v[NW];
-      bool lbad = false;
+      Key<NW> key;
 #pragma unroll
-      for (int h = 0; h < NW; ++h) {
-        const int ci = lane + 32 * h;
-        const uint64_t pos = s + ci;
-        uint32_t c;
-        if (staged) c = (pos < s1) ? uint32_t(buf[(tb + pos) - A0]) : uint32_t('\n');
-        else c = (pos < end) ? uint32_t(__ldg(text + pos)) : uint32_t('\n');
-        if (ci < k) {
-          lbad |= (c == '\n') || (pos >= end);
-          v[h] = base_code(c);
-        } else {
-          v[h] = 0;
-          // fixed-width layout: the byte after the k-mer must end the line
-          if (!starts && ci == k && line + 1 < n && c != '\n') lbad = true;
+      for (int w = 0; w < NW; ++w) key.w[w] = 0;
+      bool lbad = false;
+      const bool check_term = !starts && line + 1 < n;
+      if (staged) {
+        const uint32_t off = uint32_t((tb + s) - A0);     // line start in the staged span
+        const uint32_t lim = uint32_t((tb + s1) - A0);    // end of the staged lines
+        lbad |= (off + uint32_t(k) > lim);
+        const uint32_t sh = 8u * (off & 3u);
+        const uint32_t base = off & ~3u;
+        uint32_t cur = buf[pad_word(base)];
+        const int nwords = (k + 4) / 4;  // covers chars 0..k (k chars + terminator)
+#pragma unroll 4
+        for (int j = 0; j < nwords; ++j) {
+          const uint32_t nxt = buf[pad_word(base + 4u * (j + 1))];
+          const uint32_t x = __funnelshift_r(cur, nxt, sh);
+          cur = nxt;
+          uint32_t nl;
+          const uint32_t tc = swar_codes(x, &nl);
+          // bytes of this word that are k-mer chars
+          const int c0 = 4 * j;
+          const uint32_t inmask = (c0 + 4 <= k) ? 0xFFFFFFFFu : (c0 >= k ? 0u : (0xFFFFFFFFu >> (8 * (c0 + 4 - k))));
+          lbad |= (nl & inmask) != 0;
+          if (check_term && c0 <= k && k < c0 + 4) {
+            const uint32_t tbyte = (x >> (8 * (k - c0))) & 0xFFu;
+            lbad |= (tbyte != '\n');
+          }
+          const uint64_t g = uint64_t(gather_codes(tc & inmask));
+          if (NW == 1 || c0 < 32) key.w[0] |= g << (2 * c0);
+          else key.w[NW - 1] |= g << (2 * (c0 - 32));
+        }
+      } else {
+        for (int c = 0; c <= k; ++c) {
+          const uint64_t pos = s + c;
+          const uint32_t ch = (pos < end) ? uint32_t(__ldg(text + pos)) : uint32_t('\n');
+          if (c < k) {
+            lbad |= (ch == '\n') || (pos >= end);
+            const uint64_t code = base_code(ch);
+            if (c < 32) key.w[0] |= code << (2 * c);
+            else key.w[NW - 1] |= code << (2 * (c - 32));
+          } else if (check_term && ch != '\n') {
+            lbad = true;
+          }
         }
       }
-      if (__any_sync(0xFFFFFFFFu, lbad)) bad = 1;
-#pragma unroll
-      for (int h = 0; h < NW; ++h) {
-        const uint32_t x = v[h] << sh;
-        const uint32_t lo = __reduce_or_sync(0xFFFFFFFFu, lane < 16 ? x : 0u);
-        const uint32_t hi = __reduce_or_sync(0xFFFFFFFFu, lane >= 16 ? x : 0u);
-        if (lane == j) mine.w[h] = uint64_t(lo) | (uint64_t(hi) << 32);
-      }
-    }
-    if (lane < wcnt) {
-      const uint64_t i = b0 + wl0 + lane;
-      st_key<NW>(keys, i, mine);
+      key.w[NW - 1] &= kmask_hi;
+      if (lbad) bad = 1;
+      st_key<NW>(keys, line, key);
       if constexpr (FUSE) {
         uint32_t a, b;
-        lmins<NW>(mine, k, l, seed, nullptr, a, b);
+        lmins<NW>(key, k, l, seed, nullptr, a, b);
         a = bucket_of(a, bbits);
         b = bucket_of(b, bbits);
-        b1[i] = a;
-        b2[i] = b;
+        b1[line] = a;
+        b2[line] = b;
         atomicAdd(counts + a, 1u);
         if (a != b) atomicAdd(counts + b, 1u);
       }
     }
     __syncthreads();
   }
-  if (bad && lane == 0) atomicOr(err, starts ? ERR_LINE : ERR_LAYOUT);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(err, starts ? ERR_LINE : ERR_LAYOUT);
 }
 
 // Line starts for the general layout: '\n' positions in [body, end).
@@ -325,57 +374,123 @@ __global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Co
 
 // ================================================================= scatter
 
-// Write every k-mer into its prefix bucket (role P) and, when its suffix
-// minimizer lands in another bucket, a second copy into that bucket (role S)
-// ("partition by lmins" + "write kmers", lmin_buckets.h:357-407).  The two
+// Every k-mer goes to its prefix bucket (role P) and, when its suffix
+// minimizer lands in another bucket, a second copy goes to that bucket (role
+// S) ("partition by lmins" + "write kmers", lmin_buckets.h:357-407).  The two
 // copies of a cross k-mer share one cross index; in edges mode every copy
 // carries the k-mer's id instead.
+//
+// Two levels keep the write frontier inside L2: level 1 groups the copies
+// into 2^mcb coarse partitions (high bucket bits) with one reservation per
+// block and partition; level 2 places each coarse partition's copies into its
+// 2^fb fine buckets with shared-memory cursors.  A coarse partition occupies
+// exactly the final positions of its buckets, so level 1 writes its records
+// into the same index range of a staging array.
+constexpr int SC_CHUNK = 8192;  // k-mers per level-1 block pass
+
+__global__ void k_coarse_init(const unsigned long long* __restrict__ boff, uint32_t fb, uint32_t mc,
+                              unsigned long long* __restrict__ ccur) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < mc; j += gridDim.x * blockDim.x)
+    ccur[j] = boff[uint64_t(j) << fb];
+}
+
 template <int NW>
-__global__ void __launch_bounds__(256) k_scatter(const uint64_t* __restrict__ keys,
-                                                 const uint32_t* __restrict__ b1,
-                                                 const uint32_t* __restrict__ b2, uint64_t n,
-                                                 unsigned long long* __restrict__ cursor,
-                                                 uint64_t* __restrict__ pkeys,
-                                                 uint32_t* __restrict__ plink, int ids_mode,
-                                                 Counters* ctr) {
+__global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ b1,
+                                                        const uint32_t* __restrict__ b2, uint64_t n,
+                                                        uint32_t fb, uint32_t mc,
+                                                        unsigned long long* __restrict__ ccur,
+                                                        uint64_t* __restrict__ rkey, uint32_t* __restrict__ rlink,
+                                                        uint32_t* __restrict__ rbkt, int ids_mode, Counters* ctr) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  unsigned long long* base = reinterpret_cast<unsigned long long*>(sm_raw);  // [mc]
+  uint32_t* hist = reinterpret_cast<uint32_t*>(base + mc);                   // [mc]
   const int lane = threadIdx.x & 31;
-  for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < n;
-       base += uint64_t(gridDim.x) * blockDim.x) {
-    const uint64_t i = base + threadIdx.x;
-    const bool live = i < n;
-    uint32_t a = 0, b = 0;
-    Key<NW> key;
-    if (live) {
-      key = ld_key<NW>(keys, i);
-      a = b1[i];
-      b = b2[i];
+  for (uint64_t c0 = uint64_t(blockIdx.x) * SC_CHUNK; c0 < n; c0 += uint64_t(gridDim.x) * SC_CHUNK) {
+    const uint64_t c1 = min(n, c0 + SC_CHUNK);
+    for (uint32_t j = threadIdx.x; j < mc; j += blockDim.x) hist[j] = 0;
+    __syncthreads();
+    for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
+      const uint32_t a = b1[i], b = b2[i];
+      atomicAdd(hist + (a >> fb), 1u);
+      if (a != b) atomicAdd(hist + (b >> fb), 1u);
     }
-    const bool cross = live && (a != b);
-    uint32_t x = NONE;
-    if (!ids_mode) {
-      const uint32_t m = __ballot_sync(0xFFFFFFFFu, cross);
-      uint32_t basex = 0;
-      if (m) {
-        if (lane == __ffs(m) - 1) basex = atomicAdd(&ctr->cross_count, uint32_t(__popc(m)));
-        basex = __shfl_sync(0xFFFFFFFFu, basex, __ffs(m) - 1);
+    __syncthreads();
+    for (uint32_t j = threadIdx.x; j < mc; j += blockDim.x) {
+      const uint32_t h = hist[j];
+      base[j] = h ? atomicAdd(ccur + j, (unsigned long long)h) : 0ull;
+      hist[j] = 0;
+    }
+    __syncthreads();
+    for (uint64_t i0 = c0; i0 < c1; i0 += blockDim.x) {
+      const uint64_t i = i0 + threadIdx.x;
+      const bool live = i < c1;
+      uint32_t a = 0, b = 0;
+      Key<NW> key;
+      if (live) {
+        key = ld_key<NW>(keys, i);
+        a = b1[i];
+        b = b2[i];
       }
-      if (cross) x = basex + __popc(m & ((1u << lane) - 1u));
-    }
-    if (live) {
-      const uint32_t link = ids_mode ? uint32_t(i) : x;
-      Key<NW> kp = key;
-      kp.w[NW - 1] |= ROLE_P | (cross ? 0ull : ROLE_S);
-      const uint64_t p = atomicAdd(cursor + a, 1ull);
-      st_key<NW>(pkeys, p, kp);
-      plink[p] = link;
-      if (cross) {
-        Key<NW> ks = key;
-        ks.w[NW - 1] |= ROLE_S;
-        const uint64_t q = atomicAdd(cursor + b, 1ull);
-        st_key<NW>(pkeys, q, ks);
-        plink[q] = link;
+      const bool cross = live && (a != b);
+      uint32_t x = NONE;
+      if (!ids_mode) {
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, cross);
+        uint32_t bx = 0;
+        if (m) {
+          if (lane == __ffs(m) - 1) bx = atomicAdd(&ctr->cross_count, uint32_t(__popc(m)));
+          bx = __shfl_sync(0xFFFFFFFFu, bx, __ffs(m) - 1);
+        }
+        if (cross) x = bx + __popc(m & ((1u << lane) - 1u));
+      }
+      if (live) {
+        const uint32_t link = ids_mode ? uint32_t(i) : x;
+        Key<NW> kp = key;
+        kp.w[NW - 1] |= ROLE_P | (cross ? 0ull : ROLE_S);
+        const uint64_t p = base[a >> fb] + atomicAdd(hist + (a >> fb), 1u);
+        st_key<NW>(rkey, p, kp);
+        rlink[p] = link;
+        rbkt[p] = a;
+        if (cross) {
+          Key<NW> ks = key;
+          ks.w[NW - 1] |= ROLE_S;
+          const uint64_t q = base[b >> fb] + atomicAdd(hist + (b >> fb), 1u);
+          st_key<NW>(rkey, q, ks);
+          rlink[q] = link;
+          rbkt[q] = b;
+        }
       }
     }
+    __syncthreads();
+  }
+}
+
+template <int NW>
+__global__ void __launch_bounds__(512) k_scatter_fine(const uint64_t* __restrict__ rkey,
+                                                      const uint32_t* __restrict__ rlink,
+                                                      const uint32_t* __restrict__ rbkt,
+                                                      const unsigned long long* __restrict__ boff, uint32_t fb,
+                                                      uint32_t mc, uint64_t* __restrict__ pkeys,
+                                                      uint32_t* __restrict__ plink) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  const uint32_t F = 1u << fb;
+  unsigned long long* off = reinterpret_cast<unsigned long long*>(sm_raw);  // [F]
+  uint32_t* cur = reinterpret_cast<uint32_t*>(off + F);                      // [F]
+  for (uint32_t c = blockIdx.x; c < mc; c += gridDim.x) {
+    const uint64_t b0 = uint64_t(c) << fb;
+    for (uint32_t j = threadIdx.x; j < F; j += blockDim.x) {
+      off[j] = boff[b0 + j];
+      cur[j] = 0;
+    }
+    __syncthreads();
+    const uint64_t lo = boff[b0], hi = boff[b0 + F];
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      const uint32_t f = rbkt[i] & (F - 1u);
+      const uint64_t p = off[f] + atomicAdd(cur + f, 1u);
+      st_key<NW>(pkeys, p, ld_key<NW>(rkey, i));
+      plink[p] = rlink[i];
+    }
+    __syncthreads();
   }
 }
 
@@ -1374,11 +1489,19 @@ static int bucket_offsets(Env& e, const Front& f, uint64_t M, uint64_t& copies) 
   return UC_OK;
 }
 
-// tile plan + scatter of every k-mer into its bucket(s).
+// Level split of the scatter: 2^mcb coarse partitions of 2^fb buckets.
+static void scatter_split(uint32_t bbits, uint32_t& mcb, uint32_t& fb) {
+  mcb = std::max<int>(int(bbits) - 12, int(std::min<uint32_t>(bbits, 8)));
+  fb = bbits - mcb;
+}
+
+static size_t scatter_stage_bytes(uint64_t copies, int nw) { return copies * (8ull * nw + 8ull); }
+
+// tile plan + scatter of every k-mer into its bucket(s).  stage: staging
+// records for level 1 (scatter_stage_bytes).
 static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, int nw, int ids_mode,
-                            uint64_t* pkeys, uint32_t* plink) {
+                            uint64_t* pkeys, uint32_t* plink, char* stage, uint64_t copies) {
   const uint64_t M = P.M;
-  UC_CK(cudaMemcpyAsync(f.cursor, f.boff, M * 8, cudaMemcpyDeviceToDevice, e.stream));
   const int gm = grid_for(e, M, 256);
   e.launches += 2 + 6;
   k_tile_flags<<<gm, 256, 0, e.stream>>>(f.counts, f.boff, uint32_t(M), P.win, P.small, f.flag);
@@ -1386,10 +1509,35 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
   k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), f.tile_begin, e.ctr);
   UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
   if (n > 0) {
-    const int grid = grid_for(e, n, 256);
-    ++e.launches;
-    if (nw == 1) k_scatter<1><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, pkeys, plink, ids_mode, e.ctr);
-    else k_scatter<2><<<grid, 256, 0, e.stream>>>(f.keys, f.b1, f.b2, n, f.cursor, pkeys, plink, ids_mode, e.ctr);
+    uint32_t mcb, fb;
+    scatter_split(P.bbits, mcb, fb);
+    const uint32_t mc = 1u << mcb;
+    uint64_t* rkey = reinterpret_cast<uint64_t*>(stage);
+    uint32_t* rlink = reinterpret_cast<uint32_t*>(stage + copies * 8ull * nw);
+    uint32_t* rbkt = rlink + copies;
+    // coarse cursors: the first position of each coarse partition
+    e.launches += 1;
+    k_coarse_init<<<grid_for(e, mc, 256), 256, 0, e.stream>>>(f.boff, fb, mc, f.cursor);
+    const size_t sm1 = size_t(mc) * 12;
+    const size_t sm2 = (size_t(1) << fb) * 12;
+    if (sm1 > 48 * 1024) {
+      UC_CK(cudaFuncSetAttribute(k_scatter_coarse<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
+      UC_CK(cudaFuncSetAttribute(k_scatter_coarse<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
+    }
+    if (sm2 > 48 * 1024) {
+      UC_CK(cudaFuncSetAttribute(k_scatter_fine<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm2)));
+      UC_CK(cudaFuncSetAttribute(k_scatter_fine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm2)));
+    }
+    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + SC_CHUNK - 1) / SC_CHUNK, uint64_t(e.sm_count) * 8)));
+    const int g2 = int(std::max<uint32_t>(1, std::min<uint32_t>(mc, uint32_t(e.sm_count) * 4)));
+    e.launches += 2;
+    if (nw == 1) {
+      k_scatter_coarse<1><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
+      k_scatter_fine<1><<<g2, 512, sm2, e.stream>>>(rkey, rlink, rbkt, f.boff, fb, mc, pkeys, plink);
+    } else {
+      k_scatter_coarse<2><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
+      k_scatter_fine<2><<<g2, 512, sm2, e.stream>>>(rkey, rlink, rbkt, f.boff, fb, mc, pkeys, plink);
+    }
     UC_CK(cudaGetLastError());
   }
   ++e.launches;
@@ -1475,12 +1623,13 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   uint64_t copies = 0;
   r = bucket_offsets(e, f, P.M, copies);
   if (r) return r;
-  r = e.reserve(1, copies * (8 * nw + 4) + 1024);
+  r = e.reserve(1, copies * (8 * nw + 4) + scatter_stage_bytes(copies, nw) + 4096);
   if (r) return r;
   uint64_t* pkeys = static_cast<uint64_t*>(e.take(1, copies * 8 * nw));
   uint32_t* plink = static_cast<uint32_t*>(e.take(1, copies * 4));
-  if (!plink) return e.fail(UC_EBUDGET, "back arena overflow");
-  r = plan_and_scatter(e, f, P, n, nw, 1, pkeys, plink);
+  char* stage = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  if (!stage) return e.fail(UC_EBUDGET, "back arena overflow");
+  r = plan_and_scatter(e, f, P, n, nw, 1, pkeys, plink, stage, copies);
   if (r) return r;
   TileParams tp{};
   tp.pkeys = pkeys;
@@ -1661,6 +1810,7 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   add(S * 4); add(S * 4); add(S * 4); add(S * 4); add(S * 4);  // next, prev, w, act0, act1
   add(S * 4); add(S * 4); add(S * 8); add((S + 1) * 8); add(S); // llen, hlen, X, loff, oncyc
   add(scan_tmp_elems(S) * 8); add(8); add(R * 4);
+  add(scatter_stage_bytes(copies, nw));
   r = e.reserve(1, back);
   if (r) return r;
   auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
@@ -1687,8 +1837,9 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   unsigned long long* stmp = T64(scan_tmp_elems(S));
   unsigned long long* dtotal = T64(1);
   uint32_t* rcnt = T32(R);
-  if (!rcnt) return e.fail(UC_EBUDGET, "back arena overflow");
-  r = plan_and_scatter(e, f, P, n, nw, 0, pkeys, plink);
+  char* stage = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  if (!stage) return e.fail(UC_EBUDGET, "back arena overflow");
+  r = plan_and_scatter(e, f, P, n, nw, 0, pkeys, plink, stage, copies);
   if (r) return r;
   cudaEventRecord(e.ev[2], e.stream);
 
