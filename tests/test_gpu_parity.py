@@ -191,3 +191,53 @@ def test_fused_matches_reference_checksum(comp, name, entry):
     lines = fused_lines(comp, text, entry["k"], entry["l"])
     assert len(lines) == entry["n_lines"]
     assert digest(lines) == entry["sha256_sorted_lines"]
+
+
+@pytest.mark.parametrize("cfg", ["small_plain", "wide_k63", "k47"])
+def test_hec_contraction_matches_oracle(comp, oracle, texts, cfg):
+    """HEC matching rounds (coarsen_HEC + parallel_map_construct) give the
+    same (head, rank) as the oracle's path walk."""
+    from unitigcoarsening_b200 import CONTRACT_HEC, as_u32
+    text, k = texts[cfg]
+    words = oracle.parse(text, k)
+    keys = comp.load_kmers(dev(text), k)
+    succ, pred = comp.assemble_pruned_graph(keys, k, min(8, k - 1))
+    head, rank, cyc = comp.coarsen_de_bruijn_full_cycle(keys, succ, pred, k, method=CONTRACT_HEC)
+    osucc, opred = oracle.edges(words, k)
+    ohead, orank, ocyc = oracle.contract(words, k, osucc, opred)
+    assert np.array_equal(as_u32(head), ohead) and np.array_equal(as_u32(rank), orank)
+    assert cyc == ocyc
+
+
+@pytest.mark.parametrize("cfg", ["small_plain", "scale_sample", "wide_k63"])
+def test_fused_hec_stitch_matches_oracle(comp, oracle, texts, cfg):
+    from unitigcoarsening_b200 import CONTRACT_HEC
+    text, k = texts[cfg]
+    want, _, _ = oracle.compact(text, k)
+    comp.set_tuning(contract_method=CONTRACT_HEC)
+    try:
+        assert fused_lines(comp, text, k, min(8, k - 1)) == sorted_lines(want)
+    finally:
+        comp.set_tuning(contract_method=0)
+
+
+@pytest.mark.parametrize("k", [31, 63])
+def test_hec_with_cycles(comp, oracle, k):
+    from unitigcoarsening_b200 import CONTRACT_HEC, as_u32
+    km = cyclic_kmers(300, k, seed=k + 1) + cyclic_kmers(2, k, seed=k + 2)[:0] + walk_kmers(
+        distinct_path(200, k, seed=5 * k), k)
+    text = text_of(shuffled(km, 9))
+    want, _, ocyc = oracle.compact(text, k)
+    comp.set_tuning(contract_method=CONTRACT_HEC, tile_capacity=256, bucket_bits=6)
+    try:
+        assert fused_lines(comp, text, k, 6) == sorted_lines(want)
+    finally:
+        comp.set_tuning(contract_method=0, tile_capacity=0, bucket_bits=0)
+    words = oracle.parse(text, k)
+    keys = comp.load_kmers(dev(text), k)
+    succ, pred = comp.assemble_pruned_graph(keys, k, 6)
+    head, rank, cyc = comp.coarsen_de_bruijn_full_cycle(keys, succ, pred, k, method=CONTRACT_HEC)
+    osucc, opred = oracle.edges(words, k)
+    ohead, orank, _ = oracle.contract(words, k, osucc, opred)
+    assert np.array_equal(as_u32(head), ohead) and np.array_equal(as_u32(rank), orank)
+    assert cyc == ocyc == 1

@@ -191,6 +191,10 @@ uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
     c->env.err = "tile_threads must be 256, 512 or 1024";
     return UC_EINPUT;
   }
+  if (t->contract_method != UC_CONTRACT_POINTER_JUMP && t->contract_method != UC_CONTRACT_HEC) {
+    c->env.err = "contract_method must be UC_CONTRACT_POINTER_JUMP or UC_CONTRACT_HEC";
+    return UC_EINPUT;
+  }
   if (t->bucket_bits > 24) {
     c->env.err = "bucket_bits must be <= 24";
     return UC_EINPUT;

@@ -1097,6 +1097,227 @@ __global__ void k_add_cursor(Counters* ctr, const unsigned long long* total) {
   ctr->out_cursor += *total;
 }
 
+// ===================================================== HEC contraction
+//
+// Heavy-edge coarsening over a set of paths (and rare cycles), restating the
+// reference's round loop (coarsen_de_bruijn_full_cycle, coarseners.h:437-485):
+// every node with a predecessor wants to merge with it, a head wants its
+// successor, an isolated node is a finished chain (coarsen_HEC,
+// heuristics.h:224-245); two compare-and-swaps pair a node with its choice or
+// let it join the choice's aggregate (parallel_map_construct,
+// heuristics.h:106-203, with bounded retries and a singleton fallback instead
+// of unbounded spins); aggregates become the next level's nodes
+// (coarsen_de_bruijn_graph, coarseners.h:68-92).  Members are ordered by
+// walking from the aggregate's first member (instead of the O(m^2) sort of
+// transpose_and_sort, coarseners.h:182-235) and their offsets are composed
+// top-down (instead of copying member lists, compact_graph.h:55-112).
+// Levels live in one node pool; level r occupies [lb[r], lb[r] + ln[r]).
+// Kernels read the level sizes on the device, so every round is enqueued
+// without host round trips.
+constexpr uint32_t HV_UNSET = 0xFFFFFFFFu, HV_LOCK = 0xFFFFFFFEu, HV_FIN = 0xFFFFFFFDu, HV_CYC = 0xFFFFFFFCu;
+constexpr uint32_t HP_SENT = 0xFFFFFFFBu;  // coarse node not yet given a first member
+
+struct HecPool {
+  uint32_t *prv, *nxt, *wt, *hn, *vc, *agg, *loc, *first0;
+  uint32_t* lb;  // [R+1] level base
+  uint32_t* ln;  // [R+1] level size
+  uint32_t cap;
+  Counters* ctr;
+};
+
+__global__ void k_hec_level0(HecPool h, const uint32_t* __restrict__ prev, const uint32_t* __restrict__ next,
+                             const uint32_t* __restrict__ w, uint64_t n, const Counters* nctr) {
+  const uint64_t N = nctr ? uint64_t(nctr->seg_count) : n;
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    h.lb[0] = 0;
+    h.ln[0] = uint32_t(N);
+  }
+  for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < N; u += uint64_t(gridDim.x) * blockDim.x) {
+    h.prv[u] = prev[u];
+    h.nxt[u] = next[u];
+    h.wt[u] = w ? w[u] : 1u;
+    h.first0[u] = uint32_t(u);
+  }
+}
+
+// choice (hn) per node; isolated nodes are finished chains; a node whose
+// predecessor is still the sentinel is a whole cycle collapsed into one
+__global__ void k_hec_prep(HecPool h, int r) {
+  const uint32_t b = h.lb[r], N = h.ln[r];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const uint32_t u = b + j;
+    const uint32_t pv = h.prv[u], nx = h.nxt[u];
+    if (pv == HP_SENT) {
+      h.hn[u] = NONE;
+      h.vc[u] = HV_CYC;
+    } else if (pv == u) {  // a one-node cycle
+      h.hn[u] = NONE;
+      h.vc[u] = HV_CYC;
+    } else {
+      const uint32_t c = (pv != NONE) ? pv : nx;
+      h.hn[u] = c;
+      h.vc[u] = (c == NONE) ? HV_FIN : HV_UNSET;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    h.lb[r + 1] = b + N;
+    h.ln[r + 1] = 0;
+  }
+}
+
+// One pass of the two-CAS pairing.  A label is the pool index of the
+// aggregate's root.  Pass 1 gives up after 10 tries when u > v (the
+// reference's deadlock break, heuristics.h:142-146); pass 2 retries the rest
+// a bounded number of times and then leaves u a singleton aggregate.
+__global__ void k_hec_match(HecPool h, int r, int pass) {
+  const uint32_t b = h.lb[r], N = h.ln[r];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const uint32_t u = b + j;
+    const uint32_t v = h.hn[u];
+    if (v == NONE) continue;
+    if (pass == 2 && atomicAdd(h.vc + u, 0u) != HV_UNSET) continue;
+    bool done = false;
+    const int limit = (pass == 1) ? 64 : 256;
+    for (int it = 0; it < limit && !done; ++it) {
+      if (atomicCAS(h.vc + u, HV_UNSET, HV_LOCK) == HV_UNSET) {
+        if (atomicCAS(h.vc + v, HV_UNSET, HV_LOCK) == HV_UNSET) {
+          atomicExch(h.vc + v, u);
+          atomicExch(h.vc + u, u);
+          done = true;
+        } else {
+          const uint32_t lv = atomicAdd(h.vc + v, 0u);
+          if (lv < HV_CYC) {  // v already labelled: join its aggregate
+            atomicExch(h.vc + u, lv);
+            done = true;
+          } else {
+            atomicExch(h.vc + u, HV_UNSET);  // release and retry
+          }
+        }
+      } else {
+        done = true;  // u is labelled (or being labelled) by a neighbour
+      }
+      if (pass == 1 && it > 10 && u > v) break;
+    }
+    if (pass == 2 && !done) atomicCAS(h.vc + u, HV_UNSET, u);  // singleton
+  }
+}
+
+// Roots (label == self) take the next level's pool slots; the root's hn
+// holds its new index afterwards.
+__global__ void k_hec_roots(HecPool h, int r) {
+  const uint32_t b = h.lb[r], N = h.ln[r];
+  const uint32_t nb = h.lb[r + 1];
+  const int lane = threadIdx.x & 31;
+  for (uint32_t j0 = blockIdx.x * blockDim.x; j0 < N; j0 += gridDim.x * blockDim.x) {
+    const uint32_t j = j0 + threadIdx.x;
+    const uint32_t u = b + j;
+    const bool root = (j < N) && (h.vc[u] == u);
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, root);
+    uint32_t base = 0;
+    if (m) {
+      if (lane == __ffs(m) - 1) base = atomicAdd(h.ln + r + 1, uint32_t(__popc(m)));
+      base = __shfl_sync(0xFFFFFFFFu, base, __ffs(m) - 1);
+    }
+    if (root) {
+      const uint32_t a = nb + base + __popc(m & ((1u << lane) - 1u));
+      if (a >= h.cap) {
+        atomicOr(&h.ctr->err, ERR_CAPACITY);
+      } else {
+        h.hn[u] = a;
+        h.prv[a] = HP_SENT;
+        h.nxt[a] = NONE;
+        h.wt[a] = 0;
+        h.first0[a] = NONE;
+      }
+    }
+  }
+}
+
+__global__ void k_hec_assign(HecPool h, int r) {
+  const uint32_t b = h.lb[r], N = h.ln[r];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const uint32_t u = b + j;
+    const uint32_t c = h.vc[u];
+    h.agg[u] = (c < HV_CYC) ? h.hn[c] : NONE;
+  }
+}
+
+// The first member of each aggregate (predecessor outside it) walks its
+// members along next: local offsets, total weight, coarse neighbours.
+__global__ void k_hec_order(HecPool h, int r) {
+  const uint32_t b = h.lb[r], N = h.ln[r];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const uint32_t u = b + j;
+    const uint32_t A = h.agg[u];
+    if (A == NONE || A >= h.cap) continue;
+    const uint32_t pv = h.prv[u];
+    if (pv != NONE && h.agg[pv] == A) continue;  // not the first member
+    uint32_t off = 0, m = u, last = u;
+    for (uint32_t guard = 0; guard < N; ++guard) {
+      h.loc[m] = off;
+      off += h.wt[m];
+      last = m;
+      const uint32_t nx = h.nxt[m];
+      if (nx == NONE || h.agg[nx] != A) break;
+      m = nx;
+    }
+    h.wt[A] = off;
+    h.first0[A] = h.first0[u];
+    h.nxt[A] = (h.nxt[last] == NONE) ? NONE : h.agg[h.nxt[last]];
+    h.prv[A] = (pv == NONE) ? NONE : h.agg[pv];
+  }
+}
+
+// Top-down: (head, offset) of every node from its aggregate's, stored in
+// (hn, loc).  A finished node is a whole chain headed by its first member; a
+// cycle node marks its members with head NONE.
+__global__ void k_hec_down(HecPool h, int r) {
+  const uint32_t b = h.lb[r], N = h.ln[r];
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < N; j += gridDim.x * blockDim.x) {
+    const uint32_t u = b + j;
+    const uint32_t c = h.vc[u];
+    uint32_t hd, of;
+    if (c == HV_FIN) {
+      hd = h.first0[u];
+      of = 0;
+    } else if (c == HV_CYC) {
+      hd = NONE;
+      of = 0;
+    } else {
+      const uint32_t A = h.agg[u];
+      hd = (A == NONE || A >= h.cap) ? NONE : h.hn[A];
+      of = (hd == NONE) ? 0 : h.loc[A] + h.loc[u];
+    }
+    h.hn[u] = hd;
+    h.loc[u] = of;
+  }
+}
+
+// Level-0 results into the (pointer | HEAD_BIT, offset) form of the ranking.
+__global__ void k_hec_emit(HecPool h, unsigned long long* __restrict__ X, uint8_t* __restrict__ oncycle) {
+  const uint32_t N = h.ln[0];
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < N; s += gridDim.x * blockDim.x) {
+    const uint32_t hd = h.hn[s];
+    if (hd == NONE) {
+      X[s] = pk(s, 0);
+      if (oncycle) oncycle[s] = 1;
+    } else {
+      X[s] = pk(hd == s ? (hd | HEAD_BIT) : hd, h.loc[s]);
+    }
+  }
+}
+
+__global__ void k_cycle_list(const uint8_t* __restrict__ oncycle, uint64_t n, const Counters* nctr,
+                             uint32_t* __restrict__ act, uint32_t* __restrict__ cnt) {
+  const uint64_t N = nctr ? uint64_t(nctr->seg_count) : n;
+  for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < N; s += uint64_t(gridDim.x) * blockDim.x)
+    if (oncycle[s]) act[atomicAdd(cnt, 1u)] = uint32_t(s);
+}
+
+__global__ void k_hec_check(HecPool h, int R) {
+  if (h.ln[R] != 0) atomicOr(&h.ctr->err, ERR_TIMEOUT);
+}
+
 // ======================================================= phase-API helpers
 
 __global__ void k_head_rank(const unsigned long long* __restrict__ X, uint64_t n,
@@ -1675,13 +1896,114 @@ static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t 
   return UC_OK;
 }
 
+static size_t hec_bytes(uint64_t nmax, uint32_t R) {
+  const uint64_t cap = 2 * nmax + 64;
+  return 8 * ((cap * 4 + 255) & ~uint64_t(255)) + 2 * 256 + 2 * (R + 1) * 4 + 1024;
+}
+
+static int hec_take(Env& e, uint64_t nmax, uint32_t R, HecPool& h) {
+  const uint64_t cap = 2 * nmax + 64;
+  uint32_t** arr[8] = {&h.prv, &h.nxt, &h.wt, &h.hn, &h.vc, &h.agg, &h.loc, &h.first0};
+  for (auto a : arr) *a = static_cast<uint32_t*>(e.take(1, cap * 4));
+  h.lb = static_cast<uint32_t*>(e.take(1, (R + 1) * 4));
+  h.ln = static_cast<uint32_t*>(e.take(1, (R + 1) * 4));
+  h.cap = uint32_t(std::min<uint64_t>(cap, 0xFFFFFFF0ull));
+  h.ctr = e.ctr;
+  if (!h.ln) return e.fail(UC_EBUDGET, "arena overflow (HEC pool)");
+  return UC_OK;
+}
+
+static uint32_t hec_rounds(uint64_t nmax) {
+  uint32_t r = 8;
+  for (uint64_t t = 1; t < nmax; t <<= 1) r += 2;
+  return r;
+}
+
+// HEC contraction of the lists (prev, next, w) into X (pointer | HEAD_BIT,
+// offset) and cycle flags, all rounds enqueued on the stream.
+static void hec_contract(Env& e, HecPool& h, uint32_t R, const uint32_t* prev, const uint32_t* next,
+                         const uint32_t* w, uint64_t nmax, bool count_on_device, unsigned long long* X,
+                         uint8_t* oncycle) {
+  const int grid = grid_for(e, nmax ? nmax : 1, 256);
+  cudaMemsetAsync(h.ln, 0, (R + 1) * 4, e.stream);
+  ++e.launches;
+  k_hec_level0<<<grid, 256, 0, e.stream>>>(h, prev, next, w, nmax, count_on_device ? e.ctr : nullptr);
+  for (uint32_t r = 0; r < R; ++r) {
+    e.launches += 6;
+    k_hec_prep<<<grid, 256, 0, e.stream>>>(h, int(r));
+    k_hec_match<<<grid, 256, 0, e.stream>>>(h, int(r), 1);
+    k_hec_match<<<grid, 256, 0, e.stream>>>(h, int(r), 2);
+    k_hec_roots<<<grid, 256, 0, e.stream>>>(h, int(r));
+    k_hec_assign<<<grid, 256, 0, e.stream>>>(h, int(r));
+    k_hec_order<<<grid, 256, 0, e.stream>>>(h, int(r));
+  }
+  e.launches += 1 + R + 1;
+  k_hec_check<<<1, 1, 0, e.stream>>>(h, int(R));
+  for (int r = int(R) - 1; r >= 0; --r) k_hec_down<<<grid, 256, 0, e.stream>>>(h, r);
+  k_hec_emit<<<grid, 256, 0, e.stream>>>(h, X, oncycle);
+}
+
+static int contract_hec(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* pred, uint64_t n,
+                        int k, uint32_t* head, uint32_t* rank, uint64_t& ncyc, bool& fell_back) {
+  fell_back = false;
+  e.reset();
+  const uint32_t R = hec_rounds(n);
+  int r = e.reserve(1, hec_bytes(n, R) + n * (8 + 4 + 1) + 8 + 4096);
+  if (r) return r;
+  HecPool h{};
+  r = hec_take(e, n, R, h);
+  if (r) return r;
+  unsigned long long* X = static_cast<unsigned long long*>(e.take(1, n * 8));
+  uint32_t* act = static_cast<uint32_t*>(e.take(1, n * 4));
+  uint8_t* flag = static_cast<uint8_t*>(e.take(1, n));
+  uint32_t* cnt = static_cast<uint32_t*>(e.take(1, 4));
+  unsigned long long* dcyc = static_cast<unsigned long long*>(e.take(1, 8));
+  if (!dcyc) return e.fail(UC_EBUDGET, "arena overflow");
+  UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
+  UC_CK(cudaMemsetAsync(flag, 0, n, e.stream));
+  hec_contract(e, h, R, pred, succ, nullptr, n, false, X, flag);
+  e.launches += 2;
+  k_head_rank<<<grid_for(e, n, 256), 256, 0, e.stream>>>(X, n, head, rank);
+  UC_CK(cudaMemsetAsync(cnt, 0, 4, e.stream));
+  k_cycle_list<<<grid_for(e, n, 256), 256, 0, e.stream>>>(flag, n, nullptr, act, cnt);
+  uint32_t hleft = 0;
+  UC_CK(cudaMemcpyAsync(&hleft, cnt, 4, cudaMemcpyDeviceToHost, e.stream));
+  r = e.read_ctr();
+  if (r) return r;
+  if (e.h_ctr->err) {
+    fell_back = true;
+    UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
+    e.reset();
+    return UC_OK;
+  }
+  ncyc = 0;
+  if (hleft) {
+    UC_CK(cudaMemsetAsync(flag, 0, n, e.stream));
+    UC_CK(cudaMemsetAsync(dcyc, 0, 8, e.stream));
+    ++e.launches;
+    if (k <= 31) k_vertex_cycles<1><<<1, 1, 0, e.stream>>>(act, hleft, succ, d_keys, n, head, rank, flag, dcyc);
+    else k_vertex_cycles<2><<<1, 1, 0, e.stream>>>(act, hleft, succ, d_keys, n, head, rank, flag, dcyc);
+    unsigned long long hc = 0;
+    UC_CK(cudaMemcpyAsync(&hc, dcyc, 8, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    ncyc = hc;
+  }
+  e.reset();
+  return UC_OK;
+}
+
 int contract(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* pred, uint64_t n, int k,
              int method, uint32_t* head, uint32_t* rank, uint64_t& ncyc) {
-  (void)method;
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
   if (n >= 0x7FFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 31-bit ids");
   ncyc = 0;
   if (n == 0) return UC_OK;
+  if (method == UC_CONTRACT_HEC) {
+    bool fell_back = false;
+    const int r = contract_hec(e, d_keys, succ, pred, n, k, head, rank, ncyc, fell_back);
+    if (r || !fell_back) return r;
+    // HEC did not finish inside its pool or rounds: pointer jumping instead
+  }
   e.reset();
   int r = e.reserve(1, n * (8 + 4 + 4 + 1) + 64 * 8 + 4096);
   if (r) return r;
@@ -1811,6 +2133,9 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   add(S * 4); add(S * 4); add(S * 8); add((S + 1) * 8); add(S); // llen, hlen, X, loff, oncyc
   add(scan_tmp_elems(S) * 8); add(8); add(R * 4);
   add(scatter_stage_bytes(copies, nw));
+  const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
+  const uint32_t RH = hec_rounds(S);
+  if (want_hec) add(hec_bytes(S, RH));
   r = e.reserve(1, back);
   if (r) return r;
   auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
@@ -1839,6 +2164,11 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   uint32_t* rcnt = T32(R);
   char* stage = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
   if (!stage) return e.fail(UC_EBUDGET, "back arena overflow");
+  HecPool hp{};
+  if (want_hec) {
+    r = hec_take(e, S, RH, hp);
+    if (r) return r;
+  }
   r = plan_and_scatter(e, f, P, n, nw, 0, pkeys, plink, stage, copies);
   if (r) return r;
   cudaEventRecord(e.ev[2], e.stream);
@@ -1878,11 +2208,32 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
     e.launches += 1;
     k_seg_link<<<gs, 256, 0, e.stream>>>(e.ctr, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k);
     uint32_t *act = nullptr, *left = nullptr;
-    r = rank_lists(e, prev, wgt, nseg, true, Xr, act0, act1, rcnt, rounds, act, left);
-    if (r) return r;
-    UC_CK(cudaMemsetAsync(oncyc, 0, nseg, e.stream));
-    e.launches += 3 + 6 + 2;
-    k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
+    bool hec = want_hec;
+    if (hec) {
+      // HEC rounds; the cycle segments are listed from the flags
+      UC_CK(cudaMemsetAsync(oncyc, 0, nseg, e.stream));
+      hec_contract(e, hp, RH, prev, next, wgt, nseg, true, Xr, oncyc);
+      UC_CK(cudaMemsetAsync(rcnt, 0, 4, e.stream));
+      ++e.launches;
+      k_cycle_list<<<gs, 256, 0, e.stream>>>(oncyc, nseg, e.ctr, act0, rcnt);
+      act = act0;
+      left = rcnt;
+      rounds = RH;
+      r = e.read_ctr();
+      if (r) return r;
+      if (e.h_ctr->err) {  // did not finish in its pool/rounds: pointer jumping
+        UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
+        hec = false;
+      }
+    }
+    if (!hec) {
+      r = rank_lists(e, prev, wgt, nseg, true, Xr, act0, act1, rcnt, rounds, act, left);
+      if (r) return r;
+      UC_CK(cudaMemsetAsync(oncyc, 0, nseg, e.stream));
+      ++e.launches;
+      k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
+    }
+    e.launches += 2 + 6 + 2;
     k_chain_len<<<gs, 256, 0, e.stream>>>(e.ctr, Xr, next, wgt, oncyc, llen);
     k_head_len<<<gs, 256, 0, e.stream>>>(e.ctr, prev, llen, hlen);
     scan_excl<uint32_t, unsigned long long>(hlen, nseg, loff, stmp, e.stream, dtotal);
