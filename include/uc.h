@@ -61,6 +61,7 @@ typedef struct uc_tuning {
     uint32_t bucket_bits;     /* log2 of the bucket count */
     uint32_t load_factor_pct; /* tile hash slots per copy, percent (>=150) */
     uint32_t contract_method; /* UC_CONTRACT_* for the segment stitch */
+    uint32_t warp_capacity;   /* copies per warp tile (32..1024; 1 = no warp tier) */
 } uc_tuning;
 
 /* ---- context --------------------------------------------------------- */

@@ -84,16 +84,24 @@ def test_fused_matches_oracle(comp, oracle, texts, cfg):
     assert got == sorted_lines(want)
 
 
-@pytest.mark.parametrize("cap,bits", [(256, 0), (256, 4), (1024, 12), (2048, 8), (8192, 9)])
-def test_fused_independent_of_tiling(comp, oracle, texts, cap, bits):
+@pytest.mark.parametrize("cap,bits,wcap", [(256, 0, 0), (256, 4, 0), (1024, 12, 0), (2048, 8, 1), (8192, 9, 1),
+                                           (4096, 0, 64), (4096, 14, 32), (4096, 0, 1024), (1024, 0, 512)])
+def test_fused_independent_of_tiling(comp, oracle, texts, cap, bits, wcap):
+    """Same lines whatever the bucketing and whichever tier (warp tiles,
+    block tiles, oversized tiles in global scratch) works each tile."""
     text, k = texts["scale_sample"]
     want, _, _ = oracle.compact(text, k)
-    comp.set_tuning(tile_capacity=cap, bucket_bits=bits)
+    comp.set_tuning(tile_capacity=cap, bucket_bits=bits, warp_capacity=wcap)
     try:
         got = fused_lines(comp, text, k, 8)
+        keys = comp.load_kmers(dev(text), k)
+        succ, pred = comp.assemble_pruned_graph(keys, k, 8)
     finally:
-        comp.set_tuning(tile_capacity=0, bucket_bits=0)
+        comp.set_tuning(tile_capacity=0, bucket_bits=0, warp_capacity=0)
     assert got == sorted_lines(want)
+    from unitigcoarsening_b200 import as_u32
+    osucc, opred = oracle.edges(oracle.parse(text, k), k)
+    assert np.array_equal(as_u32(succ), osucc) and np.array_equal(as_u32(pred), opred)
 
 
 @pytest.mark.parametrize("l", [3, 8, 12, 16])

@@ -60,7 +60,7 @@ class Stats(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("tile_capacity", ctypes.c_uint32), ("tile_threads", ctypes.c_uint32),
                 ("bucket_bits", ctypes.c_uint32), ("load_factor_pct", ctypes.c_uint32),
-                ("contract_method", ctypes.c_uint32)]
+                ("contract_method", ctypes.c_uint32), ("warp_capacity", ctypes.c_uint32)]
 
 
 _lib = None

@@ -195,8 +195,12 @@ uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
     c->env.err = "contract_method must be UC_CONTRACT_POINTER_JUMP or UC_CONTRACT_HEC";
     return UC_EINPUT;
   }
-  if (t->bucket_bits > 24) {
-    c->env.err = "bucket_bits must be <= 24";
+  if (t->warp_capacity > 1 && (t->warp_capacity < 32 || t->warp_capacity > 1024 || t->warp_capacity % 32)) {
+    c->env.err = "warp_capacity must be 0, 1 or a multiple of 32 in [32, 1024]";
+    return UC_EINPUT;
+  }
+  if (t->bucket_bits > 25) {
+    c->env.err = "bucket_bits must be <= 25";
     return UC_EINPUT;
   }
   c->env.tune = *t;

@@ -22,7 +22,9 @@ struct Counters {
   uint32_t active;                   // stitch: active list length
   uint32_t active_next;
   uint32_t err;
-  uint32_t pad[4];
+  uint32_t work_next;                // level-2 scatter work counter
+  uint32_t nwarp, nblock;            // tiles per tier
+  uint32_t wtile_next;
 };
 
 struct TileParams {
@@ -31,6 +33,9 @@ struct TileParams {
   const unsigned long long* tile_begin;  // [ntiles + 1] copy offsets
   Counters* ctr;
   const uint32_t* big_list;     // big-tile launch: tile ids
+  const uint32_t* wlist;        // warp-tier tile ids
+  const uint32_t* blist;        // block-tier tile ids
+  uint32_t wcap, wts, wbytes;   // warp tiles: capacity, hash slots, shared bytes per warp
   char* big_scratch;
   const unsigned long long* big_off;
   int k;

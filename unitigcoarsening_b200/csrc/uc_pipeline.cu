@@ -352,9 +352,11 @@ __global__ void k_tile_write(const uint32_t* __restrict__ flag, const uint32_t* 
   }
 }
 
-__global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Counters* ctr, uint32_t cap,
-                           uint32_t* __restrict__ big_list, unsigned long long* __restrict__ big_size,
-                           int nw) {
+// Sort the tiles into tiers by size: warp tiles, block tiles and oversized
+// tiles (with the global scratch each one needs).
+__global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Counters* ctr, uint32_t wcap,
+                           uint32_t cap, uint32_t* __restrict__ wlist, uint32_t* __restrict__ blist,
+                           uint32_t* __restrict__ big_list, unsigned long long* __restrict__ big_size, int nw) {
   const uint32_t nt = ctr->ntiles;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     const uint64_t c = tile_begin[t + 1] - tile_begin[t];
@@ -363,7 +365,12 @@ __global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Co
       atomicOr(&ctr->err, ERR_INTERNAL);
       continue;
     }
-    if (c > cap) {
+    if (c == 0) continue;
+    if (c <= wcap) {
+      wlist[atomicAdd(&ctr->nwarp, 1u)] = t;
+    } else if (c <= cap) {
+      blist[atomicAdd(&ctr->nblock, 1u)] = t;
+    } else {
       const uint32_t i = atomicAdd(&ctr->nbig, 1u);
       big_list[i] = t;
       const uint64_t ts = uint64_t(pow2_at_least(2 * c));
@@ -380,13 +387,18 @@ __global__ void k_find_big(const unsigned long long* __restrict__ tile_begin, Co
 // copies of a cross k-mer share one cross index; in edges mode every copy
 // carries the k-mer's id instead.
 //
-// Two levels keep the write frontier inside L2: level 1 groups the copies
-// into 2^mcb coarse partitions (high bucket bits) with one reservation per
-// block and partition; level 2 places each coarse partition's copies into its
-// 2^fb fine buckets with shared-memory cursors.  A coarse partition occupies
-// exactly the final positions of its buckets, so level 1 writes its records
-// into the same index range of a staging array.
-constexpr int SC_CHUNK = 8192;  // k-mers per level-1 block pass
+// Two levels keep the write frontier inside L2.  Level 1 groups each block's
+// copies by coarse partition (high bucket bits, at most 256 partitions) in
+// shared memory and writes them out as contiguous runs, one reservation per
+// block and partition.  A coarse partition occupies exactly the final
+// positions of its buckets, so level 1 writes (key, link, bucket) records
+// into the same index range of a staging array; level 2 then walks the
+// staged records in index order - that is, partition by partition - with
+// every block taking the next chunk from a shared counter, and places each
+// record with its bucket's cursor.  All blocks therefore write into the same
+// one or two partitions at any time.
+constexpr int SC_CHUNK = 1024;   // k-mers per level-1 block pass (<= 2048 copies)
+constexpr int SC_FINE = 4096;    // staged records per level-2 work item
 
 __global__ void k_coarse_init(const unsigned long long* __restrict__ boff, uint32_t fb, uint32_t mc,
                               unsigned long long* __restrict__ ccur) {
@@ -403,34 +415,53 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
                                                         uint64_t* __restrict__ rkey, uint32_t* __restrict__ rlink,
                                                         uint32_t* __restrict__ rbkt, int ids_mode, Counters* ctr) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  unsigned long long* base = reinterpret_cast<unsigned long long*>(sm_raw);  // [mc]
-  uint32_t* hist = reinterpret_cast<uint32_t*>(base + mc);                   // [mc]
+  uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);                         // [2*CHUNK*NW]
+  uint32_t* slink = reinterpret_cast<uint32_t*>(skey + 2 * SC_CHUNK * NW);      // [2*CHUNK]
+  uint32_t* sbkt = slink + 2 * SC_CHUNK;                                        // [2*CHUNK]
+  unsigned long long* gbase = reinterpret_cast<unsigned long long*>(sbkt + 2 * SC_CHUNK);  // [mc]
+  uint32_t* hist = reinterpret_cast<uint32_t*>(gbase + mc);                     // [mc]
+  uint32_t* lofs = hist + mc;                                                   // [mc + 1]
+  __shared__ uint32_t sc[33];
   const int lane = threadIdx.x & 31;
   for (uint64_t c0 = uint64_t(blockIdx.x) * SC_CHUNK; c0 < n; c0 += uint64_t(gridDim.x) * SC_CHUNK) {
-    const uint64_t c1 = min(n, c0 + SC_CHUNK);
+    const uint32_t cn = uint32_t((n - c0) < uint64_t(SC_CHUNK) ? (n - c0) : uint64_t(SC_CHUNK));
     for (uint32_t j = threadIdx.x; j < mc; j += blockDim.x) hist[j] = 0;
     __syncthreads();
-    for (uint64_t i = c0 + threadIdx.x; i < c1; i += blockDim.x) {
-      const uint32_t a = b1[i], b = b2[i];
+    // count copies per coarse partition
+    for (uint32_t t = threadIdx.x; t < cn; t += blockDim.x) {
+      const uint32_t a = b1[c0 + t], b = b2[c0 + t];
       atomicAdd(hist + (a >> fb), 1u);
       if (a != b) atomicAdd(hist + (b >> fb), 1u);
     }
     __syncthreads();
-    for (uint32_t j = threadIdx.x; j < mc; j += blockDim.x) {
-      const uint32_t h = hist[j];
-      base[j] = h ? atomicAdd(ccur + j, (unsigned long long)h) : 0ull;
-      hist[j] = 0;
+    // local offsets (scan over the partitions) and global reservations
+    {
+      const uint32_t per = (mc + blockDim.x - 1) / blockDim.x;
+      const uint32_t j0 = min(mc, threadIdx.x * per), j1 = min(mc, j0 + per);
+      uint32_t acc = 0;
+      for (uint32_t j = j0; j < j1; ++j) acc += hist[j];
+      uint32_t tot;
+      uint32_t pre = block_excl_scan(acc, sc, &tot);
+      for (uint32_t j = j0; j < j1; ++j) {
+        const uint32_t h = hist[j];
+        lofs[j] = pre;
+        gbase[j] = h ? atomicAdd(ccur + j, (unsigned long long)h) : 0ull;
+        pre += h;
+        hist[j] = 0;
+      }
+      if (threadIdx.x == 0) lofs[mc] = tot;
     }
     __syncthreads();
-    for (uint64_t i0 = c0; i0 < c1; i0 += blockDim.x) {
-      const uint64_t i = i0 + threadIdx.x;
-      const bool live = i < c1;
+    // place every copy in its partition's run of the staging area
+    for (uint32_t t0 = 0; t0 < cn; t0 += blockDim.x) {
+      const uint32_t t = t0 + threadIdx.x;
+      const bool live = t < cn;
       uint32_t a = 0, b = 0;
       Key<NW> key;
       if (live) {
-        key = ld_key<NW>(keys, i);
-        a = b1[i];
-        b = b2[i];
+        key = ld_key<NW>(keys, c0 + t);
+        a = b1[c0 + t];
+        b = b2[c0 + t];
       }
       const bool cross = live && (a != b);
       uint32_t x = NONE;
@@ -444,53 +475,72 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
         if (cross) x = bx + __popc(m & ((1u << lane) - 1u));
       }
       if (live) {
-        const uint32_t link = ids_mode ? uint32_t(i) : x;
+        const uint32_t link = ids_mode ? uint32_t(c0 + t) : x;
         Key<NW> kp = key;
         kp.w[NW - 1] |= ROLE_P | (cross ? 0ull : ROLE_S);
-        const uint64_t p = base[a >> fb] + atomicAdd(hist + (a >> fb), 1u);
-        st_key<NW>(rkey, p, kp);
-        rlink[p] = link;
-        rbkt[p] = a;
+        const uint32_t sp = lofs[a >> fb] + atomicAdd(hist + (a >> fb), 1u);
+        st_key<NW>(skey, sp, kp);
+        slink[sp] = link;
+        sbkt[sp] = a;
         if (cross) {
           Key<NW> ks = key;
           ks.w[NW - 1] |= ROLE_S;
-          const uint64_t q = base[b >> fb] + atomicAdd(hist + (b >> fb), 1u);
-          st_key<NW>(rkey, q, ks);
-          rlink[q] = link;
-          rbkt[q] = b;
+          const uint32_t sq = lofs[b >> fb] + atomicAdd(hist + (b >> fb), 1u);
+          st_key<NW>(skey, sq, ks);
+          slink[sq] = link;
+          sbkt[sq] = b;
         }
       }
+    }
+    __syncthreads();
+    // write the runs out: consecutive slots of a partition are consecutive
+    // global positions
+    const uint32_t total = lofs[mc];
+    for (uint32_t sl = threadIdx.x; sl < total; sl += blockDim.x) {
+      const uint32_t bk = sbkt[sl];
+      const uint32_t part = bk >> fb;
+      const uint64_t pos = gbase[part] + (sl - lofs[part]);
+      st_key<NW>(rkey, pos, ld_key<NW>(skey, sl));
+      rlink[pos] = slink[sl];
+      rbkt[pos] = bk;
     }
     __syncthreads();
   }
 }
 
+// Level 2: staged records in index order, a chunk per grab.
 template <int NW>
-__global__ void __launch_bounds__(512) k_scatter_fine(const uint64_t* __restrict__ rkey,
+__global__ void __launch_bounds__(256) k_scatter_fine(const uint64_t* __restrict__ rkey,
                                                       const uint32_t* __restrict__ rlink,
-                                                      const uint32_t* __restrict__ rbkt,
-                                                      const unsigned long long* __restrict__ boff, uint32_t fb,
-                                                      uint32_t mc, uint64_t* __restrict__ pkeys,
-                                                      uint32_t* __restrict__ plink) {
-  extern __shared__ __align__(16) unsigned char sm_raw[];
-  const uint32_t F = 1u << fb;
-  unsigned long long* off = reinterpret_cast<unsigned long long*>(sm_raw);  // [F]
-  uint32_t* cur = reinterpret_cast<uint32_t*>(off + F);                      // [F]
-  for (uint32_t c = blockIdx.x; c < mc; c += gridDim.x) {
-    const uint64_t b0 = uint64_t(c) << fb;
-    for (uint32_t j = threadIdx.x; j < F; j += blockDim.x) {
-      off[j] = boff[b0 + j];
-      cur[j] = 0;
-    }
+                                                      const uint32_t* __restrict__ rbkt, uint64_t total,
+                                                      unsigned long long* __restrict__ fcur,
+                                                      uint64_t* __restrict__ pkeys, uint32_t* __restrict__ plink,
+                                                      Counters* ctr) {
+  __shared__ uint64_t s_c;
+  constexpr int PER = SC_FINE / 256;
+  for (;;) {
+    if (threadIdx.x == 0) s_c = uint64_t(atomicAdd(&ctr->work_next, 1u)) * SC_FINE;
     __syncthreads();
-    const uint64_t lo = boff[b0], hi = boff[b0 + F];
-    for (uint64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
-      const uint32_t f = rbkt[i] & (F - 1u);
-      const uint64_t p = off[f] + atomicAdd(cur + f, 1u);
-      st_key<NW>(pkeys, p, ld_key<NW>(rkey, i));
-      plink[p] = rlink[i];
-    }
+    const uint64_t c0 = s_c;
     __syncthreads();
+    if (c0 >= total) break;
+    uint32_t bk[PER];
+    uint64_t pos[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const uint64_t i = c0 + uint64_t(q) * blockDim.x + threadIdx.x;
+      bk[q] = (i < total) ? rbkt[i] : NONE;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) pos[q] = (bk[q] != NONE) ? atomicAdd(fcur + bk[q], 1ull) : 0ull;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const uint64_t i = c0 + uint64_t(q) * blockDim.x + threadIdx.x;
+      if (bk[q] != NONE) {
+        st_key<NW>(pkeys, pos[q], ld_key<NW>(rkey, i));
+        plink[pos[q]] = rlink[i];
+      }
+    }
   }
 }
 
@@ -568,29 +618,6 @@ __device__ __forceinline__ Key<NW> skey(const TileMem<NW, IT>& m, uint32_t i) {
   return k;
 }
 
-// Pointer-jumping rounds over (px, rx) with second buffers (py, ry); the
-// result lands in (ptr, rnk).  Starts point at themselves with rank 0.
-template <typename IT>
-__device__ void jump_rounds(uint32_t c, IT* px, IT* rx, IT* py, IT* ry, IT*& ptr, IT*& rnk) {
-  uint32_t rounds = 1;
-  for (uint32_t lim = 1; lim < c; lim <<= 1) ++rounds;
-  for (uint32_t r = 0; r < rounds; ++r) {
-    int changed = 0;
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
-      const uint32_t p = px[i];
-      const uint32_t np = px[p];
-      py[i] = IT(np);
-      ry[i] = IT(uint32_t(rx[i]) + uint32_t(rx[p]));
-      changed |= (np != p);
-    }
-    IT* t = px; px = py; py = t;
-    t = rx; rx = ry; ry = t;
-    if (!__syncthreads_or(changed)) break;
-  }
-  ptr = px;
-  rnk = rx;
-}
-
 struct U3 {
   unsigned long long a, b, c;
 };
@@ -629,37 +656,126 @@ __device__ __forceinline__ U3 block_excl_scan3(U3 v, U3* sc, U3* total) {
   return r;
 }
 
-template <int NW, typename IT>
+// Reserve a tile's closed-line bytes, open-segment chars and segment ids.
+__device__ __forceinline__ int reserve_space(const TileParams& p, const U3& tot, unsigned long long* b) {
+  b[0] = tot.a ? atomicAdd(&p.ctr->out_cursor, tot.a) : 0ull;
+  b[1] = tot.b ? atomicAdd(&p.ctr->seg_char_cursor, tot.b) : 0ull;
+  b[2] = tot.c ? atomicAdd(&p.ctr->seg_count, uint32_t(tot.c)) : 0u;
+  if (b[0] + tot.a > p.out_cap || b[1] + tot.b > p.segchars_cap || b[2] + tot.c > p.seg_cap) {
+    atomicOr(&p.ctr->err, ERR_CAPACITY);
+    return 0;
+  }
+  return 1;
+}
+
+// Thread-group policies: a tile is worked by a whole block or by one warp.
+struct BlockGroup {
+  static __device__ __forceinline__ uint32_t rank() { return threadIdx.x; }
+  static __device__ __forceinline__ uint32_t size() { return blockDim.x; }
+  static __device__ __forceinline__ void sync() { __syncthreads(); }
+  static __device__ __forceinline__ int sync_or(int v) { return __syncthreads_or(v); }
+  static __device__ __forceinline__ U3 scan3(U3 v, U3* total) {
+    __shared__ U3 sc[33];
+    return block_excl_scan3(v, sc, total);
+  }
+  // The leader reserves output space for the tile; false if a bound was hit.
+  static __device__ __forceinline__ bool reserve(const TileParams& p, const U3& tot, unsigned long long* base) {
+    __shared__ unsigned long long s_base[3];
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) s_ok = reserve_space(p, tot, s_base);
+    __syncthreads();
+    base[0] = s_base[0];
+    base[1] = s_base[1];
+    base[2] = s_base[2];
+    const int ok = s_ok;
+    __syncthreads();
+    return ok;
+  }
+};
+
+struct WarpGroup {
+  static __device__ __forceinline__ uint32_t rank() { return threadIdx.x & 31u; }
+  static __device__ __forceinline__ uint32_t size() { return 32u; }
+  static __device__ __forceinline__ void sync() { __syncwarp(); }
+  static __device__ __forceinline__ int sync_or(int v) { return __any_sync(0xFFFFFFFFu, v); }
+  static __device__ __forceinline__ U3 scan3(U3 v, U3* total) {
+    const int lane = threadIdx.x & 31;
+    U3 inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const U3 t = u3_shfl_up(inc, o);
+      if (lane >= o) inc = u3_add(inc, t);
+    }
+    *total = U3{__shfl_sync(0xFFFFFFFFu, inc.a, 31), __shfl_sync(0xFFFFFFFFu, inc.b, 31),
+                __shfl_sync(0xFFFFFFFFu, inc.c, 31)};
+    return U3{inc.a - v.a, inc.b - v.b, inc.c - v.c};
+  }
+  static __device__ __forceinline__ bool reserve(const TileParams& p, const U3& tot, unsigned long long* base) {
+    unsigned long long b[3] = {0, 0, 0};
+    int ok = 1;
+    if ((threadIdx.x & 31) == 0) ok = reserve_space(p, tot, b);
+    base[0] = __shfl_sync(0xFFFFFFFFu, b[0], 0);
+    base[1] = __shfl_sync(0xFFFFFFFFu, b[1], 0);
+    base[2] = __shfl_sync(0xFFFFFFFFu, b[2], 0);
+    return __shfl_sync(0xFFFFFFFFu, ok, 0);
+  }
+};
+
+// Pointer-jumping rounds over (px, rx) with second buffers (py, ry); the
+// result lands in (ptr, rnk).  Starts point at themselves with rank 0.
+template <typename G, typename IT>
+__device__ void jump_rounds(uint32_t c, IT* px, IT* rx, IT* py, IT* ry, IT*& ptr, IT*& rnk) {
+  uint32_t rounds = 1;
+  for (uint32_t lim = 1; lim < c; lim <<= 1) ++rounds;
+  for (uint32_t r = 0; r < rounds; ++r) {
+    int changed = 0;
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
+      const uint32_t p = px[i];
+      const uint32_t np = px[p];
+      py[i] = IT(np);
+      ry[i] = IT(uint32_t(rx[i]) + uint32_t(rx[p]));
+      changed |= (np != p);
+    }
+    IT* t = px; px = py; py = t;
+    t = rx; rx = ry; ry = t;
+    if (!G::sync_or(changed)) break;
+  }
+  ptr = px;
+  rnk = rx;
+}
+
+template <int NW, typename IT, typename G>
 __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint64_t beg, uint32_t c) {
   constexpr uint32_t NONE_I = Ix<IT>::NONE, DUP_I = Ix<IT>::DUP, CNONE_I = Ix<IT>::CNONE;
   const PrefMask pm = pref_mask(p.k);
-  const uint32_t tmask = m.ts - 1;
+  const uint32_t ts = pow2_at_least(2ull * c);  // this tile's slots (<= m.ts)
+  const uint32_t tmask = ts - 1;
   const int k = p.k;
   // ---- stage the tile's keys (async copies), initialise the work arrays
   if constexpr (sizeof(IT) == 2) {
     // shared-memory tile: asynchronous copies overlap the initialisation
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x)
+    for (uint32_t i = G::rank(); i < c; i += G::size())
       __pipeline_memcpy_async(m.key + size_t(i) * NW, p.pkeys + (beg + i) * NW, 8 * NW);
     __pipeline_commit();
   } else {
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
       const Key<NW> x = ld_key<NW>(p.pkeys, beg + i);
 #pragma unroll
       for (int w = 0; w < NW; ++w) m.key[size_t(i) * NW + w] = x.w[w];
     }
   }
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     m.A[i] = IT(CNONE_I);
     m.B[i] = 0;
     m.P[i] = IT(NONE_I);
   }
-  for (uint32_t i = threadIdx.x; i < m.ts; i += blockDim.x) m.T[i] = IT(NONE_I);
+  for (uint32_t i = G::rank(); i < ts; i += G::size()) m.T[i] = IT(NONE_I);
   if constexpr (sizeof(IT) == 2) __pipeline_wait_prior(0);
-  __syncthreads();
+  G::sync();
   // ---- prefix table of the P copies (generate_hashmap, assembler.h:120-150):
   // one slot per distinct (k-1)-prefix; a prefix held by two copies marks the
   // slot's copy DUP ("nullified")
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     const Key<NW> x = skey(m, i);
     if (!(roles(x) & ROLE_P)) continue;
     const Key<NW> pf = prefix_of(x, pm);
@@ -674,10 +790,10 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
       h = (h + 1) & tmask;
     }
   }
-  __syncthreads();
+  G::sync();
   // ---- suffix lookups of the S copies (find_vtx_from_edge, assembler.h:89-111)
   // and in-degree counts ("count edges", assembler.h:180-188)
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     const Key<NW> x = skey(m, i);
     if (!(roles(x) & ROLE_S)) continue;
     const Key<NW> sf = suffix_of(x, pm);
@@ -698,10 +814,10 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     }
     m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
   }
-  __syncthreads();
+  G::sync();
   // ---- kept edges: u->v iff v is u's unique successor and u is v's only
   // predecessor ("write edges", assembler.h:189-197); rank init alongside
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     const uint32_t cand = uint32_t(m.A[i]) & CNONE_I;
     const uint32_t s = (cand != CNONE_I && m.B[cand] == 1u) ? cand : NONE_I;
     const uint32_t q = (m.B[i] == 1u) ? uint32_t(m.P[i]) : NONE_I;
@@ -710,9 +826,9 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     m.Q[i] = IT(q == NONE_I ? i : q);
     m.T[i] = IT(q == NONE_I ? 0u : 1u);
   }
-  __syncthreads();
+  G::sync();
   if (p.mode == 0) {
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
       const uint64_t r = roles(skey(m, i));
       const uint32_t id = p.plink[beg + i];
       if (r & ROLE_S) p.succ[id] = (m.A[i] == NONE_I) ? NONE : p.plink[beg + m.A[i]];
@@ -722,11 +838,11 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   }
   // ---- local segments: list ranking by pointer jumping
   IT *ptr, *rnk;
-  jump_rounds<IT>(c, m.Q, m.T, m.B, m.T + c, ptr, rnk);
+  jump_rounds<G, IT>(c, m.Q, m.T, m.B, m.T + c, ptr, rnk);
   // ---- local cycles (every copy has a local predecessor): cut each at its
   // smallest key, then rank again
   int cyc = 0;
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     // a path copy points at its start (no predecessor); a cycle copy at
     // another cycle copy.  Cycle copies have a successor, so A = index | DUP.
     if (m.P[ptr[i]] != NONE_I) {
@@ -734,23 +850,23 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
       cyc = 1;
     }
   }
-  if (__syncthreads_or(cyc)) {
+  if (G::sync_or(cyc)) {
     IT *lx = m.T, *jx = m.T + c, *ly = m.B, *jy = m.Q;
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
       lx[i] = IT(i);
       jx[i] = IT(m.P[i] == NONE_I ? i : uint32_t(m.P[i]));
     }
-    __syncthreads();
+    G::sync();
     uint32_t rounds = 1;
     for (uint32_t lim = 1; lim < c; lim <<= 1) ++rounds;
     for (uint32_t r = 0; r < rounds; ++r) {
-      for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+      for (uint32_t i = G::rank(); i < c; i += G::size()) {
         const uint32_t j = jx[i];
         const uint32_t a = lx[i], b = lx[j];
         ly[i] = IT(key_lt(skey(m, b), skey(m, a)) ? b : a);
         jy[i] = jx[j];
       }
-      __syncthreads();
+      G::sync();
       IT* t = lx; lx = ly; ly = t;
       t = jx; jx = jy; jy = t;
     }
@@ -758,23 +874,23 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     // exactly one copy per cycle (the smallest key) is its own label; the edge
     // into it is cut, path copies are untouched
     auto on_cycle = [](uint32_t a) { return a != NONE_I && (a & DUP_I); };
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
       if (on_cycle(m.A[i]) && lx[i] == i) {
         const uint32_t q = m.P[i];
         m.A[q] = IT(NONE_I);
         m.P[i] = IT(NONE_I);
       }
     }
-    __syncthreads();
-    for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+    G::sync();
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
       const uint32_t a = m.A[i];
       if (on_cycle(a)) m.A[i] = IT(a & ~DUP_I);
       const uint32_t q = m.P[i];
       m.Q[i] = IT(q == NONE_I ? i : q);
       m.T[i] = IT(q == NONE_I ? 0u : 1u);
     }
-    __syncthreads();
-    jump_rounds<IT>(c, m.Q, m.T, m.B, m.T + c, ptr, rnk);
+    G::sync();
+    jump_rounds<G, IT>(c, m.Q, m.T, m.B, m.T + c, ptr, rnk);
   }
   // every copy now reaches a segment start.  Free arrays: the pair not
   // holding (ptr, rnk) keeps each start's byte offset (lo/hi halves), P its
@@ -783,11 +899,8 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   IT* hi_a = (rnk == m.T) ? m.T + c : m.T;
   // ---- emission: closed segments (start has role P, end has role S) are
   // whole unitigs; the others are stitched across tiles
-  __shared__ U3 sc3[33];
-  __shared__ unsigned long long s_base[3];
-  __shared__ int s_skip;
-  const uint32_t chunk = (c + blockDim.x - 1) / blockDim.x;
-  const uint32_t lo = min(c, threadIdx.x * chunk), hi = min(c, lo + chunk);
+  const uint32_t chunk = (c + G::size() - 1) / G::size();
+  const uint32_t lo = min(c, G::rank() * chunk), hi = min(c, lo + chunk);
   U3 mine{0, 0, 0};
   for (uint32_t i = lo; i < hi; ++i) {
     if (m.A[i] != NONE_I) continue;
@@ -798,19 +911,9 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     else { mine.b += uint64_t(k) - 1 + len; mine.c += 1; }
   }
   U3 tot;
-  U3 pre = block_excl_scan3(mine, sc3, &tot);
-  if (threadIdx.x == 0) {
-    s_skip = 0;
-    s_base[0] = tot.a ? atomicAdd(&p.ctr->out_cursor, tot.a) : 0ull;
-    s_base[1] = tot.b ? atomicAdd(&p.ctr->seg_char_cursor, tot.b) : 0ull;
-    s_base[2] = tot.c ? atomicAdd(&p.ctr->seg_count, uint32_t(tot.c)) : 0u;
-    if (s_base[0] + tot.a > p.out_cap || s_base[1] + tot.b > p.segchars_cap || s_base[2] + tot.c > p.seg_cap) {
-      atomicOr(&p.ctr->err, ERR_CAPACITY);
-      s_skip = 1;
-    }
-  }
-  __syncthreads();
-  if (s_skip) return;
+  U3 pre = G::scan3(mine, &tot);
+  unsigned long long s_base[3];
+  if (!G::reserve(p, tot, s_base)) return;
   const unsigned long long cbase = s_base[0], obase = s_base[1], sbase = s_base[2];
   for (uint32_t i = lo; i < hi; ++i) {
     if (m.A[i] != NONE_I) continue;
@@ -835,8 +938,8 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
       lo_a[s] = IT(loc);
     }
   }
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < c; i += blockDim.x) {
+  G::sync();
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     const uint32_t s = ptr[i];
     const uint32_t r = rnk[i];
     uint64_t loc = lo_a[s];
@@ -869,25 +972,46 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   }
 }
 
-// Persistent tile kernel: each CTA takes the next tile from a global
-// counter until none are left; tiles larger than the capacity are left for
+// Persistent tile kernels.  Warp tiles (<= warp capacity copies): every warp
+// of a CTA owns a slice of shared memory and takes the next warp tile from a
+// global counter, with warp-level synchronisation only.  Block tiles (up to
+// the tile capacity): the whole CTA works one tile.  Larger tiles go to
 // k_tile_big.
+template <int NW>
+__global__ void __launch_bounds__(256) k_tile_warp(TileParams p) {
+  extern __shared__ __align__(16) char smem[];
+  const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const TileMem<NW, uint16_t> m = carve<NW, uint16_t>(smem + size_t(wid) * p.wbytes, p.wcap, p.wts);
+  const uint32_t nt = p.ctr->nwarp;
+  for (;;) {
+    uint32_t j = 0;
+    if (lane == 0) j = atomicAdd(&p.ctr->wtile_next, 1u);
+    j = __shfl_sync(0xFFFFFFFFu, j, 0);
+    if (j >= nt) break;
+    const uint32_t t = p.wlist[j];
+    const uint64_t beg = p.tile_begin[t];
+    const uint32_t c = uint32_t(p.tile_begin[t + 1] - beg);
+    process_tile<NW, uint16_t, WarpGroup>(p, m, beg, c);
+    __syncwarp();
+  }
+}
+
 template <int NW>
 __global__ void __launch_bounds__(512) k_tile(TileParams p) {
   extern __shared__ __align__(16) char smem[];
   __shared__ uint32_t s_t;
   const TileMem<NW, uint16_t> m = carve<NW, uint16_t>(smem, p.cap, p.tslots);
-  const uint32_t nt = p.ctr->ntiles;
+  const uint32_t nt = p.ctr->nblock;
   for (;;) {
     if (threadIdx.x == 0) s_t = atomicAdd(&p.ctr->tile_next, 1u);
     __syncthreads();
-    const uint32_t t = s_t;
+    const uint32_t j = s_t;
     __syncthreads();
-    if (t >= nt) break;
+    if (j >= nt) break;
+    const uint32_t t = p.blist[j];
     const uint64_t beg = p.tile_begin[t];
-    const uint64_t c = p.tile_begin[t + 1] - beg;
-    if (c == 0 || c > p.cap) continue;
-    process_tile<NW, uint16_t>(p, m, beg, uint32_t(c));
+    const uint32_t c = uint32_t(p.tile_begin[t + 1] - beg);
+    process_tile<NW, uint16_t, BlockGroup>(p, m, beg, c);
     __syncthreads();
   }
 }
@@ -900,7 +1024,7 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
   const uint64_t c = p.tile_begin[t + 1] - beg;
   const uint32_t ts = pow2_at_least(2 * c);
   const TileMem<NW, uint32_t> m = carve<NW, uint32_t>(p.big_scratch + p.big_off[blockIdx.x], uint32_t(c), ts);
-  process_tile<NW, uint32_t>(p, m, beg, uint32_t(c));
+  process_tile<NW, uint32_t, BlockGroup>(p, m, beg, uint32_t(c));
 }
 
 // ================================================================= stitch
@@ -1631,7 +1755,7 @@ int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
 
 // Bucket plan for n k-mers.
 struct Plan {
-  uint32_t bbits, cap, win, small, tslots;
+  uint32_t bbits, cap, win, small, tslots, wcap, wts, wbytes;
   int l_used;
   uint64_t M;
 };
@@ -1641,12 +1765,17 @@ static Plan plan_buckets(const Env& e, uint64_t n, int k, int l) {
   const int nw = (k <= 31) ? 1 : 2;
   uint32_t cap = e.tune.tile_capacity ? e.tune.tile_capacity : 4096;
   while (cap > 256 && tile_bytes(nw, cap, pow2_at_least(2ull * cap)) > size_t(e.smem_optin)) cap -= 256;
+  // warp tiles: <= wcap copies, one warp each (1 disables the tier)
+  uint32_t wcap = e.tune.warp_capacity ? e.tune.warp_capacity : 256;
+  if (wcap > cap) wcap = cap;
+  const bool warp_tier = wcap >= 32;
+  const uint32_t pack_cap = warp_tier ? wcap : cap;  // tiles are packed for this capacity
   const uint64_t copies = n + n / 8 + 1;
   uint32_t bbits = 0;
   if (e.tune.bucket_bits) {
     bbits = e.tune.bucket_bits;
   } else {
-    while ((copies >> bbits) > cap / 8 && bbits < 24) ++bbits;  // ~cap/8 copies per bucket
+    while ((copies >> bbits) > pack_cap / 8 && bbits < 25) ++bbits;  // ~capacity/8 copies per bucket
   }
   // enough l-mers that each bucket gathers several of them
   const int lmin = int((bbits + 2 + 1) / 2);
@@ -1657,9 +1786,12 @@ static Plan plan_buckets(const Env& e, uint64_t n, int k, int l) {
   while (ts > pow2_at_least(2ull * cap) && tile_bytes(nw, cap, ts) > size_t(e.smem_optin)) ts >>= 1;
   P.bbits = bbits;
   P.cap = cap;
-  P.win = cap - cap / 4;
-  P.small = cap / 4;
+  P.win = pack_cap - pack_cap / 4;
+  P.small = pack_cap / 4;
   P.tslots = ts;
+  P.wcap = warp_tier ? wcap : 0;
+  P.wts = warp_tier ? pow2_at_least(2ull * wcap) : 0;
+  P.wbytes = warp_tier ? uint32_t((tile_bytes(nw, wcap, P.wts) + 15) & ~size_t(15)) : 0;
   P.l_used = lu;
   P.M = 1ull << bbits;
   return P;
@@ -1668,8 +1800,8 @@ static Plan plan_buckets(const Env& e, uint64_t n, int k, int l) {
 struct Front {
   uint64_t* keys;
   uint32_t *b1, *b2, *counts;
-  unsigned long long *boff, *cursor, *tile_begin, *scan_tmp;
-  uint32_t *flag, *fidx, *big_list;
+  unsigned long long *boff, *cursor, *fcur, *tile_begin, *scan_tmp;
+  uint32_t *flag, *fidx, *big_list, *wlist, *blist;
   unsigned long long* big_size;
 };
 
@@ -1677,8 +1809,9 @@ static size_t front_bytes(uint64_t n, int nw, uint64_t M, bool own_keys) {
   size_t need = 0;
   auto add = [&](size_t b) { need += (b + 255) & ~size_t(255); };
   if (own_keys) add(n * 8 * nw);
-  add(n * 4); add(n * 4); add(M * 4); add((M + 1) * 8); add(M * 8); add((M + 2) * 8);
+  add(n * 4); add(n * 4); add(M * 4); add((M + 1) * 8); add(M * 8); add(M * 8); add((M + 2) * 8);
   add(scan_tmp_elems(M) * 8); add(M * 4); add((M + 1) * 4); add(M * 4); add(M * 8);
+  add(M * 4); add(M * 4);
   return need;
 }
 
@@ -1689,13 +1822,16 @@ static int take_front(Env& e, uint64_t n, int nw, uint64_t M, bool own_keys, Fro
   f.counts = static_cast<uint32_t*>(e.take(0, M * 4));
   f.boff = static_cast<unsigned long long*>(e.take(0, (M + 1) * 8));
   f.cursor = static_cast<unsigned long long*>(e.take(0, M * 8));
+  f.fcur = static_cast<unsigned long long*>(e.take(0, M * 8));
   f.tile_begin = static_cast<unsigned long long*>(e.take(0, (M + 2) * 8));
   f.scan_tmp = static_cast<unsigned long long*>(e.take(0, scan_tmp_elems(M) * 8));
   f.flag = static_cast<uint32_t*>(e.take(0, M * 4));
   f.fidx = static_cast<uint32_t*>(e.take(0, (M + 1) * 4));
   f.big_list = static_cast<uint32_t*>(e.take(0, M * 4));
   f.big_size = static_cast<unsigned long long*>(e.take(0, M * 8));
-  if (!f.big_size) return e.fail(UC_EBUDGET, "front arena overflow");
+  f.wlist = static_cast<uint32_t*>(e.take(0, M * 4));
+  f.blist = static_cast<uint32_t*>(e.take(0, M * 4));
+  if (!f.blist) return e.fail(UC_EBUDGET, "front arena overflow");
   return UC_OK;
 }
 
@@ -1712,7 +1848,7 @@ static int bucket_offsets(Env& e, const Front& f, uint64_t M, uint64_t& copies) 
 
 // Level split of the scatter: 2^mcb coarse partitions of 2^fb buckets.
 static void scatter_split(uint32_t bbits, uint32_t& mcb, uint32_t& fb) {
-  mcb = std::max<int>(int(bbits) - 12, int(std::min<uint32_t>(bbits, 8)));
+  mcb = std::min<uint32_t>(bbits, 8);
   fb = bbits - mcb;
 }
 
@@ -1739,36 +1875,47 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
     // coarse cursors: the first position of each coarse partition
     e.launches += 1;
     k_coarse_init<<<grid_for(e, mc, 256), 256, 0, e.stream>>>(f.boff, fb, mc, f.cursor);
-    const size_t sm1 = size_t(mc) * 12;
-    const size_t sm2 = (size_t(1) << fb) * 12;
-    if (sm1 > 48 * 1024) {
-      UC_CK(cudaFuncSetAttribute(k_scatter_coarse<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
-      UC_CK(cudaFuncSetAttribute(k_scatter_coarse<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
-    }
-    if (sm2 > 48 * 1024) {
-      UC_CK(cudaFuncSetAttribute(k_scatter_fine<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm2)));
-      UC_CK(cudaFuncSetAttribute(k_scatter_fine<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm2)));
-    }
-    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + SC_CHUNK - 1) / SC_CHUNK, uint64_t(e.sm_count) * 8)));
-    const int g2 = int(std::max<uint32_t>(1, std::min<uint32_t>(mc, uint32_t(e.sm_count) * 4)));
+    const size_t sm1 = size_t(2 * SC_CHUNK) * (8 * nw + 8) + size_t(mc) * 16 + 16;
+    UC_CK(cudaFuncSetAttribute(k_scatter_coarse<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
+    UC_CK(cudaFuncSetAttribute(k_scatter_coarse<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
+    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + SC_CHUNK - 1) / SC_CHUNK, uint64_t(e.sm_count) * 6)));
+    // fine cursors start at every bucket's offset (reuses the scan's output
+    // buffer slot after the tiles are planned)
+    unsigned long long* fcur = f.fcur;
+    UC_CK(cudaMemcpyAsync(fcur, f.boff, P.M * 8, cudaMemcpyDeviceToDevice, e.stream));
+    UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
+    const int g2 = e.sm_count * 8;
     e.launches += 2;
     if (nw == 1) {
       k_scatter_coarse<1><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
-      k_scatter_fine<1><<<g2, 512, sm2, e.stream>>>(rkey, rlink, rbkt, f.boff, fb, mc, pkeys, plink);
+      k_scatter_fine<1><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, fcur, pkeys, plink, e.ctr);
     } else {
       k_scatter_coarse<2><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
-      k_scatter_fine<2><<<g2, 512, sm2, e.stream>>>(rkey, rlink, rbkt, f.boff, fb, mc, pkeys, plink);
+      k_scatter_fine<2><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, fcur, pkeys, plink, e.ctr);
     }
     UC_CK(cudaGetLastError());
   }
   ++e.launches;
-  k_find_big<<<grid_for(e, M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, P.cap, f.big_list, f.big_size, nw);
+  k_classify<<<grid_for(e, M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, P.wcap, P.cap, f.wlist, f.blist,
+                                                         f.big_list, f.big_size, nw);
   UC_CK(cudaGetLastError());
   return UC_OK;
 }
 
 template <int NW>
 static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
+  tp.wlist = f.wlist;
+  tp.blist = f.blist;
+  if (tp.wcap) {
+    const size_t wsm = size_t(tp.wbytes) * 8;
+    UC_CK(cudaFuncSetAttribute(k_tile_warp<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm)));
+    int wocc = 0;
+    UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wocc, k_tile_warp<NW>, 256, wsm));
+    if (wocc < 1) return e.fail(UC_EINTERNAL, "warp tile kernel does not fit an SM");
+    ++e.launches;
+    k_tile_warp<NW><<<e.sm_count * wocc, 256, wsm, e.stream>>>(tp);
+    UC_CK(cudaGetLastError());
+  }
   const size_t smem = tile_bytes(NW, tp.cap, tp.tslots);
   UC_CK(cudaFuncSetAttribute(k_tile<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
   int occ = 0;
@@ -1860,6 +2007,9 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   tp.k = k;
   tp.cap = P.cap;
   tp.tslots = P.tslots;
+  tp.wcap = P.wcap;
+  tp.wts = P.wts;
+  tp.wbytes = P.wbytes;
   tp.mode = 0;
   tp.succ = succ;
   tp.pred = pred;
@@ -2181,6 +2331,9 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   tp.k = k;
   tp.cap = P.cap;
   tp.tslots = P.tslots;
+  tp.wcap = P.wcap;
+  tp.wts = P.wts;
+  tp.wbytes = P.wbytes;
   tp.mode = 1;
   tp.out = out;
   tp.out_cap = cap;
