@@ -50,7 +50,7 @@ typedef struct uc_job uc_job;
 typedef struct uc_stats {
     uint64_t n_kmers, n_copies, n_cross, n_tiles, n_big_tiles;
     uint64_t n_segments, n_unitigs, n_cycles, out_bytes;
-    uint32_t l_used, bucket_bits, tile_capacity, stitch_rounds, launches;
+    uint32_t l_used, bucket_bits, tile_capacity, stitch_rounds, launches, graph_nodes;
     float ms_pack, ms_bucket, ms_tiles, ms_stitch, ms_total;
 } uc_stats;
 
@@ -142,6 +142,18 @@ uint64_t uc_output_bound(size_t text_bytes, int k);
 uc_status uc_compact_host(uc_ctx *ctx, const char *text, size_t bytes, int k,
                           int l, char *out, size_t cap, size_t *out_bytes,
                           uc_stats *stats);
+
+/* Many independent jobs in one pass (same k and l): all their buckets form
+ * one tile queue worked by one persistent launch per tier.  Job j's lines land
+ * in d_out[out_offsets[j], out_offsets[j] + out_lengths[j]).  d_out needs
+ * uc_batch_output_bound bytes.  Jobs whose lines are not exactly k chars +
+ * '\n' are compacted one by one.  (No reference counterpart: the reference
+ * runs one job per process; this is the batched form of its main.) */
+uc_status uc_compact_batch(uc_ctx *ctx, int njobs, const char *const *d_texts,
+                           const size_t *bytes, int k, int l, char *d_out,
+                           uint64_t out_cap, uint64_t *out_offsets,
+                           uint64_t *out_lengths, uc_stats *stats);
+uint64_t uc_batch_output_bound(int njobs, const size_t *bytes, int k);
 
 /* ---- host-memory jobs ------------------------------------------------- */
 

@@ -249,3 +249,51 @@ def test_hec_with_cycles(comp, oracle, k):
     ohead, orank, _ = oracle.contract(words, k, osucc, opred)
     assert np.array_equal(as_u32(head), ohead) and np.array_equal(as_u32(rank), orank)
     assert cyc == ocyc == 1
+
+
+def test_batch_matches_oracle_and_alone(comp, oracle, texts):
+    """Many jobs in one pass: every job's lines equal the oracle's and equal
+    the job compacted alone (batched-vs-alone)."""
+    from unitigcoarsening_b200 import synth
+    jobs = [synth.make_text(synth.batched_job(j, scale=0.02), 31).numpy().tobytes() for j in range(12)]
+    jobs += [texts["small_plain"][0], b"0\n", text_of(["ACGTACGTACGTACGTACGTACGTACGTACG"]),
+             text_of(cyclic_kmers(80, 31, seed=4))]
+    outs = comp.compact_batch([dev(t) for t in jobs], 31, 8)
+    torch.cuda.synchronize()
+    for t, o in zip(jobs, outs):
+        got = sorted_lines(o.cpu().numpy().tobytes())
+        want, _, _ = oracle.compact(t, 31)
+        assert got == sorted_lines(want)
+        assert got == fused_lines(comp, t, 31, 8)
+
+
+def test_batch_k63_and_mixed_layouts(comp, oracle):
+    from unitigcoarsening_b200 import synth
+    jobs = [synth.make_text(synth.wide_k(length=30_000 + 7_000 * j, seed=40 + j), 63).numpy().tobytes()
+            for j in range(5)]
+    outs = comp.compact_batch([dev(t) for t in jobs], 63, 8)
+    for t, o in zip(jobs, outs):
+        want, _, _ = oracle.compact(t, 63)
+        assert sorted_lines(o.cpu().numpy().tobytes()) == sorted_lines(want)
+    # a job with CRLF lines sends the batch one job at a time
+    seq = distinct_path(300, 31, seed=8)
+    mixed = [text_of(walk_kmers(seq, 31), crlf=True), text_of(walk_kmers(distinct_path(200, 31, seed=9), 31))]
+    outs = comp.compact_batch([dev(t) for t in mixed], 31, 8)
+    for t, o in zip(mixed, outs):
+        want, _, _ = oracle.compact(t, 31)
+        assert sorted_lines(o.cpu().numpy().tobytes()) == sorted_lines(want)
+
+
+def test_batch_with_tiers_and_hec(comp, oracle):
+    from unitigcoarsening_b200 import CONTRACT_HEC, synth
+    jobs = [synth.make_text(synth.scale_plain(length=40_000 + 9_000 * j, seed=60 + j), 31).numpy().tobytes()
+            for j in range(6)]
+    for tune in [dict(warp_capacity=1), dict(tile_capacity=512, warp_capacity=64), dict(contract_method=CONTRACT_HEC)]:
+        comp.set_tuning(**tune)
+        try:
+            outs = comp.compact_batch([dev(t) for t in jobs], 31, 8)
+        finally:
+            comp.set_tuning(tile_capacity=0, warp_capacity=0, contract_method=0)
+        for t, o in zip(jobs, outs):
+            want, _, _ = oracle.compact(t, 31)
+            assert sorted_lines(o.cpu().numpy().tobytes()) == sorted_lines(want)

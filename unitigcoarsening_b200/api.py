@@ -50,7 +50,8 @@ class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "n_kmers", "n_copies", "n_cross", "n_tiles", "n_big_tiles",
         "n_segments", "n_unitigs", "n_cycles", "out_bytes")] + \
-        [(n, ctypes.c_uint32) for n in ("l_used", "bucket_bits", "tile_capacity", "stitch_rounds", "launches")] + \
+        [(n, ctypes.c_uint32) for n in ("l_used", "bucket_bits", "tile_capacity", "stitch_rounds", "launches",
+                                          "graph_nodes")] + \
         [(n, ctypes.c_float) for n in ("ms_pack", "ms_bucket", "ms_tiles", "ms_stitch", "ms_total")]
 
     def as_dict(self) -> dict:
@@ -93,6 +94,9 @@ def lib():
             "uc_compact_device": ([vp, vp, sz, i, i, vp, u64, pu64, ctypes.POINTER(Stats)], i),
             "uc_output_bound": ([sz, i], u64),
             "uc_compact_host": ([vp, vp, sz, i, i, vp, sz, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(Stats)], i),
+            "uc_compact_batch": ([vp, i, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t), i, i, vp, u64,
+                                  pu64, pu64, ctypes.POINTER(Stats)], i),
+            "uc_batch_output_bound": ([i, ctypes.POINTER(ctypes.c_size_t), i], u64),
             "uc_job_submit": ([vp, vp, sz, i, i, ctypes.POINTER(vp)], i),
             "uc_job_poll": ([vp, ctypes.POINTER(ctypes.c_int)], i),
             "uc_job_wait": ([vp], i),
@@ -242,6 +246,24 @@ class Compactor:
         self._check(self._L.uc_compact_device(self._h, _ptr(text), text.numel(), k, l, _ptr(out), out.numel(),
                                               ctypes.byref(nb), ctypes.byref(st)))
         res = out[: nb.value]
+        return (res, st.as_dict()) if stats else res
+
+    def compact_batch(self, texts, k: int, l: int, out: torch.Tensor | None = None, stats: bool = False):
+        """Many device-resident jobs in one pass; returns one uint8 CUDA tensor
+        (a view of the shared output buffer) per job."""
+        self._bind_stream()
+        nj = len(texts)
+        ptrs = (ctypes.c_void_p * max(nj, 1))(*[t.data_ptr() for t in texts])
+        sizes = (ctypes.c_size_t * max(nj, 1))(*[t.numel() for t in texts])
+        cap = int(self._L.uc_batch_output_bound(nj, sizes, k))
+        if out is None or out.numel() < cap:
+            out = torch.empty(max(cap, 1), dtype=torch.uint8, device=self._dev())
+        off = (ctypes.c_uint64 * max(nj, 1))()
+        ln = (ctypes.c_uint64 * max(nj, 1))()
+        st = Stats()
+        self._check(self._L.uc_compact_batch(self._h, nj, ptrs, sizes, k, l, _ptr(out), out.numel(), off, ln,
+                                             ctypes.byref(st)))
+        res = [out[off[j]: off[j] + ln[j]] for j in range(nj)]
         return (res, st.as_dict()) if stats else res
 
     def compact_host(self, text, k: int, l: int, out=None, stats: bool = False):

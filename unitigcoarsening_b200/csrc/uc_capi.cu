@@ -153,6 +153,10 @@ uc_status uc_ctx_destroy(uc_ctx* c) {
   for (auto& a : c->env.ar)
     if (a.base) cudaFree(a.base);
   if (c->env.big_buf) cudaFree(c->env.big_buf);
+  if (c->env.jbuf) cudaFree(c->env.jbuf);
+  for (auto& g : c->env.gexec)
+    if (g) cudaGraphExecDestroy(g);
+  if (c->env.gstream) cudaStreamDestroy(c->env.gstream);
   if (c->io_text) cudaFree(c->io_text);
   if (c->io_out) cudaFree(c->io_out);
   if (c->env.ctr) cudaFree(c->env.ctr);
@@ -292,6 +296,44 @@ uc_status uc_compact_device(uc_ctx* c, const char* d_text, size_t bytes, int k, 
   const int r = uc::compact_device(c->env, d_text, bytes, k, l, d_out, cap, ob, stats);
   c->env.reset();
   *out_bytes = ob;
+  return as_status(r);
+}
+
+uint64_t uc_batch_output_bound(int njobs, const size_t* bytes, int k) {
+  uint64_t t = 0;
+  for (int j = 0; j < njobs; ++j) t += (uc::output_bound(bytes[j], k) + 15) & ~uint64_t(15);
+  return t;
+}
+
+uc_status uc_compact_batch(uc_ctx* c, int njobs, const char* const* d_texts, const size_t* bytes, int k, int l,
+                           char* d_out, uint64_t out_cap, uint64_t* out_off, uint64_t* out_len, uc_stats* stats) {
+  if (!c || njobs < 0 || (njobs > 0 && (!d_texts || !bytes || !d_out || !out_off || !out_len))) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  int r = uc::compact_batch(c->env, uint32_t(njobs), d_texts, bytes, k, l, d_out, out_cap, out_off, out_len, stats);
+  c->env.reset();
+  if (r == UC_EINPUT && c->env.err.find("batched jobs need") != std::string::npos) {
+    // a job with another line layout: compact the jobs one by one
+    uint64_t base = 0;
+    for (int j = 0; j < njobs; ++j) {
+      const uint64_t cap = uc::output_bound(bytes[j], k);
+      uint64_t ob = 0;
+      uc_stats one{};
+      r = uc::compact_device(c->env, d_texts[j], bytes[j], k, l, d_out + base, cap, ob, stats ? &one : nullptr);
+      c->env.reset();
+      if (r) return as_status(r);
+      out_off[j] = base;
+      out_len[j] = ob;
+      if (stats) {
+        stats->n_kmers += one.n_kmers;
+        stats->out_bytes += one.out_bytes;
+        stats->ms_total += one.ms_total;
+      }
+      base += (cap + 15) & ~uint64_t(15);
+    }
+    return UC_OK;
+  }
   return as_status(r);
 }
 

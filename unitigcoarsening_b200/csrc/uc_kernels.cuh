@@ -27,6 +27,19 @@ struct Counters {
   uint32_t wtile_next;
 };
 
+// One job of a batch (a single call is a batch of one).  Its k-mers occupy
+// keys[koff, koff + n); its buckets are (job << job_bits) | local; its lines
+// go to out[obase, obase + ocap); its open segments use ids
+// [seg_base, seg_base + seg_cap).
+struct JobTab {
+  const uint8_t* text;
+  unsigned long long tbytes, body, end, n, koff, lb0;  // lb0: first 256-line block
+  unsigned long long obase, ocap;
+  uint32_t seg_base, seg_cap;
+  uint32_t fixed;  // every line is k chars + '\n'
+  uint32_t err;    // header/layout problems found on the device
+};
+
 struct TileParams {
   const uint64_t* pkeys;        // copies (NW words each, role bits in the last word)
   const uint32_t* plink;        // cross index (fused) or k-mer id (edges)
@@ -36,6 +49,11 @@ struct TileParams {
   const uint32_t* wlist;        // warp-tier tile ids
   const uint32_t* blist;        // block-tier tile ids
   uint32_t wcap, wts, wbytes;   // warp tiles: capacity, hash slots, shared bytes per warp
+  const JobTab* jobs;
+  const uint32_t* tile_job;     // job of each tile
+  unsigned long long* jout;     // per-job closed-line cursor (bytes)
+  uint32_t* jseg;               // per-job segment cursor
+  uint32_t* seg_job;            // job of each segment
   char* big_scratch;
   const unsigned long long* big_off;
   int k;

@@ -130,26 +130,42 @@ constexpr int PACK_WORDS = PACK_SPAN / 4 + PACK_SPAN / 32 + 32;
 
 __device__ __forceinline__ uint32_t pad_word(uint32_t byte_off) { return (byte_off >> 2) + (byte_off >> 5); }
 
+__device__ __forceinline__ uint32_t job_of_block(const JobTab* __restrict__ jobs, uint32_t njobs, uint64_t g) {
+  uint32_t lo = 0, hi = njobs;  // last job with lb0 <= g
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (jobs[mid].lb0 <= g) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <int NW, bool FUSE>
-__global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, uint64_t tbytes,
-                                              uint64_t body, uint64_t end,
-                                              const unsigned long long* __restrict__ starts,
-                                              uint32_t stride, uint64_t n, int k,
-                                              uint64_t* __restrict__ keys, uint32_t* err, int l,
-                                              uint64_t seed, uint32_t bbits, uint32_t* __restrict__ b1,
-                                              uint32_t* __restrict__ b2, uint32_t* __restrict__ counts) {
+__global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, uint32_t njobs, uint64_t nblocks,
+                                              const unsigned long long* __restrict__ starts, int k,
+                                              uint64_t* __restrict__ keys, uint32_t* err, int l, uint64_t seed,
+                                              uint32_t jb, uint32_t* __restrict__ b1, uint32_t* __restrict__ b2,
+                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ jcross) {
   __shared__ uint32_t buf[PACK_WORDS];
-  const uintptr_t tb = reinterpret_cast<uintptr_t>(text);
+  __shared__ uint32_t s_cross;
   uint32_t bad = 0;
+  const uint32_t stride = uint32_t(k) + 1;
   const uint64_t kmask_hi = (NW == 1) ? ((k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull))
                                       : ((2 * k - 64 >= 64) ? ~0ull : ((1ull << (2 * k - 64)) - 1ull));
-  for (uint64_t b0 = uint64_t(blockIdx.x) * PACK_LINES; b0 < n; b0 += uint64_t(gridDim.x) * PACK_LINES) {
+  for (uint64_t g = blockIdx.x; g < nblocks; g += gridDim.x) {
+    const uint32_t j = job_of_block(jobs, njobs, g);
+    const uint8_t* text = jobs[j].text;
+    const uint64_t tbytes = jobs[j].tbytes, body = jobs[j].body, end = jobs[j].end, n = jobs[j].n;
+    const uint64_t koff = jobs[j].koff;
+    const uint64_t b0 = (g - jobs[j].lb0) * PACK_LINES;
+    const uintptr_t tb = reinterpret_cast<uintptr_t>(text);
     const uint32_t cnt = uint32_t((n - b0) < PACK_LINES ? (n - b0) : PACK_LINES);
     const uint64_t s0 = starts ? uint64_t(starts[b0]) : body + b0 * stride;
     const uint64_t s1 = (b0 + cnt < n) ? (starts ? uint64_t(starts[b0 + cnt]) : body + (b0 + cnt) * stride) : end;
     const uintptr_t A0 = (tb + s0) & ~uintptr_t(15);
     const uint64_t span = (tb + s1) - A0;
     const bool staged = span + 16 <= PACK_SPAN;
+    if (threadIdx.x == 0) s_cross = 0;
     if (staged) {
       const uint32_t nch = uint32_t((span + 15) / 16);
       for (uint32_t c = threadIdx.x; c < nch; c += blockDim.x) {
@@ -177,6 +193,7 @@ __global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, 
     }
     __syncthreads();
     const uint32_t t = threadIdx.x;
+    uint32_t mycross = 0;
     if (t < cnt) {
       const uint64_t line = b0 + t;
       const uint64_t s = starts ? uint64_t(starts[line]) : body + line * stride;
@@ -194,23 +211,22 @@ __global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, 
         uint32_t cur = buf[pad_word(base)];
         const int nwords = (k + 4) / 4;  // covers chars 0..k (k chars + terminator)
 #pragma unroll 4
-        for (int j = 0; j < nwords; ++j) {
-          const uint32_t nxt = buf[pad_word(base + 4u * (j + 1))];
+        for (int jw = 0; jw < nwords; ++jw) {
+          const uint32_t nxt = buf[pad_word(base + 4u * (jw + 1))];
           const uint32_t x = __funnelshift_r(cur, nxt, sh);
           cur = nxt;
           uint32_t nl;
           const uint32_t tc = swar_codes(x, &nl);
-          // bytes of this word that are k-mer chars
-          const int c0 = 4 * j;
+          const int c0 = 4 * jw;
           const uint32_t inmask = (c0 + 4 <= k) ? 0xFFFFFFFFu : (c0 >= k ? 0u : (0xFFFFFFFFu >> (8 * (c0 + 4 - k))));
           lbad |= (nl & inmask) != 0;
           if (check_term && c0 <= k && k < c0 + 4) {
             const uint32_t tbyte = (x >> (8 * (k - c0))) & 0xFFu;
             lbad |= (tbyte != '\n');
           }
-          const uint64_t g = uint64_t(gather_codes(tc & inmask));
-          if (NW == 1 || c0 < 32) key.w[0] |= g << (2 * c0);
-          else key.w[NW - 1] |= g << (2 * (c0 - 32));
+          const uint64_t gc = uint64_t(gather_codes(tc & inmask));
+          if (NW == 1 || c0 < 32) key.w[0] |= gc << (2 * c0);
+          else key.w[NW - 1] |= gc << (2 * (c0 - 32));
         }
       } else {
         for (int c = 0; c <= k; ++c) {
@@ -228,21 +244,62 @@ __global__ void __launch_bounds__(256) k_pack(const uint8_t* __restrict__ text, 
       }
       key.w[NW - 1] &= kmask_hi;
       if (lbad) bad = 1;
-      st_key<NW>(keys, line, key);
+      st_key<NW>(keys, koff + line, key);
       if constexpr (FUSE) {
         uint32_t a, b;
         lmins<NW>(key, k, l, seed, nullptr, a, b);
-        a = bucket_of(a, bbits);
-        b = bucket_of(b, bbits);
-        b1[line] = a;
-        b2[line] = b;
+        const uint32_t jp = j << jb;
+        a = jp | bucket_of(a, jb);
+        b = jp | bucket_of(b, jb);
+        b1[koff + line] = a;
+        b2[koff + line] = b;
         atomicAdd(counts + a, 1u);
-        if (a != b) atomicAdd(counts + b, 1u);
+        if (a != b) {
+          atomicAdd(counts + b, 1u);
+          mycross = 1;
+        }
       }
     }
+    if constexpr (FUSE) {
+      mycross = __reduce_add_sync(0xFFFFFFFFu, mycross);
+      if ((threadIdx.x & 31) == 0 && mycross) atomicAdd(&s_cross, mycross);
+    }
     __syncthreads();
+    if (FUSE && threadIdx.x == 0 && s_cross) atomicAdd(jcross + j, s_cross);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(err, starts ? ERR_LINE : ERR_LAYOUT);
+}
+
+// Header and end of every job's text (batches of more than one job): the
+// count line, the first k-mer line, the end of the last line, and whether
+// every line is k chars + '\n'.  One thread per job.
+__global__ void k_headers(JobTab* __restrict__ jobs, uint32_t njobs, int k) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  JobTab J = jobs[j];
+  const uint8_t* t = J.text;
+  const uint64_t bytes = J.tbytes;
+  uint64_t p = 0;
+  while (p < bytes && (t[p] == ' ' || t[p] == '\t' || t[p] == '\r')) ++p;
+  uint32_t e = 0;
+  uint64_t v = 0;
+  if (p >= bytes || t[p] < '0' || t[p] > '9') e = 1;
+  while (!e && p < bytes && t[p] >= '0' && t[p] <= '9') {
+    v = v * 10 + uint64_t(t[p] - '0');
+    if (v > 0x7FFFFFFEull) e = 1;
+    ++p;
+  }
+  while (p < bytes && t[p] != '\n') ++p;
+  const uint64_t body = (p < bytes) ? p + 1 : bytes;
+  uint64_t end = bytes;
+  while (end > body && (t[end - 1] == '\n' || t[end - 1] == '\r')) --end;
+  J.n = e ? 0 : v;
+  J.body = body;
+  J.end = end;
+  J.err = e;
+  const uint64_t stride = uint64_t(k) + 1;
+  J.fixed = (!e && ((J.n == 0 && end == body) || (J.n > 0 && end - body == J.n * stride - 1))) ? 1u : 0u;
+  jobs[j] = J;
 }
 
 // Line starts for the general layout: '\n' positions in [body, end).
@@ -327,23 +384,28 @@ __global__ void __launch_bounds__(256) k_lmin_count(const uint64_t* __restrict__
 // copies, or when it or its predecessor is larger than `small` (such buckets
 // sit alone).  Every packed tile then holds < win + small <= capacity copies.
 __global__ void k_tile_flags(const uint32_t* __restrict__ counts, const unsigned long long* __restrict__ off,
-                             uint32_t m, uint32_t win, uint32_t small, uint32_t* __restrict__ flag) {
+                             uint32_t m, uint32_t win, uint32_t small, uint32_t jb, uint32_t* __restrict__ flag) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < m; b += gridDim.x * blockDim.x) {
     uint32_t f = (b == 0);
     if (b > 0) {
       f |= (off[b] / win) != (off[b - 1] / win);
       f |= counts[b] > small;
       f |= counts[b - 1] > small;
+      f |= (b >> jb) != ((b - 1) >> jb);  // tiles never mix jobs
     }
     flag[b] = f;
   }
 }
 
 __global__ void k_tile_write(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ fidx,
-                             const unsigned long long* __restrict__ off, uint32_t m,
-                             unsigned long long* __restrict__ tile_begin, Counters* ctr) {
+                             const unsigned long long* __restrict__ off, uint32_t m, uint32_t jb,
+                             unsigned long long* __restrict__ tile_begin, uint32_t* __restrict__ tile_job,
+                             Counters* ctr) {
   for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < m; b += gridDim.x * blockDim.x) {
-    if (flag[b]) tile_begin[fidx[b]] = off[b];
+    if (flag[b]) {
+      tile_begin[fidx[b]] = off[b];
+      tile_job[fidx[b]] = b >> jb;
+    }
     if (b == m - 1) {
       const uint32_t nt = fidx[b] + flag[b];
       tile_begin[nt] = off[m];
@@ -657,14 +719,18 @@ __device__ __forceinline__ U3 block_excl_scan3(U3 v, U3* sc, U3* total) {
 }
 
 // Reserve a tile's closed-line bytes, open-segment chars and segment ids.
-__device__ __forceinline__ int reserve_space(const TileParams& p, const U3& tot, unsigned long long* b) {
-  b[0] = tot.a ? atomicAdd(&p.ctr->out_cursor, tot.a) : 0ull;
+__device__ __forceinline__ int reserve_space(const TileParams& p, uint32_t job, const U3& tot,
+                                             unsigned long long* b) {
+  const JobTab& J = p.jobs[job];
+  b[0] = tot.a ? atomicAdd(p.jout + job, tot.a) : 0ull;
   b[1] = tot.b ? atomicAdd(&p.ctr->seg_char_cursor, tot.b) : 0ull;
-  b[2] = tot.c ? atomicAdd(&p.ctr->seg_count, uint32_t(tot.c)) : 0u;
-  if (b[0] + tot.a > p.out_cap || b[1] + tot.b > p.segchars_cap || b[2] + tot.c > p.seg_cap) {
+  b[2] = tot.c ? atomicAdd(p.jseg + job, uint32_t(tot.c)) : 0u;
+  if (b[0] + tot.a > J.ocap || b[1] + tot.b > p.segchars_cap || b[2] + tot.c > J.seg_cap) {
     atomicOr(&p.ctr->err, ERR_CAPACITY);
     return 0;
   }
+  b[0] += J.obase;
+  b[2] += J.seg_base;
   return 1;
 }
 
@@ -679,10 +745,11 @@ struct BlockGroup {
     return block_excl_scan3(v, sc, total);
   }
   // The leader reserves output space for the tile; false if a bound was hit.
-  static __device__ __forceinline__ bool reserve(const TileParams& p, const U3& tot, unsigned long long* base) {
+  static __device__ __forceinline__ bool reserve(const TileParams& p, uint32_t job, const U3& tot,
+                                                 unsigned long long* base) {
     __shared__ unsigned long long s_base[3];
     __shared__ int s_ok;
-    if (threadIdx.x == 0) s_ok = reserve_space(p, tot, s_base);
+    if (threadIdx.x == 0) s_ok = reserve_space(p, job, tot, s_base);
     __syncthreads();
     base[0] = s_base[0];
     base[1] = s_base[1];
@@ -710,10 +777,11 @@ struct WarpGroup {
                 __shfl_sync(0xFFFFFFFFu, inc.c, 31)};
     return U3{inc.a - v.a, inc.b - v.b, inc.c - v.c};
   }
-  static __device__ __forceinline__ bool reserve(const TileParams& p, const U3& tot, unsigned long long* base) {
+  static __device__ __forceinline__ bool reserve(const TileParams& p, uint32_t job, const U3& tot,
+                                                 unsigned long long* base) {
     unsigned long long b[3] = {0, 0, 0};
     int ok = 1;
-    if ((threadIdx.x & 31) == 0) ok = reserve_space(p, tot, b);
+    if ((threadIdx.x & 31) == 0) ok = reserve_space(p, job, tot, b);
     base[0] = __shfl_sync(0xFFFFFFFFu, b[0], 0);
     base[1] = __shfl_sync(0xFFFFFFFFu, b[1], 0);
     base[2] = __shfl_sync(0xFFFFFFFFu, b[2], 0);
@@ -745,7 +813,8 @@ __device__ void jump_rounds(uint32_t c, IT* px, IT* rx, IT* py, IT* ry, IT*& ptr
 }
 
 template <int NW, typename IT, typename G>
-__device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint64_t beg, uint32_t c) {
+__device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint64_t beg, uint32_t c,
+                             uint32_t job) {
   constexpr uint32_t NONE_I = Ix<IT>::NONE, DUP_I = Ix<IT>::DUP, CNONE_I = Ix<IT>::CNONE;
   const PrefMask pm = pref_mask(p.k);
   const uint32_t ts = pow2_at_least(2ull * c);  // this tile's slots (<= m.ts)
@@ -913,7 +982,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   U3 tot;
   U3 pre = G::scan3(mine, &tot);
   unsigned long long s_base[3];
-  if (!G::reserve(p, tot, s_base)) return;
+  if (!G::reserve(p, job, tot, s_base)) return;
   const unsigned long long cbase = s_base[0], obase = s_base[1], sbase = s_base[2];
   for (uint32_t i = lo; i < hi; ++i) {
     if (m.A[i] != NONE_I) continue;
@@ -961,6 +1030,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
         const bool p_only = (roles(x) & ROLE_S) == 0;
         p.seg_off[g] = obase + loc;
         p.seg_len[g] = r + 1;
+        p.seg_job[g] = job;
         const uint32_t sx = s_only ? p.plink[beg + s] : NONE;
         const uint32_t ex = p_only ? p.plink[beg + i] : NONE;
         p.seg_sx[g] = sx;
@@ -991,7 +1061,7 @@ __global__ void __launch_bounds__(256) k_tile_warp(TileParams p) {
     const uint32_t t = p.wlist[j];
     const uint64_t beg = p.tile_begin[t];
     const uint32_t c = uint32_t(p.tile_begin[t + 1] - beg);
-    process_tile<NW, uint16_t, WarpGroup>(p, m, beg, c);
+    process_tile<NW, uint16_t, WarpGroup>(p, m, beg, c, p.tile_job[t]);
     __syncwarp();
   }
 }
@@ -1011,7 +1081,7 @@ __global__ void __launch_bounds__(512) k_tile(TileParams p) {
     const uint32_t t = p.blist[j];
     const uint64_t beg = p.tile_begin[t];
     const uint32_t c = uint32_t(p.tile_begin[t + 1] - beg);
-    process_tile<NW, uint16_t, BlockGroup>(p, m, beg, c);
+    process_tile<NW, uint16_t, BlockGroup>(p, m, beg, c, p.tile_job[t]);
     __syncthreads();
   }
 }
@@ -1024,7 +1094,7 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
   const uint64_t c = p.tile_begin[t + 1] - beg;
   const uint32_t ts = pow2_at_least(2 * c);
   const TileMem<NW, uint32_t> m = carve<NW, uint32_t>(p.big_scratch + p.big_off[blockIdx.x], uint32_t(c), ts);
-  process_tile<NW, uint32_t, BlockGroup>(p, m, beg, uint32_t(c));
+  process_tile<NW, uint32_t, BlockGroup>(p, m, beg, uint32_t(c), p.tile_job[t]);
 }
 
 // ================================================================= stitch
@@ -1033,13 +1103,19 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
 // of cross k-mer x continues with the segment starting at x's S-only copy;
 // both hold x, so every later segment drops its first k chars
 // (write_unitigs4, compact.h:59-112).
-__global__ void k_seg_link(const Counters* __restrict__ ctr, const uint32_t* __restrict__ seg_sx,
+// Segment ids come from per-job pools; an unused id has length 0.
+__global__ void k_seg_link(uint32_t S, const uint32_t* __restrict__ seg_sx,
                            const uint32_t* __restrict__ seg_ex, const uint32_t* __restrict__ seg_len,
                            const uint32_t* __restrict__ start_seg, const uint32_t* __restrict__ end_seg,
                            uint32_t* __restrict__ next, uint32_t* __restrict__ prev,
                            uint32_t* __restrict__ w, int k) {
-  const uint32_t S = ctr->seg_count;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+    if (seg_len[s] == 0) {
+      next[s] = NONE;
+      prev[s] = NONE;
+      w[s] = 0;
+      continue;
+    }
     const uint32_t ex = seg_ex[s], sx = seg_sx[s];
     const uint32_t nx = (ex == NONE) ? NONE : start_seg[ex];
     const uint32_t pv = (sx == NONE) ? NONE : end_seg[sx];
@@ -1099,40 +1175,42 @@ __global__ void k_rank_round(unsigned long long* __restrict__ X, const uint32_t*
 }
 
 // Line length of each chain, stored at its head.
-__global__ void k_chain_len(const Counters* __restrict__ ctr, const unsigned long long* __restrict__ X,
+__global__ void k_chain_len(uint32_t S, const uint32_t* __restrict__ seg_len, const unsigned long long* __restrict__ X,
                             const uint32_t* __restrict__ next, const uint32_t* __restrict__ w,
                             const uint8_t* __restrict__ oncycle, uint32_t* __restrict__ linelen) {
-  const uint32_t S = ctr->seg_count;
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
-    if (next[s] == NONE && !oncycle[s]) {
+    if (seg_len[s] && next[s] == NONE && !oncycle[s]) {
       const unsigned long long v = X[s];
       linelen[ptr_of(v)] = pk_o(v) + w[s] + 1u;
     }
   }
 }
 
-__global__ void k_head_len(const Counters* __restrict__ ctr, const uint32_t* __restrict__ prev,
-                           const uint32_t* __restrict__ linelen, uint32_t* __restrict__ v) {
-  const uint32_t S = ctr->seg_count;
+__global__ void k_head_len(uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ prev,
+                           const uint8_t* __restrict__ oncycle, const uint32_t* __restrict__ linelen,
+                           uint32_t* __restrict__ v) {
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x)
-    v[s] = (prev[s] == NONE) ? linelen[s] : 0u;
+    v[s] = (seg_len[s] && prev[s] == NONE && !oncycle[s]) ? linelen[s] : 0u;
 }
 
 // Copy each segment's chars into its line (warp per segment).
-__global__ void k_seg_copy(Counters* __restrict__ ctr, const unsigned long long* __restrict__ X,
+__global__ void k_seg_copy(uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
+                           const JobTab* __restrict__ jobs, const unsigned long long* __restrict__ jclosed,
+                           const unsigned long long* __restrict__ X,
                            const uint32_t* __restrict__ next, const uint32_t* __restrict__ prev,
                            const uint32_t* __restrict__ w, const uint8_t* __restrict__ oncycle,
                            const unsigned long long* __restrict__ seg_off,
                            const unsigned long long* __restrict__ loff, const char* __restrict__ segchars,
-                           char* __restrict__ out, unsigned long long base, int k) {
-  const uint32_t S = ctr->seg_count;
+                           char* __restrict__ out, int k) {
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
   for (uint32_t s = warp; s < S; s += nwarps) {
-    if (oncycle[s]) continue;
+    if (!seg_len[s] || oncycle[s]) continue;
     const unsigned long long v = X[s];
-    char* dst = out + base + loff[ptr_of(v)] + pk_o(v);
+    const uint32_t job = seg_job[s];
+    const JobTab& J = jobs[job];
+    char* dst = out + J.obase + jclosed[job] + (loff[ptr_of(v)] - loff[J.seg_base]) + pk_o(v);
     const char* src = segchars + seg_off[s] + ((prev[s] == NONE) ? 0 : k);
     const uint32_t nb = w[s];
     for (uint32_t j = lane; j < nb; j += 32) dst[j] = src[j];
@@ -1151,12 +1229,12 @@ __global__ void k_mark_cycle(const uint32_t* __restrict__ act, const uint32_t* a
 // smallest k-mer.  The cycle's distinct k-mers are the last chars of each
 // segment after its first k-mer, read circularly.
 template <int NW>
-__global__ void k_seg_cycles(Counters* ctr, const uint32_t* __restrict__ act, uint32_t na,
+__global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restrict__ act, uint32_t na,
                              uint8_t* __restrict__ oncycle, const uint32_t* __restrict__ next,
-                             const uint32_t* __restrict__ seg_len,
+                             const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
+                             const JobTab* __restrict__ jobs, unsigned long long* __restrict__ jout,
                              const unsigned long long* __restrict__ seg_off,
-                             const char* __restrict__ segchars, char* __restrict__ out,
-                             unsigned long long out_cap, int k) {
+                             const char* __restrict__ segchars, char* __restrict__ out, int k) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   for (uint32_t j = 0; j < na; ++j) {
     const uint32_t s0 = act[j];
@@ -1164,7 +1242,6 @@ __global__ void k_seg_cycles(Counters* ctr, const uint32_t* __restrict__ act, ui
     // total distinct k-mers N and the circular char accessor
     uint64_t N = 0;
     uint32_t s = s0, steps = 0;
-    const uint32_t S = ctr->seg_count;
     do {
       N += seg_len[s] - 1u;
       oncycle[s] = 2;
@@ -1206,19 +1283,28 @@ __global__ void k_seg_cycles(Counters* ctr, const uint32_t* __restrict__ act, ui
       if (key_lt(x, bk)) { bk = x; best = q; }
     }
     const uint64_t len = uint64_t(k) + N;  // k + (N - 1) chars + '\n'
-    const unsigned long long o = atomicAdd(&ctr->out_cursor, len);
-    if (o + len > out_cap) {
+    const uint32_t job = seg_job[s0];
+    const unsigned long long o = atomicAdd(jout + job, len);
+    if (o + len > jobs[job].ocap) {
       atomicOr(&ctr->err, ERR_CAPACITY);
       return;
     }
-    for (uint64_t t = 0; t + 1 < len; ++t) out[o + t] = at((best + N * 64 - (k - 1) + t) % N);
-    out[o + len - 1] = '\n';
+    char* dst = out + jobs[job].obase + o;
+    for (uint64_t t = 0; t + 1 < len; ++t) dst[t] = at((best + N * 64 - (k - 1) + t) % N);
+    dst[len - 1] = '\n';
     atomicAdd(&ctr->cycles, 1ull);
   }
 }
 
-__global__ void k_add_cursor(Counters* ctr, const unsigned long long* total) {
-  ctr->out_cursor += *total;
+// After the copy: each job's byte count = closed lines + stitched lines
+// (the scan total over its segment pool range).
+__global__ void k_job_finish(const JobTab* __restrict__ jobs, uint32_t njobs,
+                             const unsigned long long* __restrict__ jclosed,
+                             const unsigned long long* __restrict__ loff, unsigned long long* __restrict__ jout) {
+  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x) {
+    const JobTab& J = jobs[j];
+    jout[j] = jclosed[j] + (loff[J.seg_base + J.seg_cap] - loff[J.seg_base]);
+  }
 }
 
 // ===================================================== HEC contraction
@@ -1648,56 +1734,89 @@ static size_t line_index_bytes(size_t bytes, uint64_t n) {
 struct FuseArgs {
   int l = 0;
   uint64_t seed = 0;
-  uint32_t bbits = 0;
-  uint32_t *b1 = nullptr, *b2 = nullptr, *counts = nullptr;
+  uint32_t jb = 0;
+  uint32_t *b1 = nullptr, *b2 = nullptr, *counts = nullptr, *jcross = nullptr;
   uint64_t M = 0;
 };
 
 template <int NW>
-static void launch_pack(Env& e, const uint8_t* text, size_t bytes, uint64_t body, uint64_t end,
-                        const unsigned long long* starts, uint32_t stride, uint64_t n, int k, uint64_t* keys,
-                        const FuseArgs* fz) {
-  const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>((n + PACK_LINES - 1) / PACK_LINES,
-                                                                 uint64_t(e.sm_count) * 8)));
+static void launch_pack(Env& e, const JobTab* jobs, uint32_t njobs, uint64_t nblocks,
+                        const unsigned long long* starts, int k, uint64_t* keys, const FuseArgs* fz) {
+  const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(nblocks, uint64_t(e.sm_count) * 8)));
   ++e.launches;
   if (fz)
-    k_pack<NW, true><<<grid, 256, 0, e.stream>>>(text, bytes, body, end, starts, stride, n, k, keys, &e.ctr->err,
-                                                 fz->l, fz->seed, fz->bbits, fz->b1, fz->b2, fz->counts);
+    k_pack<NW, true><<<grid, 256, 0, e.stream>>>(jobs, njobs, nblocks, starts, k, keys, &e.ctr->err, fz->l,
+                                                 fz->seed, fz->jb, fz->b1, fz->b2, fz->counts, fz->jcross);
   else
-    k_pack<NW, false><<<grid, 256, 0, e.stream>>>(text, bytes, body, end, starts, stride, n, k, keys, &e.ctr->err,
-                                                  0, 0, 0, nullptr, nullptr, nullptr);
+    k_pack<NW, false><<<grid, 256, 0, e.stream>>>(jobs, njobs, nblocks, starts, k, keys, &e.ctr->err, 0, 0, 0,
+                                                  nullptr, nullptr, nullptr, nullptr);
 }
 
-// Text -> keys (and, with fz, minimizer buckets + counts).  The general line
-// layout uses the back arena for its line index; it must be empty.
-static int pack_impl(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t& n_out,
-                     const FuseArgs* fz) {
-  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
-  uint64_t n = 0, body = 0, end = 0;
-  int st = parse_header(e, d_text, bytes, n, body);
-  if (st) return st;
-  st = text_end(e, d_text, bytes, body, end);
-  if (st) return st;
-  n_out = n;
+// Grow-only device buffers for the job table and the per-job counters.
+static int job_buffers(Env& e, uint32_t njobs) {
+  const size_t want = size_t(njobs) * (sizeof(JobTab) + 4 * 8) + 1024;
+  if (want <= e.jcap) return UC_OK;
+  if (e.jbuf) {
+    cudaStreamSynchronize(e.stream);
+    cudaFree(e.jbuf);
+  }
+  e.jbuf = nullptr;
+  e.jcap = 0;
+  if (cudaMalloc(&e.jbuf, want) != cudaSuccess) {
+    cudaGetLastError();
+    e.jbuf = nullptr;
+    return e.fail(UC_ENOMEM, "job table");
+  }
+  e.jcap = want;
+  return UC_OK;
+}
+struct JobDev {
+  JobTab* tab;
+  uint32_t* jcross;
+  uint32_t* jseg;
+  unsigned long long* jout;
+  unsigned long long* jclosed;
+};
+static JobDev job_dev(Env& e, uint32_t njobs) {
+  JobDev d;
+  d.tab = reinterpret_cast<JobTab*>(e.jbuf);
+  char* q = e.jbuf + ((size_t(njobs) * sizeof(JobTab) + 255) & ~size_t(255));
+  d.jout = reinterpret_cast<unsigned long long*>(q);
+  d.jclosed = d.jout + njobs;
+  d.jcross = reinterpret_cast<uint32_t*>(d.jclosed + njobs);
+  d.jseg = d.jcross + njobs;
+  return d;
+}
+
+// Text -> keys for one job (and, with fz, buckets + counts).  Fixed-width
+// lines are packed directly; any other layout indexes the line starts first
+// (back arena, which must be empty).
+static int pack_single(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, const FuseArgs* fz,
+                       JobTab& J, JobTab* jdev) {
   const uint8_t* text = reinterpret_cast<const uint8_t*>(d_text);
+  const uint64_t n = J.n, body = J.body, end = J.end;
   UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
   if (n == 0) {
     if (end > body) return e.fail(UC_EINPUT, "header count differs from the number of lines");
     return UC_OK;
   }
   const int nw = (k <= 31) ? 1 : 2;
-  const uint32_t stride = uint32_t(k) + 1;
-  bool fixed = (end - body) == n * stride - 1;
+  const uint64_t nblocks = (n + PACK_LINES - 1) / PACK_LINES;
+  bool fixed = J.fixed != 0;
+  int st;
   if (fixed) {
-    if (nw == 1) launch_pack<1>(e, text, bytes, body, end, nullptr, stride, n, k, d_keys, fz);
-    else launch_pack<2>(e, text, bytes, body, end, nullptr, stride, n, k, d_keys, fz);
+    if (nw == 1) launch_pack<1>(e, jdev, 1, nblocks, nullptr, k, d_keys, fz);
+    else launch_pack<2>(e, jdev, 1, nblocks, nullptr, k, d_keys, fz);
     UC_CK(cudaGetLastError());
     st = e.read_ctr();
     if (st) return st;
     if (e.h_ctr->err & ERR_LAYOUT) {
       fixed = false;
       UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
-      if (fz) UC_CK(cudaMemsetAsync(fz->counts, 0, fz->M * 4, e.stream));
+      if (fz) {
+        UC_CK(cudaMemsetAsync(fz->counts, 0, fz->M * 4, e.stream));
+        UC_CK(cudaMemsetAsync(fz->jcross, 0, 4, e.stream));
+      }
     } else if (e.h_ctr->err) {
       return e.check_err(e.h_ctr);
     }
@@ -1722,8 +1841,8 @@ static int pack_impl(Env& e, const char* d_text, size_t bytes, int k, uint64_t* 
     if (lines_m1 + 1 != n) return e.fail(UC_EINPUT, "header count differs from the number of lines");
     ++e.launches;
     k_write_starts<<<unsigned(nchunks), 256, 0, e.stream>>>(text, body, end, off, chunk, starts, n);
-    if (nw == 1) launch_pack<1>(e, text, bytes, body, end, starts, stride, n, k, d_keys, fz);
-    else launch_pack<2>(e, text, bytes, body, end, starts, stride, n, k, d_keys, fz);
+    if (nw == 1) launch_pack<1>(e, jdev, 1, nblocks, starts, k, d_keys, fz);
+    else launch_pack<2>(e, jdev, 1, nblocks, starts, k, d_keys, fz);
     UC_CK(cudaGetLastError());
     st = e.read_ctr();
     e.ar[1].used = 0;
@@ -1733,9 +1852,36 @@ static int pack_impl(Env& e, const char* d_text, size_t bytes, int k, uint64_t* 
   return UC_OK;
 }
 
+// Host view of one job's text: count line, body offset, end, layout.
+static int host_job(Env& e, const char* d_text, size_t bytes, int k, JobTab& J) {
+  uint64_t n = 0, body = 0, end = 0;
+  int st = parse_header(e, d_text, bytes, n, body);
+  if (st) return st;
+  st = text_end(e, d_text, bytes, body, end);
+  if (st) return st;
+  J = JobTab{};
+  J.text = reinterpret_cast<const uint8_t*>(d_text);
+  J.tbytes = bytes;
+  J.n = n;
+  J.body = body;
+  J.end = end;
+  const uint64_t stride = uint64_t(k) + 1;
+  J.fixed = ((n == 0 && end == body) || (n > 0 && end - body == n * stride - 1)) ? 1u : 0u;
+  return UC_OK;
+}
+
 int pack(Env& e, const char* d_text, size_t bytes, int k, uint64_t* d_keys, uint64_t& n_out) {
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
   e.reset();
-  const int r = pack_impl(e, d_text, bytes, k, d_keys, n_out, nullptr);
+  JobTab J;
+  int r = host_job(e, d_text, bytes, k, J);
+  if (r) return r;
+  n_out = J.n;
+  r = job_buffers(e, 1);
+  if (r) return r;
+  JobDev jd = job_dev(e, 1);
+  UC_CK(cudaMemcpyAsync(jd.tab, &J, sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
+  r = pack_single(e, d_text, bytes, k, d_keys, nullptr, J, jd.tab);
   e.reset();
   return r;
 }
@@ -1753,14 +1899,22 @@ int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   return UC_OK;
 }
 
-// Bucket plan for n k-mers.
+// Bucket plan.  A job's buckets are (job << jb) | local: the largest job
+// sizes jb, and njobs << jb buckets in all (rounded up to a power of two,
+// bits = log2 of that).
 struct Plan {
-  uint32_t bbits, cap, win, small, tslots, wcap, wts, wbytes;
+  uint32_t bits, jb, cap, win, small, tslots, wcap, wts, wbytes;
   int l_used;
   uint64_t M;
 };
 
-static Plan plan_buckets(const Env& e, uint64_t n, int k, int l) {
+static uint32_t ceil_log2(uint64_t x) {
+  uint32_t b = 0;
+  while ((1ull << b) < x) ++b;
+  return b;
+}
+
+static Plan plan_buckets(const Env& e, uint64_t nmax, uint32_t njobs, int k, int l) {
   Plan P{};
   const int nw = (k <= 31) ? 1 : 2;
   uint32_t cap = e.tune.tile_capacity ? e.tune.tile_capacity : 4096;
@@ -1770,21 +1924,24 @@ static Plan plan_buckets(const Env& e, uint64_t n, int k, int l) {
   if (wcap > cap) wcap = cap;
   const bool warp_tier = wcap >= 32;
   const uint32_t pack_cap = warp_tier ? wcap : cap;  // tiles are packed for this capacity
-  const uint64_t copies = n + n / 8 + 1;
-  uint32_t bbits = 0;
+  const uint32_t jbits_max = 25 - std::min<uint32_t>(25, ceil_log2(njobs));
+  const uint64_t copies = nmax + nmax / 8 + 1;
+  uint32_t jb = 0;
   if (e.tune.bucket_bits) {
-    bbits = e.tune.bucket_bits;
+    jb = e.tune.bucket_bits;
   } else {
-    while ((copies >> bbits) > pack_cap / 8 && bbits < 25) ++bbits;  // ~capacity/8 copies per bucket
+    while ((copies >> jb) > pack_cap / 8 && jb < 25) ++jb;  // ~capacity/8 copies per bucket
   }
+  jb = std::min(jb, jbits_max);
   // enough l-mers that each bucket gathers several of them
-  const int lmin = int((bbits + 2 + 1) / 2);
+  const int lmin = int((jb + 2 + 1) / 2);
   int lu = std::max(l, lmin);
   lu = std::min(lu, std::min(16, k - 1));
   uint32_t ts = pow2_at_least(uint64_t(cap) * std::max<uint32_t>(200, e.tune.load_factor_pct) / 100);
   if (ts < 2 * cap) ts = pow2_at_least(2ull * cap);
   while (ts > pow2_at_least(2ull * cap) && tile_bytes(nw, cap, ts) > size_t(e.smem_optin)) ts >>= 1;
-  P.bbits = bbits;
+  P.jb = jb;
+  P.bits = ceil_log2(uint64_t(njobs) << jb);
   P.cap = cap;
   P.win = pack_cap - pack_cap / 4;
   P.small = pack_cap / 4;
@@ -1793,7 +1950,7 @@ static Plan plan_buckets(const Env& e, uint64_t n, int k, int l) {
   P.wts = warp_tier ? pow2_at_least(2ull * wcap) : 0;
   P.wbytes = warp_tier ? uint32_t((tile_bytes(nw, wcap, P.wts) + 15) & ~size_t(15)) : 0;
   P.l_used = lu;
-  P.M = 1ull << bbits;
+  P.M = 1ull << P.bits;
   return P;
 }
 
@@ -1801,7 +1958,7 @@ struct Front {
   uint64_t* keys;
   uint32_t *b1, *b2, *counts;
   unsigned long long *boff, *cursor, *fcur, *tile_begin, *scan_tmp;
-  uint32_t *flag, *fidx, *big_list, *wlist, *blist;
+  uint32_t *flag, *fidx, *big_list, *wlist, *blist, *tile_job;
   unsigned long long* big_size;
 };
 
@@ -1811,7 +1968,7 @@ static size_t front_bytes(uint64_t n, int nw, uint64_t M, bool own_keys) {
   if (own_keys) add(n * 8 * nw);
   add(n * 4); add(n * 4); add(M * 4); add((M + 1) * 8); add(M * 8); add(M * 8); add((M + 2) * 8);
   add(scan_tmp_elems(M) * 8); add(M * 4); add((M + 1) * 4); add(M * 4); add(M * 8);
-  add(M * 4); add(M * 4);
+  add(M * 4); add(M * 4); add(M * 4);
   return need;
 }
 
@@ -1831,7 +1988,8 @@ static int take_front(Env& e, uint64_t n, int nw, uint64_t M, bool own_keys, Fro
   f.big_size = static_cast<unsigned long long*>(e.take(0, M * 8));
   f.wlist = static_cast<uint32_t*>(e.take(0, M * 4));
   f.blist = static_cast<uint32_t*>(e.take(0, M * 4));
-  if (!f.blist) return e.fail(UC_EBUDGET, "front arena overflow");
+  f.tile_job = static_cast<uint32_t*>(e.take(0, M * 4));
+  if (!f.tile_job) return e.fail(UC_EBUDGET, "front arena overflow");
   return UC_OK;
 }
 
@@ -1861,37 +2019,33 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
   const uint64_t M = P.M;
   const int gm = grid_for(e, M, 256);
   e.launches += 2 + 6;
-  k_tile_flags<<<gm, 256, 0, e.stream>>>(f.counts, f.boff, uint32_t(M), P.win, P.small, f.flag);
+  k_tile_flags<<<gm, 256, 0, e.stream>>>(f.counts, f.boff, uint32_t(M), P.win, P.small, P.jb, f.flag);
   scan_excl<uint32_t, uint32_t>(f.flag, M, f.fidx, reinterpret_cast<uint32_t*>(f.scan_tmp), e.stream);
-  k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), f.tile_begin, e.ctr);
+  k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), P.jb, f.tile_begin, f.tile_job, e.ctr);
   UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
   if (n > 0) {
     uint32_t mcb, fb;
-    scatter_split(P.bbits, mcb, fb);
+    scatter_split(P.bits, mcb, fb);
     const uint32_t mc = 1u << mcb;
     uint64_t* rkey = reinterpret_cast<uint64_t*>(stage);
     uint32_t* rlink = reinterpret_cast<uint32_t*>(stage + copies * 8ull * nw);
     uint32_t* rbkt = rlink + copies;
-    // coarse cursors: the first position of each coarse partition
     e.launches += 1;
     k_coarse_init<<<grid_for(e, mc, 256), 256, 0, e.stream>>>(f.boff, fb, mc, f.cursor);
     const size_t sm1 = size_t(2 * SC_CHUNK) * (8 * nw + 8) + size_t(mc) * 16 + 16;
     UC_CK(cudaFuncSetAttribute(k_scatter_coarse<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
     UC_CK(cudaFuncSetAttribute(k_scatter_coarse<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
     const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + SC_CHUNK - 1) / SC_CHUNK, uint64_t(e.sm_count) * 6)));
-    // fine cursors start at every bucket's offset (reuses the scan's output
-    // buffer slot after the tiles are planned)
-    unsigned long long* fcur = f.fcur;
-    UC_CK(cudaMemcpyAsync(fcur, f.boff, P.M * 8, cudaMemcpyDeviceToDevice, e.stream));
+    UC_CK(cudaMemcpyAsync(f.fcur, f.boff, M * 8, cudaMemcpyDeviceToDevice, e.stream));
     UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
     const int g2 = e.sm_count * 8;
     e.launches += 2;
     if (nw == 1) {
       k_scatter_coarse<1><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
-      k_scatter_fine<1><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, fcur, pkeys, plink, e.ctr);
+      k_scatter_fine<1><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, f.fcur, pkeys, plink, e.ctr);
     } else {
       k_scatter_coarse<2><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
-      k_scatter_fine<2><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, fcur, pkeys, plink, e.ctr);
+      k_scatter_fine<2><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, f.fcur, pkeys, plink, e.ctr);
     }
     UC_CK(cudaGetLastError());
   }
@@ -1976,7 +2130,7 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   if (n == 0) return UC_OK;
   e.reset();
   const int nw = (k <= 31) ? 1 : 2;
-  const Plan P = plan_buckets(e, n, k, l);
+  const Plan P = plan_buckets(e, n, 1, k, l);
   int r = e.reserve(0, front_bytes(n, nw, P.M, false));
   if (r) return r;
   Front f{};
@@ -1986,8 +2140,8 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
   UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
   ++e.launches;
-  if (nw == 1) k_lmin_count<1><<<grid_for(e, n, 256), 256, 0, e.stream>>>(d_keys, n, k, P.l_used, seed, P.bbits, f.b1, f.b2, f.counts);
-  else k_lmin_count<2><<<grid_for(e, n, 256), 256, 0, e.stream>>>(d_keys, n, k, P.l_used, seed, P.bbits, f.b1, f.b2, f.counts);
+  if (nw == 1) k_lmin_count<1><<<grid_for(e, n, 256), 256, 0, e.stream>>>(d_keys, n, k, P.l_used, seed, P.jb, f.b1, f.b2, f.counts);
+  else k_lmin_count<2><<<grid_for(e, n, 256), 256, 0, e.stream>>>(d_keys, n, k, P.l_used, seed, P.jb, f.b1, f.b2, f.counts);
   uint64_t copies = 0;
   r = bucket_offsets(e, f, P.M, copies);
   if (r) return r;
@@ -2003,6 +2157,7 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   tp.pkeys = pkeys;
   tp.plink = plink;
   tp.tile_begin = f.tile_begin;
+  tp.tile_job = f.tile_job;
   tp.ctr = e.ctr;
   tp.k = k;
   tp.cap = P.cap;
@@ -2021,11 +2176,64 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   return e.check_err(e.h_ctr);
 }
 
-// Weighted list ranking over `prev` by asynchronous pointer jumping, all
-// rounds enqueued without host round trips: round r reads list r%2 with its
-// count in cnt[r] and appends survivors to the other list, count cnt[r+1].
-// A round whose count is 0 returns at once.  The last list holds the
-// entries left on cycles, its count in cnt[rounds].
+// Enqueue `body` through a CUDA graph: capture it, update the cached
+// executable of this slot when the shape key matches (cudaGraphExecUpdate),
+// instantiate otherwise, and launch.  The body must only enqueue work.
+template <class F>
+static int run_graph(Env& e, int slot, uint64_t key, F&& body) {
+  if (!e.use_graphs) {
+    body();
+    return UC_OK;
+  }
+  const uint32_t before = e.launches;
+  // the legacy default stream cannot be captured: capture on an internal
+  // stream joined to the caller's stream by events
+  const cudaStream_t user = e.stream;
+  const bool swap = (user == nullptr || user == cudaStreamLegacy || user == cudaStreamPerThread);
+  if (swap) {
+    if (!e.gstream) UC_CK(cudaStreamCreateWithFlags(&e.gstream, cudaStreamNonBlocking));
+    UC_CK(cudaEventRecord(e.ev[6], user));
+    UC_CK(cudaStreamWaitEvent(e.gstream, e.ev[6], 0));
+    e.stream = e.gstream;
+  }
+  struct Restore {
+    Env& e;
+    cudaStream_t user;
+    bool swap;
+    ~Restore() {
+      if (swap) {
+        cudaEventRecord(e.ev[7], e.stream);
+        cudaStreamWaitEvent(user, e.ev[7], 0);
+        e.stream = user;
+      }
+    }
+  } restore{e, user, swap};
+  UC_CK(cudaStreamBeginCapture(e.stream, cudaStreamCaptureModeThreadLocal));
+  body();
+  cudaGraph_t g = nullptr;
+  UC_CK(cudaStreamEndCapture(e.stream, &g));
+  bool ok = false;
+  if (e.gexec[slot] && e.gkey[slot] == key) {
+    cudaGraphExecUpdateResultInfo info;
+    ok = cudaGraphExecUpdate(e.gexec[slot], g, &info) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+  }
+  if (!ok) {
+    if (e.gexec[slot]) cudaGraphExecDestroy(e.gexec[slot]);
+    e.gexec[slot] = nullptr;
+    const cudaError_t ie = cudaGraphInstantiate(&e.gexec[slot], g, 0);
+    if (ie != cudaSuccess) {
+      cudaGraphDestroy(g);
+      return e.fail(UC_ECUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(ie));
+    }
+    e.gkey[slot] = key;
+  }
+  cudaGraphDestroy(g);
+  UC_CK(cudaGraphLaunch(e.gexec[slot], e.stream));
+  e.graph_nodes += e.launches - before;
+  return UC_OK;
+}
+
 static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t nmax, bool count_on_device,
                       unsigned long long* X, uint32_t* act0, uint32_t* act1, uint32_t* cnt, uint32_t& rounds,
                       uint32_t*& act_final, uint32_t*& cnt_final) {
@@ -2234,92 +2442,159 @@ uint64_t output_bound(size_t text_bytes, int k) {
 // cross k-mers X are counted, holds the n+X bucketed copies and the segment
 // arrays (at most 2X open segments: each holds an S-only start or a P-only
 // end, one of each per cross k-mer).
-int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char* out, uint64_t cap,
-                   uint64_t& out_bytes, uc_stats* st) {
+// The fused path over a batch of jobs (one job is a batch of one).  Device
+// memory: the front arena holds per-k-mer arrays (keys, bucket ids) and
+// per-bucket arrays; the back arena, sized once the cross k-mers are counted,
+// holds the bucketed copies and the segment pools (a job with X cross k-mers
+// has at most 2X open segments: each holds an S-only start or a P-only end).
+int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t* bytes, int k, int l, char* out,
+                  uint64_t out_cap, uint64_t* out_off, uint64_t* out_len, uc_stats* st) {
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
   if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
+  if (njobs == 0) return UC_OK;
   const int nw = (k <= 31) ? 1 : 2;
   e.reset();
   e.launches = 0;
-  uint64_t n = 0, body = 0;
-  int r = parse_header(e, d_text, bytes, n, body);
+  e.graph_nodes = 0;
+  int r = job_buffers(e, njobs);
   if (r) return r;
-  if (n >= 0x7FFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 31-bit ids");
-  const Plan P = plan_buckets(e, n, k, l);
-  r = e.reserve(0, front_bytes(n, nw, P.M, true));
+  JobDev jd = job_dev(e, njobs);
+  std::vector<JobTab> J(njobs);
+  if (njobs == 1) {
+    r = host_job(e, texts[0], bytes[0], k, J[0]);
+    if (r) return r;
+  } else {
+    for (uint32_t j = 0; j < njobs; ++j) {
+      J[j] = JobTab{};
+      J[j].text = reinterpret_cast<const uint8_t*>(texts[j]);
+      J[j].tbytes = bytes[j];
+    }
+    UC_CK(cudaMemcpyAsync(jd.tab, J.data(), njobs * sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
+    ++e.launches;
+    k_headers<<<(njobs + 127) / 128, 128, 0, e.stream>>>(jd.tab, njobs, k);
+    UC_CK(cudaMemcpyAsync(J.data(), jd.tab, njobs * sizeof(JobTab), cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    for (uint32_t j = 0; j < njobs; ++j) {
+      if (J[j].err) return e.fail(UC_EINPUT, "job " + std::to_string(j) + ": missing or too large k-mer count");
+      if (!J[j].fixed)
+        return e.fail(UC_EINPUT, "job " + std::to_string(j) +
+                                     ": batched jobs need k chars + '\\n' per line and a matching count");
+    }
+  }
+  uint64_t N = 0, lb = 0, ob = 0, nmax = 0;
+  for (uint32_t j = 0; j < njobs; ++j) {
+    J[j].koff = N;
+    J[j].lb0 = lb;
+    J[j].obase = ob;
+    J[j].ocap = output_bound(bytes[j], k);
+    N += J[j].n;
+    lb += (J[j].n + PACK_LINES - 1) / PACK_LINES;
+    ob += (J[j].ocap + 15) & ~uint64_t(15);
+    nmax = std::max<uint64_t>(nmax, J[j].n);
+  }
+  if (N >= 0x7FFFFFFFull) return e.fail(UC_EINPUT, "too many k-mers for 31-bit ids");
+  if (ob > out_cap + 15) return e.fail(UC_EINPUT, "output buffer smaller than uc_output_bound");
+  const Plan P = plan_buckets(e, nmax, njobs, k, l);
+  r = e.reserve(0, front_bytes(N, nw, P.M, true));
   if (r) return r;
   Front f{};
-  r = take_front(e, n, nw, P.M, true, f);
+  r = take_front(e, N, nw, P.M, true, f);
   if (r) return r;
   UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
   UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
+  UC_CK(cudaMemsetAsync(jd.jcross, 0, njobs * 4, e.stream));
+  UC_CK(cudaMemcpyAsync(jd.tab, J.data(), njobs * sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
   cudaEventRecord(e.ev[0], e.stream);
   FuseArgs fz;
   fz.l = P.l_used;
   fz.seed = e.seed;
-  fz.bbits = P.bbits;
+  fz.jb = P.jb;
   fz.b1 = f.b1;
   fz.b2 = f.b2;
   fz.counts = f.counts;
+  fz.jcross = jd.jcross;
   fz.M = P.M;
-  uint64_t n2 = 0;
-  r = pack_impl(e, d_text, bytes, k, f.keys, n2, &fz);
-  if (r) return r;
+  if (njobs == 1) {
+    r = pack_single(e, texts[0], bytes[0], k, f.keys, &fz, J[0], jd.tab);
+    if (r) return r;
+  } else if (N > 0) {
+    if (nw == 1) launch_pack<1>(e, jd.tab, njobs, lb, nullptr, k, f.keys, &fz);
+    else launch_pack<2>(e, jd.tab, njobs, lb, nullptr, k, f.keys, &fz);
+    UC_CK(cudaGetLastError());
+  }
   cudaEventRecord(e.ev[1], e.stream);
   uint64_t copies = 0;
   r = bucket_offsets(e, f, P.M, copies);
   if (r) return r;
-  const uint64_t X = copies - n;
-  const uint64_t S = 2 * X + 1;
-  const uint64_t segchars = S * uint64_t(k) + copies + 64;
+  std::vector<uint32_t> xc(njobs);
+  UC_CK(cudaMemcpyAsync(xc.data(), jd.jcross, njobs * 4, cudaMemcpyDeviceToHost, e.stream));
+  r = e.read_ctr();
+  if (r) return r;
+  if (e.h_ctr->err) {
+    if (e.h_ctr->err & ERR_LAYOUT) return e.fail(UC_EINPUT, "a k-mer line is shorter than k");
+    return e.check_err(e.h_ctr);
+  }
+  const uint64_t X = copies - N;
+  uint64_t Sp = 0;
+  for (uint32_t j = 0; j < njobs; ++j) {
+    J[j].seg_base = uint32_t(Sp);
+    J[j].seg_cap = 2 * xc[j] + 1;
+    Sp += J[j].seg_cap;
+  }
+  if (Sp >= 0x7FFFFFF0ull) return e.fail(UC_EINPUT, "too many cross-tile segments");
+  UC_CK(cudaMemcpyAsync(jd.tab, J.data(), njobs * sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
+  const uint64_t segchars = Sp * uint64_t(k) + copies + 64;
   const uint32_t R = 64;
+  const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
+  const uint32_t RH = hec_rounds(Sp);
   size_t back = 0;
   auto add = [&](size_t b) { back += (b + 255) & ~size_t(255); };
-  add(copies * 8 * nw); add(copies * 4);                       // copies
-  add(S * 8); add(S * 4); add(S * 4); add(S * 4);              // seg_off, len, sx, ex
-  add((X + 1) * 4); add((X + 1) * 4);                          // start_seg, end_seg
+  add(copies * 8 * nw); add(copies * 4);                                  // copies
+  add(scatter_stage_bytes(copies, nw));                                   // level-1 staging
+  add(Sp * 8); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // seg_off, len, sx, ex, job
+  add((X + 1) * 4); add((X + 1) * 4);                                     // start_seg, end_seg
   add(segchars);
-  add(S * 4); add(S * 4); add(S * 4); add(S * 4); add(S * 4);  // next, prev, w, act0, act1
-  add(S * 4); add(S * 4); add(S * 8); add((S + 1) * 8); add(S); // llen, hlen, X, loff, oncyc
-  add(scan_tmp_elems(S) * 8); add(8); add(R * 4);
-  add(scatter_stage_bytes(copies, nw));
-  const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
-  const uint32_t RH = hec_rounds(S);
-  if (want_hec) add(hec_bytes(S, RH));
+  add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // next, prev, w, act0, act1
+  add(Sp * 4); add(Sp * 4); add(Sp * 8); add((Sp + 1) * 8); add(Sp);     // llen, hlen, X, loff, oncyc
+  add(scan_tmp_elems(Sp) * 8); add(R * 4);
+  if (want_hec) add(hec_bytes(Sp, RH));
   r = e.reserve(1, back);
   if (r) return r;
   auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
   auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(1, c * 4)); };
   uint64_t* pkeys = reinterpret_cast<uint64_t*>(T64(copies * nw));
   uint32_t* plink = T32(copies);
-  unsigned long long* seg_off = T64(S);
-  uint32_t* seg_len = T32(S);
-  uint32_t* seg_sx = T32(S);
-  uint32_t* seg_ex = T32(S);
+  char* stage = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  unsigned long long* seg_off = T64(Sp);
+  uint32_t* seg_len = T32(Sp);
+  uint32_t* seg_sx = T32(Sp);
+  uint32_t* seg_ex = T32(Sp);
+  uint32_t* seg_job = T32(Sp);
   uint32_t* start_seg = T32(X + 1);
   uint32_t* end_seg = T32(X + 1);
   char* segc = static_cast<char*>(e.take(1, segchars));
-  uint32_t* next = T32(S);
-  uint32_t* prev = T32(S);
-  uint32_t* wgt = T32(S);
-  uint32_t* act0 = T32(S);
-  uint32_t* act1 = T32(S);
-  uint32_t* llen = T32(S);
-  uint32_t* hlen = T32(S);
-  unsigned long long* Xr = T64(S);
-  unsigned long long* loff = T64(S + 1);
-  uint8_t* oncyc = static_cast<uint8_t*>(e.take(1, S));
-  unsigned long long* stmp = T64(scan_tmp_elems(S));
-  unsigned long long* dtotal = T64(1);
+  uint32_t* next = T32(Sp);
+  uint32_t* prev = T32(Sp);
+  uint32_t* wgt = T32(Sp);
+  uint32_t* act0 = T32(Sp);
+  uint32_t* act1 = T32(Sp);
+  uint32_t* llen = T32(Sp);
+  uint32_t* hlen = T32(Sp);
+  unsigned long long* Xr = T64(Sp);
+  unsigned long long* loff = T64(Sp + 1);
+  uint8_t* oncyc = static_cast<uint8_t*>(e.take(1, Sp));
+  unsigned long long* stmp = T64(scan_tmp_elems(Sp));
   uint32_t* rcnt = T32(R);
-  char* stage = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
-  if (!stage) return e.fail(UC_EBUDGET, "back arena overflow");
+  if (!rcnt) return e.fail(UC_EBUDGET, "back arena overflow");
   HecPool hp{};
   if (want_hec) {
-    r = hec_take(e, S, RH, hp);
+    r = hec_take(e, Sp, RH, hp);
     if (r) return r;
   }
-  r = plan_and_scatter(e, f, P, n, nw, 0, pkeys, plink, stage, copies);
+  UC_CK(cudaMemsetAsync(seg_len, 0, Sp * 4, e.stream));
+  UC_CK(cudaMemsetAsync(jd.jout, 0, njobs * 8, e.stream));
+  UC_CK(cudaMemsetAsync(jd.jseg, 0, njobs * 4, e.stream));
+  r = plan_and_scatter(e, f, P, N, nw, 0, pkeys, plink, stage, copies);
   if (r) return r;
   cudaEventRecord(e.ev[2], e.stream);
 
@@ -2327,6 +2602,7 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   tp.pkeys = pkeys;
   tp.plink = plink;
   tp.tile_begin = f.tile_begin;
+  tp.tile_job = f.tile_job;
   tp.ctr = e.ctr;
   tp.k = k;
   tp.cap = P.cap;
@@ -2336,16 +2612,18 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   tp.wbytes = P.wbytes;
   tp.mode = 1;
   tp.out = out;
-  tp.out_cap = cap;
   tp.segchars = segc;
   tp.segchars_cap = segchars;
-  tp.seg_cap = uint32_t(S);
   tp.seg_off = seg_off;
   tp.seg_len = seg_len;
   tp.seg_sx = seg_sx;
   tp.seg_ex = seg_ex;
+  tp.seg_job = seg_job;
   tp.start_seg = start_seg;
   tp.end_seg = end_seg;
+  tp.jobs = jd.tab;
+  tp.jout = jd.jout;
+  tp.jseg = jd.jseg;
   const uint32_t threads = e.tune.tile_threads ? e.tune.tile_threads : 512;
   r = (nw == 1) ? run_tiles<1>(e, tp, f, threads) : run_tiles<2>(e, tp, f, threads);
   if (r) return r;
@@ -2353,76 +2631,97 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   r = e.read_ctr();
   if (r) return r;
   if (e.h_ctr->err) return e.check_err(e.h_ctr);
-  const uint32_t nseg = e.h_ctr->seg_count;
-  const unsigned long long closed_bytes = e.h_ctr->out_cursor;
+  UC_CK(cudaMemcpyAsync(jd.jclosed, jd.jout, njobs * 8, cudaMemcpyDeviceToDevice, e.stream));
   uint32_t rounds = 0;
-  if (nseg) {
-    const int gs = grid_for(e, nseg, 256);
-    e.launches += 1;
-    k_seg_link<<<gs, 256, 0, e.stream>>>(e.ctr, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k);
-    uint32_t *act = nullptr, *left = nullptr;
-    bool hec = want_hec;
-    if (hec) {
-      // HEC rounds; the cycle segments are listed from the flags
-      UC_CK(cudaMemsetAsync(oncyc, 0, nseg, e.stream));
-      hec_contract(e, hp, RH, prev, next, wgt, nseg, true, Xr, oncyc);
-      UC_CK(cudaMemsetAsync(rcnt, 0, 4, e.stream));
+  const uint32_t S = uint32_t(Sp);
+  const int gs = grid_for(e, S, 256);
+  ++e.launches;
+  k_seg_link<<<gs, 256, 0, e.stream>>>(S, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k);
+  uint32_t *act = nullptr, *left = nullptr;
+  bool hec = want_hec;
+  if (hec) {
+    // HEC matching rounds, captured as one graph
+    r = run_graph(e, 1, (uint64_t(RH) << 32) | uint32_t(gs), [&] {
+      cudaMemsetAsync(oncyc, 0, S, e.stream);
+      hec_contract(e, hp, RH, prev, next, wgt, S, false, Xr, oncyc);
+      cudaMemsetAsync(rcnt, 0, 4, e.stream);
       ++e.launches;
-      k_cycle_list<<<gs, 256, 0, e.stream>>>(oncyc, nseg, e.ctr, act0, rcnt);
-      act = act0;
-      left = rcnt;
-      rounds = RH;
-      r = e.read_ctr();
-      if (r) return r;
-      if (e.h_ctr->err) {  // did not finish in its pool/rounds: pointer jumping
-        UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
-        hec = false;
-      }
+      k_cycle_list<<<gs, 256, 0, e.stream>>>(oncyc, S, nullptr, act0, rcnt);
+    });
+    if (r) return r;
+    act = act0;
+    left = rcnt;
+    rounds = RH;
+    r = e.read_ctr();
+    if (r) return r;
+    if (e.h_ctr->err) {  // did not finish in its pool/rounds: pointer jumping
+      UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
+      hec = false;
     }
-    if (!hec) {
-      r = rank_lists(e, prev, wgt, nseg, true, Xr, act0, act1, rcnt, rounds, act, left);
-      if (r) return r;
-      UC_CK(cudaMemsetAsync(oncyc, 0, nseg, e.stream));
+  }
+  if (!hec) {
+    // pointer-jumping rounds, captured as one graph
+    uint32_t rr = 2;
+    for (uint64_t t = 1; t < S; t <<= 1) ++rr;
+    int rl = UC_OK;
+    r = run_graph(e, 0, (uint64_t(rr) << 32) | uint32_t(gs), [&] {
+      rl = rank_lists(e, prev, wgt, S, false, Xr, act0, act1, rcnt, rounds, act, left);
+      cudaMemsetAsync(oncyc, 0, S, e.stream);
       ++e.launches;
       k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
-    }
-    e.launches += 2 + 6 + 2;
-    k_chain_len<<<gs, 256, 0, e.stream>>>(e.ctr, Xr, next, wgt, oncyc, llen);
-    k_head_len<<<gs, 256, 0, e.stream>>>(e.ctr, prev, llen, hlen);
-    scan_excl<uint32_t, unsigned long long>(hlen, nseg, loff, stmp, e.stream, dtotal);
-    k_seg_copy<<<grid_for(e, uint64_t(nseg) * 32, 256), 256, 0, e.stream>>>(e.ctr, Xr, next, prev, wgt, oncyc,
-                                                                             seg_off, loff, segc, out, closed_bytes, k);
-    k_add_cursor<<<1, 1, 0, e.stream>>>(e.ctr, dtotal);
-    uint32_t hleft = 0;
-    UC_CK(cudaMemcpyAsync(&hleft, left, 4, cudaMemcpyDeviceToHost, e.stream));
-    UC_CK(cudaStreamSynchronize(e.stream));
-    if (hleft) {
-      ++e.launches;
-      if (nw == 1) k_seg_cycles<1><<<1, 1, 0, e.stream>>>(e.ctr, act, hleft, oncyc, next, seg_len, seg_off, segc, out, cap, k);
-      else k_seg_cycles<2><<<1, 1, 0, e.stream>>>(e.ctr, act, hleft, oncyc, next, seg_len, seg_off, segc, out, cap, k);
-    }
-    UC_CK(cudaGetLastError());
+    });
+    if (r) return r;
+    if (rl) return rl;
   }
+  e.launches += 2 + 6 + 2;
+  k_chain_len<<<gs, 256, 0, e.stream>>>(S, seg_len, Xr, next, wgt, oncyc, llen);
+  k_head_len<<<gs, 256, 0, e.stream>>>(S, seg_len, prev, oncyc, llen, hlen);
+  scan_excl<uint32_t, unsigned long long>(hlen, S, loff, stmp, e.stream);
+  k_seg_copy<<<grid_for(e, uint64_t(S) * 32, 256), 256, 0, e.stream>>>(S, seg_len, seg_job, jd.tab, jd.jclosed, Xr,
+                                                                        next, prev, wgt, oncyc, seg_off, loff, segc,
+                                                                        out, k);
+  k_job_finish<<<(njobs + 255) / 256, 256, 0, e.stream>>>(jd.tab, njobs, jd.jclosed, loff, jd.jout);
+  uint32_t hleft = 0;
+  UC_CK(cudaMemcpyAsync(&hleft, left, 4, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  if (hleft) {
+    ++e.launches;
+    if (nw == 1)
+      k_seg_cycles<1><<<1, 1, 0, e.stream>>>(e.ctr, S, act, hleft, oncyc, next, seg_len, seg_job, jd.tab, jd.jout,
+                                            seg_off, segc, out, k);
+    else
+      k_seg_cycles<2><<<1, 1, 0, e.stream>>>(e.ctr, S, act, hleft, oncyc, next, seg_len, seg_job, jd.tab, jd.jout,
+                                            seg_off, segc, out, k);
+  }
+  UC_CK(cudaGetLastError());
   cudaEventRecord(e.ev[4], e.stream);
+  std::vector<unsigned long long> jo(njobs);
+  UC_CK(cudaMemcpyAsync(jo.data(), jd.jout, njobs * 8, cudaMemcpyDeviceToHost, e.stream));
   r = e.read_ctr();
   if (r) return r;
   if (e.h_ctr->err) return e.check_err(e.h_ctr);
-  out_bytes = e.h_ctr->out_cursor;
-  if (out_bytes > cap) return e.fail(UC_EINTERNAL, "output bound exceeded");
+  uint64_t total = 0;
+  for (uint32_t j = 0; j < njobs; ++j) {
+    if (jo[j] > J[j].ocap) return e.fail(UC_EINTERNAL, "output bound exceeded");
+    if (out_off) out_off[j] = J[j].obase;
+    if (out_len) out_len[j] = jo[j];
+    total += jo[j];
+  }
   if (st) {
-    st->n_kmers = n;
+    st->n_kmers = N;
     st->n_copies = copies;
     st->n_cross = X;
     st->n_tiles = e.h_ctr->ntiles;
     st->n_big_tiles = e.h_ctr->nbig;
-    st->n_segments = nseg;
+    st->n_segments = Sp;
     st->n_cycles = e.h_ctr->cycles;
-    st->out_bytes = out_bytes;
+    st->out_bytes = total;
     st->stitch_rounds = rounds;
     st->l_used = uint32_t(P.l_used);
-    st->bucket_bits = P.bbits;
+    st->bucket_bits = P.bits;
     st->tile_capacity = P.cap;
     st->launches = e.launches;
+    st->graph_nodes = e.graph_nodes;
     float a = 0, b = 0, c = 0, d = 0;
     cudaEventElapsedTime(&a, e.ev[0], e.ev[1]);
     cudaEventElapsedTime(&b, e.ev[1], e.ev[2]);
@@ -2436,6 +2735,14 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
   }
   e.reset();
   return UC_OK;
+}
+
+int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char* out, uint64_t cap,
+                   uint64_t& out_bytes, uc_stats* st) {
+  uint64_t off = 0, len = 0;
+  const int r = compact_batch(e, 1, &d_text, &bytes, k, l, out, cap, &off, &len, st);
+  out_bytes = len;
+  return r;
 }
 
 }  // namespace uc

@@ -28,12 +28,21 @@ struct Env {
   Arena ar[2];              // 0: per-k-mer arrays, 1: copies/segments/scratch
   char* big_buf = nullptr;  // scratch of oversized tiles (grow only)
   size_t big_cap = 0;
+  char* jbuf = nullptr;     // job table and per-job counters (grow only)
+  size_t jcap = 0;
   Counters* ctr = nullptr;    // device
   Counters* h_ctr = nullptr;  // pinned host mirror
   cudaEvent_t ev[8] = {};
   uc_tuning tune{};
   uint64_t seed = 0x00C0FFEE5EEDull;
   uint32_t launches = 0;    // kernels launched by the last call
+  uint32_t graph_nodes = 0; // of which inside CUDA graphs
+  // instantiated graphs of the contraction rounds, reused while the round
+  // count (the graph's shape) stays the same
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  uint64_t gkey[2] = {0, 0};
+  bool use_graphs = true;
+  cudaStream_t gstream = nullptr;  // capture stream when the caller's stream is the legacy one
   std::string err;
 
   int fail(int code, const std::string& msg);
@@ -57,6 +66,8 @@ int emit(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* h
          const uint32_t* rank, uint64_t n, int k, char* out, uint64_t cap, uint64_t& out_bytes);
 int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char* out, uint64_t cap,
                    uint64_t& out_bytes, uc_stats* st);
+int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t* bytes, int k, int l, char* out,
+                  uint64_t out_cap, uint64_t* out_off, uint64_t* out_len, uc_stats* st);
 uint64_t output_bound(size_t text_bytes, int k);
 
 }  // namespace uc
