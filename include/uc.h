@@ -122,6 +122,25 @@ uc_status uc_emit(uc_ctx *ctx, const uint64_t *d_keys, const uint32_t *d_succ,
                   const uint32_t *d_head, const uint32_t *d_rank, uint64_t n,
                   int k, char *d_out, uint64_t cap, uint64_t *out_bytes);
 
+/* uc_emit for callers that cannot allocate device memory (a process whose
+ * own pool holds all free HBM, a plugin whose host framework owns the
+ * allocator, code whose other streams must not wait on the device-wide
+ * synchronisation cudaMalloc/cudaFree may do).  No counterpart in the
+ * reference.  Same arguments and output as uc_emit, without a context: the
+ * work runs on cuda_stream (NULL = legacy default stream) of the current
+ * device.  Calls no cudaMalloc or cudaFree; its scratch is one static device
+ * array per device, so n is limited to UC_EMIT_NOALLOC_MAX_KMERS (larger n
+ * fails with UC_EINPUT).  The first call on a device looks that array up
+ * (make it before any stream capture).  All calls on a device share the
+ * array: calls that overlap on the GPU race.  err (err_len bytes, may be
+ * NULL) receives a one-line reason on failure. */
+#define UC_EMIT_NOALLOC_MAX_KMERS (1u << 20)
+uc_status uc_emit_noalloc(void *cuda_stream, const uint64_t *d_keys,
+                          const uint32_t *d_succ, const uint32_t *d_head,
+                          const uint32_t *d_rank, uint64_t n, int k,
+                          char *d_out, uint64_t cap, uint64_t *out_bytes,
+                          char *err, size_t err_len);
+
 /* ---- fused path ------------------------------------------------------ */
 
 /* Whole path on device-resident text: pack, minimizer bucketing, per-tile

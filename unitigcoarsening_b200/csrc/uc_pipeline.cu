@@ -2432,6 +2432,55 @@ int emit(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* h
   return UC_OK;
 }
 
+uint64_t emit_scratch_bytes(uint64_t n) {
+  auto al = [](uint64_t b) { return (b + 255) & ~uint64_t(255); };
+  return 2 * al(n * 4) + al((n + 1) * 8) + al(scan_tmp_elems(n) * 8);
+}
+
+int emit_in(cudaStream_t s, int sm_count, const uint64_t* d_keys, const uint32_t* head, const uint32_t* rank,
+            uint64_t n, int k, char* out, uint64_t cap, uint64_t& out_bytes, void* scratch, std::string& err) {
+  out_bytes = 0;
+  if (k < 2 || k > 63) {
+    err = "k must be in [2, 63]";
+    return UC_EINPUT;
+  }
+  if (n == 0) return UC_OK;
+  auto al = [](uint64_t b) { return (b + 255) & ~uint64_t(255); };
+  char* p = static_cast<char*>(scratch);
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(p);
+  uint32_t* len = reinterpret_cast<uint32_t*>(p + al(n * 4));
+  unsigned long long* loff = reinterpret_cast<unsigned long long*>(p + 2 * al(n * 4));
+  unsigned long long* tmp = reinterpret_cast<unsigned long long*>(p + 2 * al(n * 4) + al((n + 1) * 8));
+  auto ck = [&](cudaError_t c, const char* what) -> int {
+    if (c == cudaSuccess) return UC_OK;
+    err = std::string(what) + ": " + cudaGetErrorString(c);
+    return int(UC_ECUDA);
+  };
+  const uint64_t want = (n + 255) / 256, gcap = uint64_t(sm_count) * 16;
+  const int grid = int(std::max<uint64_t>(1, std::min(want, gcap)));
+  int r = ck(cudaMemsetAsync(cnt, 0, n * 4, s), "cudaMemsetAsync");
+  if (r) return r;
+  k_count_members<<<grid, 256, 0, s>>>(head, n, cnt);
+  k_line_len<<<grid, 256, 0, s>>>(head, cnt, n, k, len);
+  scan_excl<uint32_t, unsigned long long>(len, n, loff, tmp, s);
+  unsigned long long total = 0;
+  if ((r = ck(cudaGetLastError(), "launch"))) return r;
+  if ((r = ck(cudaMemcpyAsync(&total, loff + n, 8, cudaMemcpyDeviceToHost, s), "cudaMemcpyAsync"))) return r;
+  if ((r = ck(cudaStreamSynchronize(s), "cudaStreamSynchronize"))) return r;
+  out_bytes = total;
+  if (out) {
+    if (total > cap) {
+      err = "output buffer too small";
+      return UC_EINPUT;
+    }
+    if (k <= 31) k_spell<1><<<grid, 256, 0, s>>>(d_keys, head, rank, cnt, loff, n, k, out);
+    else k_spell<2><<<grid, 256, 0, s>>>(d_keys, head, rank, cnt, loff, n, k, out);
+    if ((r = ck(cudaGetLastError(), "launch"))) return r;
+    if ((r = ck(cudaStreamSynchronize(s), "cudaStreamSynchronize"))) return r;
+  }
+  return UC_OK;
+}
+
 uint64_t output_bound(size_t text_bytes, int k) {
   (void)k;
   return uint64_t(text_bytes) + 64;

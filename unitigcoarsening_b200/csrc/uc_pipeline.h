@@ -69,5 +69,11 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
 int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t* bytes, int k, int l, char* out,
                   uint64_t out_cap, uint64_t* out_off, uint64_t* out_len, uc_stats* st);
 uint64_t output_bound(size_t text_bytes, int k);
+// emit() over caller-provided device scratch of emit_scratch_bytes(n) bytes
+// (256-byte aligned) on stream s: the same kernels, no allocation.  Clears
+// the member counts it needs at zero itself.
+uint64_t emit_scratch_bytes(uint64_t n);
+int emit_in(cudaStream_t s, int sm_count, const uint64_t* d_keys, const uint32_t* head, const uint32_t* rank,
+            uint64_t n, int k, char* out, uint64_t cap, uint64_t& out_bytes, void* scratch, std::string& err);
 
 }  // namespace uc
