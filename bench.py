@@ -28,7 +28,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "k-mers compacted/s on 1 B200 (plain single job)"
+METRIC = "k-mers compacted/s on 1 B200, batched vs plain (bit-exact); HBM % peak; job p99"
 UNIT = "k-mers/s"
 
 
@@ -96,16 +96,39 @@ class Clocks:
 
 
 def algorithmic_bytes(st: dict, text_bytes: int, k: int) -> dict:
-    """Bytes each phase must move at minimum (each logical array element read
-    or written once), from the run's own counts."""
+    """Bytes each phase must move at minimum (every logical array element
+    read or written once), from the run's own counts.  W = key bytes, 4-byte
+    ids, 8 bytes of bucket ids per k-mer, 20 bytes per segment record."""
     W = 8 if k <= 31 else 16
     n, cp, S, ob = st["n_kmers"], st["n_copies"], st["n_segments"], st["out_bytes"]
+    closed, segc = st["closed_bytes"], st["seg_chars"]
     return {
-        "pack": text_bytes + n * W,                                # text in, keys out
-        "bucket": n * W + n * 8 + (n * W + n * 8) + cp * (W + 4),  # minimizers+counts, scatter
-        "tiles": cp * (W + 4) + ob,                                # copies in, lines out
-        "stitch": S * 40,                                          # segment records, links, copy
+        "pack": text_bytes + n * (W + 8),                 # text in; keys and bucket ids out
+        "bucket": n * (W + 8) + cp * (W + 4),             # keys and bucket ids in; copies out
+        "tiles": cp * (W + 4) + closed + segc + S * 20,   # copies in; lines, segment chars and records out
+        "stitch": S * 20 + segc + (ob - closed),          # segments in; cross-tile lines out
     }
+
+
+def whole_path_bytes(st: dict, text_bytes: int, k: int) -> int:
+    """B_alg of the whole path: in + n (7W + 14I) + out (each phase's minimum
+    traffic summed, I = 4-byte ids)."""
+    W = 8 if k <= 31 else 16
+    return text_bytes + st["n_kmers"] * (7 * W + 14 * 4) + st["out_bytes"]
+
+
+def traffic_per_copy(kernel: str):
+    """DRAM bytes per copy of a tile kernel from the committed ncu summary
+    (profiles/traffic.txt: kernel, bytes per copy, the capture it came
+    from), or None."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        f = line.split()
+        if len(f) >= 2 and f[0] == kernel:
+            return float(f[1])
+    return None
 
 
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "uc_ref_large")
@@ -190,6 +213,140 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def measure_batched(args, comp):
+    """Many small jobs (log-normal lengths, median 3 Mbp, 0.5-8 Mbp, GC
+    30-70%, 0.2% SNPs, k=31): all of them in one batched pass against the
+    plain loop of one compaction per job, both device-resident on this GPU,
+    each the mean of the timed passes after warm-up."""
+    import torch
+    from unitigcoarsening_b200 import synth
+    texts = []
+    with torch.no_grad():
+        for j in range(args.batch_jobs):
+            texts.append(synth.make_text(synth.batched_job(j, seed=4), 31, device="cuda"))
+    torch.cuda.synchronize()
+    caps = [comp.output_bound(t.numel(), 31) for t in texts]
+    one = torch.empty(max(caps), dtype=torch.uint8, device="cuda")  # the plain loop reuses one buffer
+    bout = torch.empty(sum((c + 15) // 16 * 16 for c in caps) + 64, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def plain():
+        lens = []
+        for t in texts:
+            lens.append(comp.compact(t, 31, args.l, out=one).numel())
+        return lens
+
+    def batched():
+        res, st = comp.compact_batch(texts, 31, args.l, out=bout, stats=True)
+        return [r.numel() for r in res], st
+
+    for _ in range(2):
+        plain_len = plain()
+        batch_len, bst = batched()
+    reps = 2
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        plain()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1) / reps
+    e0.record(stream)
+    for _ in range(reps):
+        batched()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batch_ms = e0.elapsed_time(e1) / reps
+    n = int(bst["n_kmers"])
+    del texts, one, bout
+    torch.cuda.empty_cache()
+    return {"workload": f"{args.batch_jobs} jobs: log-normal length (median 3 Mbp, 0.5-8 Mbp), GC 30-70%, "
+                        f"0.2% SNPs, k=31, device-resident", "jobs": args.batch_jobs, "n_kmers": n,
+            "batched": {"value": n / (batch_ms / 1e3), "ms": batch_ms, "launches": int(bst["launches"])},
+            "plain": {"value": n / (plain_ms / 1e3), "ms": plain_ms},
+            "speedup": plain_ms / batch_ms, "out_bytes_equal": plain_len == batch_len, "unit": UNIT}
+
+
+def measure_serving(args, device: int):
+    """Serving loop: a pool of distinct jobs (k-mer counts log-uniform in
+    [10k, 50M], k = 31 with p 0.7 else 63) in pinned host memory; capacity =
+    the plain sequential host-to-host path over the pool; then Poisson
+    arrivals at 80% of that capacity, each a job drawn from the pool, served
+    by uc_server (footprint admission, batching, overlapping lanes)."""
+    import random
+    import threading
+    import torch
+    from unitigcoarsening_b200 import Compactor, Server, synth
+    pool = []
+    with torch.no_grad():
+        for j in range(args.serve_pool):
+            spec, k = synth.served_job(j, seed=5)
+            t = synth.make_text(spec, k, device="cuda")
+            h = torch.empty(t.numel(), dtype=torch.uint8, pin_memory=True)
+            h.copy_(t)
+            del t
+            pool.append((h, k, int(bytes(h[:24].numpy()).split(b"\n")[0])))
+    torch.cuda.empty_cache()
+    # capacity: plain sequential path, host text to host lines (pinned both
+    # ways, like the server's lanes)
+    comp = Compactor(device)
+    houts = [torch.empty(comp.output_bound(h.numel(), k), dtype=torch.uint8, pin_memory=True) for h, k, _ in pool]
+    seq_s = 0.0
+    for rep in range(2):
+        t0 = time.perf_counter()
+        for (h, k, n), o in zip(pool, houts):
+            comp.compact_host(h, k, min(args.l, k - 1), out=o)
+        if rep:
+            seq_s = time.perf_counter() - t0
+    comp.close()
+    del comp, houts
+    torch.cuda.empty_cache()
+    pool_kmers = sum(n for _, _, n in pool)
+    capacity = pool_kmers / seq_s
+    mean_n = pool_kmers / len(pool)
+    rate = 0.8 * capacity / mean_n  # jobs per second
+    rnd = random.Random(7)
+    arrivals, t = [], 0.0
+    for _ in range(args.serve_jobs):
+        t += rnd.expovariate(rate)
+        arrivals.append((t, rnd.randrange(len(pool))))
+    results = [None] * len(arrivals)
+    with Server(device=device, lanes=4, max_batch=32) as srv:
+        tickets = [None] * len(arrivals)
+        ready = threading.Semaphore(0)
+
+        def waiter():
+            for i in range(len(arrivals)):
+                ready.acquire()
+                results[i] = srv.wait(tickets[i], timeout=600, fetch=False)[1]
+
+        wt = threading.Thread(target=waiter)
+        wt.start()
+        t0 = time.perf_counter()
+        for i, (ta, j) in enumerate(arrivals):
+            d = ta - (time.perf_counter() - t0)
+            if d > 0:
+                time.sleep(d)
+            h, k, _ = pool[j]
+            tickets[i] = srv.submit(h, k, min(args.l, k - 1))
+            ready.release()
+        wt.join()
+        wall = time.perf_counter() - t0
+        tot = srv.stats()
+    served = sum(pool[j][2] for _, j in arrivals)
+    lat = sorted(r["latency_ms"] for r in results)
+    pct = lambda q: lat[min(len(lat) - 1, int(q * (len(lat) - 1) + 0.5))]
+    return {"workload": f"Poisson arrivals at 80% of the plain sequential capacity; {args.serve_jobs} jobs drawn "
+                        f"from {len(pool)} distinct jobs, k-mer counts log-uniform in [10k, 50M], k = 31 (p 0.7) "
+                        f"or 63, host memory to host memory", "jobs": args.serve_jobs,
+            "offered_jobs_per_s": rate, "sustained": {"value": served / wall, "unit": UNIT},
+            "plain_sequential": {"value": capacity, "unit": UNIT},
+            "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": lat[-1], "mean": sum(lat) / len(lat)},
+            "batches": int(tot["batches"]), "batched_jobs": int(tot["batched_jobs"]),
+            "pool_gb": tot["pool_bytes"] / 1e9, "pool_peak_gb": tot["pool_peak_bytes"] / 1e9}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -203,6 +360,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=float, default=4e6, help="genome length of the CPU sample")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
+    ap.add_argument("--tune-sample", type=float, default=2e8, help="genome length the autotuner times")
+    ap.add_argument("--batch-jobs", type=int, default=256, help="jobs of the batched-vs-plain comparison (0: skip)")
+    ap.add_argument("--serve-jobs", type=int, default=400, help="arrivals of the serving measurement (0: skip)")
+    ap.add_argument("--serve-pool", type=int, default=24, help="distinct jobs the arrivals draw from")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -224,6 +386,17 @@ def main():
     from unitigcoarsening_b200 import Compactor, synth
     from unitigcoarsening_b200 import build as B
     B.build()
+    comp = Compactor(local)
+
+    # autotuner (untimed): the library's tuner on a sample of the same model
+    tuning = None
+    if not args.no_tune:
+        with torch.no_grad():
+            sample = synth.make_text(synth.scale_plain(length=int(args.tune_sample), seed=3 + rank), args.k,
+                                     device="cuda")
+        tuning = comp.autotune(sample, args.k, args.l, reps=3, max_ms=20000)
+        del sample
+        torch.cuda.empty_cache()
 
     t0 = time.time()
     spec = synth.scale_plain(length=int(args.genome), seed=2 + rank)
@@ -234,7 +407,6 @@ def main():
     text_bytes = text.numel()
     torch.cuda.empty_cache()
 
-    comp = Compactor(local)
     out = torch.empty(comp.output_bound(text_bytes, args.k), dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
     st = None
@@ -245,6 +417,7 @@ def main():
 
     # timed region: device-resident text (> L2, so no flush is needed)
     phase = {"pack": 0.0, "bucket": 0.0, "tiles": 0.0, "stitch": 0.0}
+    kern = {"tile_warp": 0.0, "tile_block": 0.0}
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     if dist:
@@ -256,6 +429,8 @@ def main():
             res, st = comp.compact(text, args.k, args.l, out=out, stats=True)
             for p in phase:
                 phase[p] += st["ms_" + p]
+            for p in kern:
+                kern[p] += st["ms_" + p]
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
@@ -266,14 +441,19 @@ def main():
         dist.barrier()
     for p in phase:
         phase[p] /= args.steps
+    for p in kern:
+        kern[p] /= args.steps
     value = world * n / (ms / 1e3)
 
-    # roofline of the dominant phase
+    # roofline of the dominant kernels: the two tile kernels (warp tiles and
+    # block tiles), timed by CUDA events on the library's stream around their
+    # launches; algorithmic bytes = the tile phase's minimum traffic
     peak, peak_kind = peaks()
     alg = algorithmic_bytes(st, text_bytes, args.k)
-    dom = max(phase, key=lambda p: phase[p])
-    achieved = alg[dom] / (phase[dom] / 1e3) / 1e9
-    whole = sum(alg.values()) / (ms / 1e3) / 1e9
+    tile_ms = kern["tile_warp"] + kern["tile_block"]
+    achieved = alg["tiles"] / (tile_ms / 1e3) / 1e9
+    tpc = traffic_per_copy("k_tile_warp")
+    whole = whole_path_bytes(st, text_bytes, args.k) / (ms / 1e3) / 1e9
 
     # e2e: host text -> host lines through the C ABI
     e2e = None
@@ -284,7 +464,7 @@ def main():
             htext = torch.empty(text_bytes, dtype=torch.uint8, pin_memory=True)
             htext.copy_(text)
             hout = torch.empty(comp.output_bound(text_bytes, args.k), dtype=torch.uint8, pin_memory=True)
-            del text
+            del text, out
             torch.cuda.empty_cache()
             comp.compact_host(htext, args.k, args.l, out=hout)
             t1 = time.perf_counter()
@@ -294,8 +474,17 @@ def main():
             e2e = {"value": world * n / e2e_s, "unit": UNIT, "h2d_bytes_per_step": text_bytes,
                    "d2h_bytes_per_step": int(est["out_bytes"]), "ms_per_step": e2e_s * 1e3,
                    "pinned": True}
+            del htext, hout
         else:
             e2e = {"value": None, "unit": UNIT, "skipped": f"host RAM below {need >> 30} GiB"}
+    text = out = None
+    torch.cuda.empty_cache()
+
+    batched = measure_batched(args, comp) if args.batch_jobs > 0 else None
+    comp.close()
+    del comp
+    torch.cuda.empty_cache()
+    serving = measure_serving(args, local) if args.serve_jobs > 0 else None
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -310,13 +499,17 @@ def main():
                                    f"families, 0.1% SNPs, k={args.k}", "k": args.k, "l": args.l,
                        "n_kmers": n, "text_bytes": text_bytes, "l2_flush": "inputs larger than L2",
                        "parallelism": f"replicas x{world}", "genome_seed": 2},
-            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "roofline": {"bound": "hbm", "kernel": "k_tile_warp + k_tile", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (tpc * st["n_copies"]) if tpc else None,
+                         "algorithmic_bytes": alg["tiles"], "ms": tile_ms,
                          "whole_path_achieved": whole, "whole_path_frac": whole / peak},
-            "phase_ms": phase, "algorithmic_bytes": alg,
+            "phase_ms": phase, "kernel_ms": kern, "algorithmic_bytes": alg,
             "stats": {k2: (float(v) if isinstance(v, float) else int(v)) for k2, v in st.items()},
+            "tuning": tuning,
+            "batched_vs_plain": batched, "serving": serving,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
-            "gpu_launches": int(st.get("launches", 0)) * args.steps if "launches" in st else None,
+            "gpu_launches": int(st["launches"]) * args.steps,
             "gen_seconds": gen_s,
         }
         print(json.dumps(line), flush=True)

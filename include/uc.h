@@ -50,18 +50,21 @@ typedef struct uc_job uc_job;
 typedef struct uc_stats {
     uint64_t n_kmers, n_copies, n_cross, n_tiles, n_big_tiles;
     uint64_t n_segments, n_unitigs, n_cycles, out_bytes;
+    uint64_t closed_bytes, seg_chars; /* written by the tile kernels: lines, segment chars */
     uint32_t l_used, bucket_bits, tile_capacity, stitch_rounds, launches, graph_nodes;
     float ms_pack, ms_bucket, ms_tiles, ms_stitch, ms_total;
+    float ms_tile_warp, ms_tile_block; /* the warp- and block-tile kernels */
 } uc_stats;
 
 /* Tuning knobs (0 = automatic).  Filled by the autotuner or by hand. */
 typedef struct uc_tuning {
     uint32_t tile_capacity;   /* copies per shared-memory tile (max 8192) */
-    uint32_t tile_threads;    /* threads per tile CTA (256, 512 or 1024) */
+    uint32_t tile_threads;    /* threads per tile CTA (256 or 512) */
     uint32_t bucket_bits;     /* log2 of the bucket count */
-    uint32_t load_factor_pct; /* tile hash slots per copy, percent (>=150) */
+    uint32_t load_factor_pct; /* tile hash slots per 100 copies (150..800; 200) */
     uint32_t contract_method; /* UC_CONTRACT_* for the segment stitch */
     uint32_t warp_capacity;   /* copies per warp tile (32..1024; 1 = no warp tier) */
+    uint32_t bucket_fill;     /* buckets per tile when bucket_bits is 0 (1..64; 8) */
 } uc_tuning;
 
 /* ---- context --------------------------------------------------------- */
@@ -141,6 +144,20 @@ uc_status uc_emit_noalloc(void *cuda_stream, const uint64_t *d_keys,
                           char *d_out, uint64_t cap, uint64_t *out_bytes,
                           char *err, size_t err_len);
 
+/* Autotuner; no counterpart in the reference (its bucket and table sizes
+ * are fixed in the code).  Times the fused path (uc_compact_device) on
+ * d_text, a representative job already in device memory, for candidate
+ * tunings: coordinate descent over warp_capacity, bucket_fill,
+ * tile_capacity, tile_threads, load_factor_pct and contract_method, each
+ * candidate the median device time of reps runs (0 = 3) after one warm-up.
+ * Every candidate must produce the same output size (UC_EINTERNAL if not).
+ * Stops after a pass without improvement or after max_ms of device time
+ * (0 = 60000).  Leaves the fastest tuning set on ctx and returns it, with its
+ * time and the number of candidates timed (best_ms, trials may be NULL). */
+uc_status uc_autotune(uc_ctx *ctx, const char *d_text, size_t bytes, int k,
+                      int l, int reps, uint32_t max_ms, uc_tuning *best,
+                      float *best_ms, uint32_t *trials);
+
 /* ---- fused path ------------------------------------------------------ */
 
 /* Whole path on device-resident text: pack, minimizer bucketing, per-tile
@@ -188,6 +205,59 @@ uc_status uc_job_result(uc_job *job, char **buf, size_t *len,
                         uc_stats *stats);
 uc_status uc_job_release(uc_job *job);
 void uc_free(void *p);
+
+/* ---- serving loop ------------------------------------------------------
+ * No counterpart in the reference, which compacts one file per process.  A
+ * server owns one device pool of hbm_budget bytes (0 = the smaller of
+ * 160 GiB and 90% of free memory), allocated at creation.  Jobs are admitted
+ * in arrival order when a lane (a host thread with its own stream) is idle
+ * and a slice of the pool covering the job's footprint bound is free; jobs
+ * of at most batch_bytes of text queued behind the admitted one, with the
+ * same k and l, join its launch (up to max_batch jobs, uc_compact_batch).
+ * Lanes run concurrently, so admitted work overlaps on the GPU.  Results
+ * equal uc_compact_host's for the same text, line order aside. */
+typedef struct uc_server uc_server;
+typedef struct uc_server_config {
+    int device;
+    int lanes;           /* concurrent device lanes (0 = 4) */
+    int max_batch;       /* most jobs in one launch (0 = 64) */
+    int reserved;
+    size_t hbm_budget;   /* device pool bytes */
+    size_t batch_bytes;  /* jobs up to this text size may be batched (0 = 64 MiB) */
+    size_t host_budget;  /* pinned host pool for results (0 = 16 GiB) */
+    uc_tuning tuning;    /* tuning of every lane (zeros = automatic) */
+} uc_server_config;
+typedef struct uc_server_job_info {
+    uc_status status;
+    uint32_t batch;       /* jobs in the launch that served this one */
+    uint64_t n_kmers;
+    double queue_ms;      /* submit to admission */
+    double latency_ms;    /* submit to result on the host */
+    char error[128];
+} uc_server_job_info;
+typedef struct uc_server_totals {
+    uint64_t jobs_done, kmers_done, batches, batched_jobs, queued;
+    uint64_t pool_bytes, pool_peak_bytes;
+    double p50_ms, p99_ms, max_ms, mean_ms; /* job latency over completed jobs */
+    double wall_s;                          /* first submit to last completion */
+} uc_server_totals;
+uc_status uc_server_create(const uc_server_config *cfg, uc_server **out);
+/* The text stays owned by the caller and must stay valid until the job's
+ * uc_server_wait returns. */
+uc_status uc_server_submit(uc_server *srv, const char *text, size_t bytes,
+                           int k, int l, uint64_t *ticket);
+uc_status uc_server_poll(uc_server *srv, uint64_t ticket, int *done);
+/* Blocks until the job is done (timeout_s <= 0: no limit; UC_ETIMEOUT when
+ * it runs out).  Hands over the lines and forgets the ticket; returns the
+ * job's status.  The lines sit in the server's pinned host pool (or in
+ * malloc'd memory when that pool is full); give them back with
+ * uc_server_free.  buf NULL: the lines are dropped at once. */
+uc_status uc_server_wait(uc_server *srv, uint64_t ticket, double timeout_s,
+                         char **buf, size_t *len, uc_server_job_info *info);
+uc_status uc_server_free(uc_server *srv, char *buf);
+uc_status uc_server_stats(uc_server *srv, uc_server_totals *stats);
+/* Finishes the launches in flight; jobs still queued are dropped. */
+uc_status uc_server_destroy(uc_server *srv);
 
 /* File to file, appending to out_path like write_to_f (compact.h:7-37).
  * The reference CLI `main <k-mer file> k l <output file>`. */

@@ -84,20 +84,22 @@ def test_fused_matches_oracle(comp, oracle, texts, cfg):
     assert got == sorted_lines(want)
 
 
-@pytest.mark.parametrize("cap,bits,wcap", [(256, 0, 0), (256, 4, 0), (1024, 12, 0), (2048, 8, 1), (8192, 9, 1),
-                                           (4096, 0, 64), (4096, 14, 32), (4096, 0, 1024), (1024, 0, 512)])
-def test_fused_independent_of_tiling(comp, oracle, texts, cap, bits, wcap):
-    """Same lines whatever the bucketing and whichever tier (warp tiles,
-    block tiles, oversized tiles in global scratch) works each tile."""
+@pytest.mark.parametrize("cap,bits,wcap,lf", [(256, 0, 0, 0), (256, 4, 0, 150), (1024, 12, 0, 0), (2048, 8, 1, 400),
+                                              (8192, 9, 1, 0), (4096, 0, 64, 800), (4096, 14, 32, 0),
+                                              (4096, 0, 1024, 150), (1024, 0, 512, 300)])
+def test_fused_independent_of_tiling(comp, oracle, texts, cap, bits, wcap, lf):
+    """Same lines whatever the bucketing, the hash load factor and whichever
+    tier (warp tiles, block tiles, oversized tiles in global scratch) works
+    each tile."""
     text, k = texts["scale_sample"]
     want, _, _ = oracle.compact(text, k)
-    comp.set_tuning(tile_capacity=cap, bucket_bits=bits, warp_capacity=wcap)
+    comp.set_tuning(tile_capacity=cap, bucket_bits=bits, warp_capacity=wcap, load_factor_pct=lf)
     try:
         got = fused_lines(comp, text, k, 8)
         keys = comp.load_kmers(dev(text), k)
         succ, pred = comp.assemble_pruned_graph(keys, k, 8)
     finally:
-        comp.set_tuning(tile_capacity=0, bucket_bits=0, warp_capacity=0)
+        comp.set_tuning(tile_capacity=0, bucket_bits=0, warp_capacity=0, load_factor_pct=0)
     assert got == sorted_lines(want)
     from unitigcoarsening_b200 import as_u32
     osucc, opred = oracle.edges(oracle.parse(text, k), k)

@@ -24,6 +24,7 @@ stream.  There is no CPU fallback: without the CUDA library every call raises.
 from __future__ import annotations
 
 import ctypes
+import json
 import os
 
 import numpy as np
@@ -49,10 +50,11 @@ class UCError(RuntimeError):
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in (
         "n_kmers", "n_copies", "n_cross", "n_tiles", "n_big_tiles",
-        "n_segments", "n_unitigs", "n_cycles", "out_bytes")] + \
+        "n_segments", "n_unitigs", "n_cycles", "out_bytes", "closed_bytes", "seg_chars")] + \
         [(n, ctypes.c_uint32) for n in ("l_used", "bucket_bits", "tile_capacity", "stitch_rounds", "launches",
                                           "graph_nodes")] + \
-        [(n, ctypes.c_float) for n in ("ms_pack", "ms_bucket", "ms_tiles", "ms_stitch", "ms_total")]
+        [(n, ctypes.c_float) for n in ("ms_pack", "ms_bucket", "ms_tiles", "ms_stitch", "ms_total",
+                                       "ms_tile_warp", "ms_tile_block")]
 
     def as_dict(self) -> dict:
         return {n: getattr(self, n) for n, _ in self._fields_}
@@ -61,7 +63,25 @@ class Stats(ctypes.Structure):
 class Tuning(ctypes.Structure):
     _fields_ = [("tile_capacity", ctypes.c_uint32), ("tile_threads", ctypes.c_uint32),
                 ("bucket_bits", ctypes.c_uint32), ("load_factor_pct", ctypes.c_uint32),
-                ("contract_method", ctypes.c_uint32), ("warp_capacity", ctypes.c_uint32)]
+                ("contract_method", ctypes.c_uint32), ("warp_capacity", ctypes.c_uint32),
+                ("bucket_fill", ctypes.c_uint32)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("hbm_budget", ctypes.c_size_t), ("batch_bytes", ctypes.c_size_t),
+                ("host_budget", ctypes.c_size_t), ("tuning", Tuning)]
+
+
+class JobInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("batch", ctypes.c_uint32), ("n_kmers", ctypes.c_uint64),
+                ("queue_ms", ctypes.c_double), ("latency_ms", ctypes.c_double), ("error", ctypes.c_char * 128)]
+
+
+class ServerTotals(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("jobs_done", "kmers_done", "batches", "batched_jobs", "queued",
+                                               "pool_bytes", "pool_peak_bytes")] + \
+               [(n, ctypes.c_double) for n in ("p50_ms", "p99_ms", "max_ms", "mean_ms", "wall_s")]
 
 
 _lib = None
@@ -104,6 +124,16 @@ def lib():
             "uc_job_release": ([vp], i),
             "uc_free": ([vp], None),
             "uc_compact_file": ([vp, ctypes.c_char_p, i, i, ctypes.c_char_p, ctypes.POINTER(Stats)], i),
+            "uc_server_create": ([ctypes.POINTER(ServerConfig), ctypes.POINTER(vp)], i),
+            "uc_server_submit": ([vp, vp, sz, i, i, pu64], i),
+            "uc_server_poll": ([vp, u64, ctypes.POINTER(ctypes.c_int)], i),
+            "uc_server_wait": ([vp, u64, ctypes.c_double, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t),
+                                ctypes.POINTER(JobInfo)], i),
+            "uc_server_stats": ([vp, ctypes.POINTER(ServerTotals)], i),
+            "uc_server_free": ([vp, vp], i),
+            "uc_server_destroy": ([vp], i),
+            "uc_autotune": ([vp, vp, sz, i, i, i, u32, ctypes.POINTER(Tuning), ctypes.POINTER(ctypes.c_float),
+                             ctypes.POINTER(u32)], i),
         }
         for name, (args, res) in sig.items():
             f = getattr(L, name)
@@ -286,10 +316,150 @@ class Compactor:
         res = out[: ob.value]
         return (res, st.as_dict()) if stats else res
 
+    def autotune(self, text: torch.Tensor, k: int, l: int, reps: int = 3, max_ms: int = 60000,
+                 cache: str | None = None) -> dict:
+        """Pick the fastest tuning for jobs like ``text`` (device-resident)
+        with the library's coordinate-descent tuner (uc_autotune) and leave it
+        set on this context.  With ``cache`` (a JSON file) the result is stored
+        under this GPU, k and the job's size class, and reused from there on
+        later calls without timing anything."""
+        key = tuning_key(self.device, k, text.numel())
+        if cache:
+            got = load_tuning(cache, key)
+            if got is not None:
+                self.set_tuning(**got)
+                return dict(got, cached=True)
+        self._bind_stream()
+        t = Tuning()
+        ms = ctypes.c_float()
+        n = ctypes.c_uint32()
+        self._check(self._L.uc_autotune(self._h, _ptr(text), text.numel(), k, l, reps, max_ms, ctypes.byref(t),
+                                        ctypes.byref(ms), ctypes.byref(n)))
+        res = {f: getattr(t, f) for f, _ in Tuning._fields_}
+        if cache:
+            store_tuning(cache, key, res, ms.value)
+        return dict(res, ms=ms.value, trials=n.value, cached=False)
+
     def compact_file(self, in_path: str, k: int, l: int, out_path: str) -> dict:
         st = Stats()
         self._check(self._L.uc_compact_file(self._h, in_path.encode(), k, l, out_path.encode(), ctypes.byref(st)))
         return st.as_dict()
+
+
+class Server:
+    """Serving loop over one GPU (uc_server_*): jobs submitted from host
+    memory at any time, admitted by their HBM footprint into one device pool,
+    small queued jobs batched into one launch, several lanes overlapping on
+    the device.  ``wait`` returns each job's lines and its latency."""
+
+    def __init__(self, device: int = 0, lanes: int = 4, max_batch: int = 64, hbm_budget: int = 0,
+                 batch_bytes: int = 0, host_budget: int = 0, tuning: dict | None = None):
+        self._L = lib()
+        cfg = ServerConfig(device=device, lanes=lanes, max_batch=max_batch, hbm_budget=hbm_budget,
+                           batch_bytes=batch_bytes, host_budget=host_budget)
+        for k, v in (tuning or {}).items():
+            setattr(cfg.tuning, k, int(v))
+        h = ctypes.c_void_p()
+        st = self._L.uc_server_create(ctypes.byref(cfg), ctypes.byref(h))
+        if st:
+            raise UCError(st, "uc_server_create failed")
+        self._h = h
+        self._keep = {}  # ticket -> host text kept alive until its result is taken
+
+    def submit(self, text, k: int, l: int) -> int:
+        if isinstance(text, (bytes, bytearray)):
+            arr = np.frombuffer(text, dtype=np.uint8)
+            ptr, n = arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes
+        elif isinstance(text, np.ndarray):
+            arr = text
+            ptr, n = arr.ctypes.data_as(ctypes.c_void_p), arr.nbytes
+        else:
+            arr = text
+            ptr, n = ctypes.c_void_p(text.data_ptr()), text.numel()
+        t = ctypes.c_uint64()
+        st = self._L.uc_server_submit(self._h, ptr, n, k, l, ctypes.byref(t))
+        if st:
+            raise UCError(st, "uc_server_submit failed")
+        self._keep[t.value] = arr
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        d = ctypes.c_int()
+        st = self._L.uc_server_poll(self._h, ticket, ctypes.byref(d))
+        if st:
+            raise UCError(st, "uc_server_poll failed")
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout: float = 0.0, fetch: bool = True):
+        """(lines as bytes, info dict); raises UCError if the job failed.
+        fetch=False drops the lines in the server (returns b"")."""
+        buf = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        info = JobInfo()
+        st = self._L.uc_server_wait(self._h, ticket, timeout, ctypes.byref(buf) if fetch else None,
+                                    ctypes.byref(n), ctypes.byref(info))
+        if st == 4 and info.latency_ms == 0 and not info.error:  # UC_ETIMEOUT: still running
+            raise TimeoutError(f"job {ticket} not done within {timeout} s")
+        self._keep.pop(ticket, None)
+        data = ctypes.string_at(buf, n.value) if buf.value else b""
+        if buf.value:
+            self._L.uc_server_free(self._h, buf)
+        d = {"status": info.status, "batch": info.batch, "n_kmers": info.n_kmers, "queue_ms": info.queue_ms,
+             "latency_ms": info.latency_ms, "error": info.error.decode()}
+        if st:
+            raise UCError(st, d["error"] or "job failed")
+        return data, d
+
+    def stats(self) -> dict:
+        t = ServerTotals()
+        self._L.uc_server_stats(self._h, ctypes.byref(t))
+        return {n: getattr(t, n) for n, _ in ServerTotals._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.uc_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def tuning_key(device: int, k: int, text_bytes: int) -> str:
+    """Cache key of a tuning: GPU name, key width and the job's size class
+    (power of two of its text bytes)."""
+    name = torch.cuda.get_device_name(device).replace(" ", "_")
+    return f"{name}|k{'31' if k <= 31 else '63'}|2^{max(0, int(text_bytes).bit_length() - 1)}"
+
+
+def load_tuning(path: str, key: str):
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        d = json.load(f)
+    e = d.get(key)
+    return None if e is None else {n: int(e[n]) for n, _ in Tuning._fields_ if n in e}
+
+
+def store_tuning(path: str, key: str, tuning: dict, ms: float):
+    d = {}
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+    d[key] = dict(tuning, ms=round(float(ms), 4))
+    tmp = path + ".tmp"
+    with open(tmp, "w") as f:
+        json.dump(d, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
 
 
 def keys_to_words(keys: torch.Tensor, k: int) -> np.ndarray:

@@ -15,7 +15,7 @@ BUILD = os.path.join(HERE, "_build")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
-SOURCES = ["uc_pipeline.cu", "uc_capi.cu", "uc_noalloc.cu"]
+SOURCES = ["uc_pipeline.cu", "uc_capi.cu", "uc_noalloc.cu", "uc_server.cu"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -1,8 +1,10 @@
 // uc_capi.cu — the extern "C" boundary of libuc.so (declared in include/uc.h).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include "../../include/uc.h"
 #include "uc_pipeline.h"
@@ -135,7 +137,7 @@ uc_status uc_ctx_create(int device, size_t hbm_budget, uc_ctx** out) {
   e = cudaStreamCreateWithFlags(&c->env.stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaMalloc(&c->env.ctr, sizeof(uc::Counters));
   if (e == cudaSuccess) e = cudaMallocHost(&c->env.h_ctr, sizeof(uc::Counters));
-  for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->env.ev[i]);
+  for (int i = 0; i < uc::Env::NEV && e == cudaSuccess; ++i) e = cudaEventCreate(&c->env.ev[i]);
   if (e != cudaSuccess) {
     cudaGetLastError();
     uc_ctx_destroy(c);
@@ -161,7 +163,7 @@ uc_status uc_ctx_destroy(uc_ctx* c) {
   if (c->io_out) cudaFree(c->io_out);
   if (c->env.ctr) cudaFree(c->env.ctr);
   if (c->env.h_ctr) cudaFreeHost(c->env.h_ctr);
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < uc::Env::NEV; ++i)
     if (c->env.ev[i]) cudaEventDestroy(c->env.ev[i]);
   if (c->env.own_stream && c->env.stream) cudaStreamDestroy(c->env.stream);
   delete c;
@@ -191,8 +193,8 @@ uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
     c->env.err = "tile_capacity must be in [256, 8192]";
     return UC_EINPUT;
   }
-  if (t->tile_threads && t->tile_threads != 256 && t->tile_threads != 512 && t->tile_threads != 1024) {
-    c->env.err = "tile_threads must be 256, 512 or 1024";
+  if (t->tile_threads && t->tile_threads != 256 && t->tile_threads != 512) {
+    c->env.err = "tile_threads must be 256 or 512";
     return UC_EINPUT;
   }
   if (t->contract_method != UC_CONTRACT_POINTER_JUMP && t->contract_method != UC_CONTRACT_HEC) {
@@ -201,6 +203,14 @@ uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
   }
   if (t->warp_capacity > 1 && (t->warp_capacity < 32 || t->warp_capacity > 1024 || t->warp_capacity % 32)) {
     c->env.err = "warp_capacity must be 0, 1 or a multiple of 32 in [32, 1024]";
+    return UC_EINPUT;
+  }
+  if (t->load_factor_pct && (t->load_factor_pct < 150 || t->load_factor_pct > 800)) {
+    c->env.err = "load_factor_pct must be 0 or in [150, 800]";
+    return UC_EINPUT;
+  }
+  if (t->bucket_fill > 64) {
+    c->env.err = "bucket_fill must be 0 or in [1, 64]";
     return UC_EINPUT;
   }
   if (t->bucket_bits > 25) {
@@ -297,6 +307,120 @@ uc_status uc_compact_device(uc_ctx* c, const char* d_text, size_t bytes, int k, 
   c->env.reset();
   *out_bytes = ob;
   return as_status(r);
+}
+
+// ---- autotuner --------------------------------------------------------
+
+namespace {
+
+struct Knob {
+  uint32_t uc_tuning::*field;
+  std::vector<uint32_t> values;
+};
+
+bool tuning_valid(const uc_tuning& t) {
+  return t.warp_capacity <= 1 || t.warp_capacity <= t.tile_capacity;
+}
+
+}  // namespace
+
+uc_status uc_autotune(uc_ctx* c, const char* d_text, size_t bytes, int k, int l, int reps, uint32_t max_ms,
+                      uc_tuning* best, float* best_ms, uint32_t* trials) {
+  if (!c || !d_text || !best) return UC_EINPUT;
+  uc_status s = set_device(c);
+  if (s) return s;
+  const uint64_t bound = uc::output_bound(bytes, k);
+  s = grow(c, &c->io_out, &c->io_out_cap, bound);
+  if (s) return s;
+  if (reps < 1) reps = 3;
+  const double limit = max_ms ? double(max_ms) : 60000.0;
+  const uc_tuning saved = c->env.tune;
+  double spent = 0.0;
+  uint32_t n_trials = 0;
+  uint64_t ref_bytes = 0;
+  bool have_ref = false;
+  // median device time of reps runs after one warm-up run
+  auto time_one = [&](const uc_tuning& t, float& ms) -> int {
+    c->env.tune = t;
+    uint64_t ob = 0;
+    uc_stats st{};
+    int r = uc::compact_device(c->env, d_text, bytes, k, l, c->io_out, bound, ob, &st);
+    c->env.reset();
+    if (r) return r;
+    spent += st.ms_total;
+    std::vector<float> v;
+    for (int i = 0; i < reps; ++i) {
+      r = uc::compact_device(c->env, d_text, bytes, k, l, c->io_out, bound, ob, &st);
+      c->env.reset();
+      if (r) return r;
+      v.push_back(st.ms_total);
+      spent += st.ms_total;
+    }
+    std::sort(v.begin(), v.end());
+    ms = v[v.size() / 2];
+    ++n_trials;
+    if (!have_ref) {
+      ref_bytes = ob;
+      have_ref = true;
+    } else if (ob != ref_bytes) {
+      c->env.err = "autotune: a candidate tuning produced a different output size";
+      return UC_EINTERNAL;
+    }
+    return UC_OK;
+  };
+  uc_tuning cur{};
+  cur.tile_capacity = 4096;
+  cur.tile_threads = 512;
+  cur.load_factor_pct = 200;
+  cur.contract_method = UC_CONTRACT_POINTER_JUMP;
+  cur.warp_capacity = 256;
+  cur.bucket_fill = 8;
+  float cur_ms = 0.f;
+  int r = time_one(cur, cur_ms);
+  if (r) {
+    c->env.tune = saved;
+    return as_status(r);
+  }
+  const Knob knobs[] = {
+      {&uc_tuning::warp_capacity, {1, 64, 128, 256, 512}},
+      {&uc_tuning::bucket_fill, {2, 4, 8, 16, 32}},
+      {&uc_tuning::tile_capacity, {1024, 2048, 4096, 8192}},
+      {&uc_tuning::tile_threads, {256, 512}},
+      {&uc_tuning::load_factor_pct, {150, 200, 300, 400}},
+      {&uc_tuning::contract_method, {UC_CONTRACT_POINTER_JUMP, UC_CONTRACT_HEC}},
+  };
+  // coordinate descent: each knob in turn over its values, the others held;
+  // a change must win by 1% to be kept; stop after a pass with no change
+  for (int pass = 0; pass < 3 && spent < limit; ++pass) {
+    bool changed = false;
+    for (const Knob& kn : knobs) {
+      for (uint32_t v : kn.values) {
+        if (spent >= limit) break;
+        if (cur.*(kn.field) == v) continue;
+        uc_tuning cand = cur;
+        cand.*(kn.field) = v;
+        if (!tuning_valid(cand)) continue;
+        float ms = 0.f;
+        r = time_one(cand, ms);
+        if (r == UC_EINTERNAL || r == UC_ECUDA) {
+          c->env.tune = saved;
+          return as_status(r);
+        }
+        if (r) continue;  // a candidate that does not fit (budget, shared memory) is skipped
+        if (ms < cur_ms * 0.99f) {
+          cur = cand;
+          cur_ms = ms;
+          changed = true;
+        }
+      }
+    }
+    if (!changed) break;
+  }
+  c->env.tune = cur;
+  *best = cur;
+  if (best_ms) *best_ms = cur_ms;
+  if (trials) *trials = n_trials;
+  return UC_OK;
 }
 
 uint64_t uc_batch_output_bound(int njobs, const size_t* bytes, int k) {

@@ -59,6 +59,7 @@ struct TileParams {
   int k;
   uint32_t cap;                 // shared-memory tile capacity (copies)
   uint32_t tslots;              // shared-memory hash slots (power of two >= 2*cap)
+  uint32_t lf;                  // hash slots per 100 copies of a tile (150..800)
   int mode;                     // 0 = edges by id, 1 = fused emission
   uint32_t* succ;
   uint32_t* pred;
@@ -87,6 +88,13 @@ __host__ __device__ inline uint32_t pow2_at_least(uint64_t x) {
   uint32_t p = 1;
   for (int i = 0; i < 31 && p < x; ++i) p <<= 1;
   return p;
+}
+
+// Carved table of a tile of c copies: the hash slots, and at least 2c
+// entries because the table doubles as rank scratch after hashing.
+__host__ __device__ inline uint32_t big_slots(uint64_t c, uint32_t lf) {
+  const uint64_t want = c * lf / 100;
+  return pow2_at_least(want > 2 * c ? want : 2 * c);
 }
 
 }  // namespace uc

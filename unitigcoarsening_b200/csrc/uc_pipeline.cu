@@ -140,8 +140,11 @@ __device__ __forceinline__ uint32_t job_of_block(const JobTab* __restrict__ jobs
   return lo;
 }
 
-template <int NW, bool FUSE>
-__global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, uint32_t njobs, uint64_t nblocks,
+// MULTI: the block's job comes from the job table (batches); otherwise the
+// one job is a kernel parameter, read from the constant bank.
+template <int NW, bool FUSE, bool MULTI>
+__global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, const JobTab one, uint32_t njobs,
+                                              uint64_t nblocks,
                                               const unsigned long long* __restrict__ starts, int k,
                                               uint64_t* __restrict__ keys, uint32_t* err, int l, uint64_t seed,
                                               uint32_t jb, uint32_t* __restrict__ b1, uint32_t* __restrict__ b2,
@@ -153,11 +156,14 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, u
   const uint64_t kmask_hi = (NW == 1) ? ((k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull))
                                       : ((2 * k - 64 >= 64) ? ~0ull : ((1ull << (2 * k - 64)) - 1ull));
   for (uint64_t g = blockIdx.x; g < nblocks; g += gridDim.x) {
-    const uint32_t j = job_of_block(jobs, njobs, g);
-    const uint8_t* text = jobs[j].text;
-    const uint64_t tbytes = jobs[j].tbytes, body = jobs[j].body, end = jobs[j].end, n = jobs[j].n;
-    const uint64_t koff = jobs[j].koff;
-    const uint64_t b0 = (g - jobs[j].lb0) * PACK_LINES;
+    const uint32_t j = MULTI ? job_of_block(jobs, njobs, g) : 0u;
+    const uint8_t* text = MULTI ? jobs[j].text : one.text;
+    const uint64_t tbytes = MULTI ? jobs[j].tbytes : one.tbytes;
+    const uint64_t body = MULTI ? jobs[j].body : one.body;
+    const uint64_t end = MULTI ? jobs[j].end : one.end;
+    const uint64_t n = MULTI ? jobs[j].n : one.n;
+    const uint64_t koff = MULTI ? jobs[j].koff : one.koff;
+    const uint64_t b0 = (g - (MULTI ? jobs[j].lb0 : one.lb0)) * PACK_LINES;
     const uintptr_t tb = reinterpret_cast<uintptr_t>(text);
     const uint32_t cnt = uint32_t((n - b0) < PACK_LINES ? (n - b0) : PACK_LINES);
     const uint64_t s0 = starts ? uint64_t(starts[b0]) : body + b0 * stride;
@@ -418,7 +424,8 @@ __global__ void k_tile_write(const uint32_t* __restrict__ flag, const uint32_t* 
 // tiles (with the global scratch each one needs).
 __global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Counters* ctr, uint32_t wcap,
                            uint32_t cap, uint32_t* __restrict__ wlist, uint32_t* __restrict__ blist,
-                           uint32_t* __restrict__ big_list, unsigned long long* __restrict__ big_size, int nw) {
+                           uint32_t* __restrict__ big_list, unsigned long long* __restrict__ big_size, int nw,
+                           uint32_t lf) {
   const uint32_t nt = ctr->ntiles;
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     const uint64_t c = tile_begin[t + 1] - tile_begin[t];
@@ -435,7 +442,7 @@ __global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Co
     } else {
       const uint32_t i = atomicAdd(&ctr->nbig, 1u);
       big_list[i] = t;
-      const uint64_t ts = uint64_t(pow2_at_least(2 * c));
+      const uint64_t ts = big_slots(c, lf);
       big_size[i] = (c * (8ull * nw + 16ull) + ts * 4ull + 255ull) & ~255ull;
     }
   }
@@ -817,7 +824,15 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
                              uint32_t job) {
   constexpr uint32_t NONE_I = Ix<IT>::NONE, DUP_I = Ix<IT>::DUP, CNONE_I = Ix<IT>::CNONE;
   const PrefMask pm = pref_mask(p.k);
-  const uint32_t ts = pow2_at_least(2ull * c);  // this tile's slots (<= m.ts)
+  // this tile's hash slots: the power of two above c * lf / 100, at most the
+  // carved table (32-bit arithmetic for shared-memory tiles, c <= 8192)
+  uint32_t ts;
+  {
+    const uint32_t want = (sizeof(IT) == 2) ? (c * p.lf) / 100u : uint32_t((uint64_t(c) * p.lf) / 100u);
+    const uint32_t x = want > c ? want : c + 1u;
+    ts = 1u << (32 - __clz(x - 1u));
+    ts = ts < m.ts ? ts : m.ts;
+  }
   const uint32_t tmask = ts - 1;
   const int k = p.k;
   // ---- stage the tile's keys (async copies), initialise the work arrays
@@ -1092,7 +1107,7 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
   const uint32_t t = p.big_list[blockIdx.x];
   const uint64_t beg = p.tile_begin[t];
   const uint64_t c = p.tile_begin[t + 1] - beg;
-  const uint32_t ts = pow2_at_least(2 * c);
+  const uint32_t ts = big_slots(c, p.lf);
   const TileMem<NW, uint32_t> m = carve<NW, uint32_t>(p.big_scratch + p.big_off[blockIdx.x], uint32_t(c), ts);
   process_tile<NW, uint32_t, BlockGroup>(p, m, beg, uint32_t(c), p.tile_job[t]);
 }
@@ -1137,20 +1152,40 @@ constexpr uint32_t HEAD_BIT = 0x80000000u;
 __device__ __forceinline__ uint32_t ptr_of(unsigned long long v) { return pk_p(v) & ~HEAD_BIT; }
 __device__ __forceinline__ bool is_head_entry(unsigned long long v) { return (pk_p(v) & HEAD_BIT) != 0; }
 
+// Slot for a lane that appends to a shared list: one atomic per warp.
+// Every lane of the warp must call it (pred false = no slot).
+__device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool pred) {
+  const uint32_t m = __ballot_sync(0xFFFFFFFFu, pred);
+  if (!m) return NONE;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(m) - 1;
+  uint32_t b = 0;
+  if (lane == leader) b = atomicAdd(count, uint32_t(__popc(m)));
+  b = __shfl_sync(0xFFFFFFFFu, b, leader);
+  return pred ? b + uint32_t(__popc(m & ((1u << lane) - 1u))) : NONE;
+}
+
 // X[v] = (start pointer, weight distance); heads point at themselves.
 __global__ void k_rank_init(const uint32_t* __restrict__ prev, const uint32_t* __restrict__ w,
                             uint64_t n, const Counters* ctr, unsigned long long* __restrict__ X,
                             uint32_t* __restrict__ act, uint32_t* act_count) {
   const uint64_t N = ctr ? uint64_t(ctr->seg_count) : n;
-  for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < N;
-       s += uint64_t(gridDim.x) * blockDim.x) {
-    const uint32_t pv = prev[s];
-    if (pv == NONE) {
-      X[s] = pk(uint32_t(s) | HEAD_BIT, 0);
-    } else {
-      X[s] = pk(pv, w ? w[pv] : 1u);
-      act[atomicAdd(act_count, 1u)] = uint32_t(s);
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  // whole warps iterate together (warp_append needs every lane)
+  for (uint64_t s0 = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); s0 < N; s0 += stride) {
+    const uint64_t s = s0 + (threadIdx.x & 31);
+    bool tail = false;
+    if (s < N) {
+      const uint32_t pv = prev[s];
+      if (pv == NONE) {
+        X[s] = pk(uint32_t(s) | HEAD_BIT, 0);
+      } else {
+        X[s] = pk(pv, w ? w[pv] : 1u);
+        tail = true;
+      }
     }
+    const uint32_t slot = warp_append(act_count, tail);
+    if (tail) act[slot] = uint32_t(s);
   }
 }
 
@@ -1162,15 +1197,24 @@ __global__ void k_rank_round(unsigned long long* __restrict__ X, const uint32_t*
                              const uint32_t* act_count, uint32_t* __restrict__ act_out,
                              uint32_t* act_out_count) {
   const uint32_t na = *act_count;
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < na; j += gridDim.x * blockDim.x) {
-    const uint32_t s = act[j];
-    const unsigned long long v = reinterpret_cast<volatile unsigned long long*>(X)[s];
-    const unsigned long long u = reinterpret_cast<volatile unsigned long long*>(X)[ptr_of(v)];
-    if (is_head_entry(u)) continue;  // already points at a head
-    const unsigned long long nv = pk(ptr_of(u), pk_o(v) + pk_o(u));
-    reinterpret_cast<volatile unsigned long long*>(X)[s] = nv;
-    const unsigned long long z = reinterpret_cast<volatile unsigned long long*>(X)[ptr_of(nv)];
-    if (!is_head_entry(z)) act_out[atomicAdd(act_out_count, 1u)] = s;
+  const uint32_t stride = gridDim.x * blockDim.x;
+  for (uint32_t j0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); j0 < na; j0 += stride) {
+    const uint32_t j = j0 + (threadIdx.x & 31);
+    bool keep = false;
+    uint32_t s = 0;
+    if (j < na) {
+      s = act[j];
+      const unsigned long long v = reinterpret_cast<volatile unsigned long long*>(X)[s];
+      const unsigned long long u = reinterpret_cast<volatile unsigned long long*>(X)[ptr_of(v)];
+      if (!is_head_entry(u)) {  // not yet pointing at a head
+        const unsigned long long nv = pk(ptr_of(u), pk_o(v) + pk_o(u));
+        reinterpret_cast<volatile unsigned long long*>(X)[s] = nv;
+        const unsigned long long z = reinterpret_cast<volatile unsigned long long*>(X)[ptr_of(nv)];
+        keep = !is_head_entry(z);
+      }
+    }
+    const uint32_t slot = warp_append(act_out_count, keep);
+    if (keep) act_out[slot] = s;
   }
 }
 
@@ -1193,28 +1237,47 @@ __global__ void k_head_len(uint32_t S, const uint32_t* __restrict__ seg_len, con
     v[s] = (seg_len[s] && prev[s] == NONE && !oncycle[s]) ? linelen[s] : 0u;
 }
 
-// Copy each segment's chars into its line (warp per segment).
-__global__ void k_seg_copy(uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
-                           const JobTab* __restrict__ jobs, const unsigned long long* __restrict__ jclosed,
-                           const unsigned long long* __restrict__ X,
-                           const uint32_t* __restrict__ next, const uint32_t* __restrict__ prev,
-                           const uint32_t* __restrict__ w, const uint8_t* __restrict__ oncycle,
-                           const unsigned long long* __restrict__ seg_off,
-                           const unsigned long long* __restrict__ loff, const char* __restrict__ segchars,
-                           char* __restrict__ out, int k) {
+// Copy each segment's chars into its line.  A warp takes 32 consecutive
+// segments: each lane resolves one segment's source, destination and length
+// (independent loads, issued together), then the warp copies the 32
+// segments one after another, 32 bytes per step.
+__global__ void __launch_bounds__(256) k_seg_copy(
+    uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
+    const JobTab* __restrict__ jobs, const unsigned long long* __restrict__ jclosed,
+    const unsigned long long* __restrict__ X, const uint32_t* __restrict__ next,
+    const uint32_t* __restrict__ prev, const uint32_t* __restrict__ w, const uint8_t* __restrict__ oncycle,
+    const unsigned long long* __restrict__ seg_off, const unsigned long long* __restrict__ loff,
+    const char* __restrict__ segchars, char* __restrict__ out, int k) {
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t s = warp; s < S; s += nwarps) {
-    if (!seg_len[s] || oncycle[s]) continue;
-    const unsigned long long v = X[s];
-    const uint32_t job = seg_job[s];
-    const JobTab& J = jobs[job];
-    char* dst = out + J.obase + jclosed[job] + (loff[ptr_of(v)] - loff[J.seg_base]) + pk_o(v);
-    const char* src = segchars + seg_off[s] + ((prev[s] == NONE) ? 0 : k);
-    const uint32_t nb = w[s];
-    for (uint32_t j = lane; j < nb; j += 32) dst[j] = src[j];
-    if (lane == 0 && next[s] == NONE) dst[nb] = '\n';
+  for (uint32_t base = warp * 32u; base < S; base += nwarps * 32u) {
+    const uint32_t s = base + uint32_t(lane);
+    bool live = s < S;
+    uint64_t dst = 0, src = 0;
+    uint32_t nb = 0, last = 0;
+    if (live) live = seg_len[s] != 0 && !oncycle[s];
+    if (live) {
+      const unsigned long long v = X[s];
+      const uint32_t job = seg_job[s];
+      const uint64_t obase = jobs[job].obase;
+      const uint32_t sb = jobs[job].seg_base;
+      dst = obase + jclosed[job] + (loff[ptr_of(v)] - loff[sb]) + pk_o(v);
+      src = seg_off[s] + ((prev[s] == NONE) ? 0u : uint32_t(k));
+      nb = w[s];
+      last = next[s] == NONE;
+    }
+    uint32_t todo = __ballot_sync(0xFFFFFFFFu, live);
+    while (todo) {
+      const int q = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint64_t d = __shfl_sync(0xFFFFFFFFu, dst, q);
+      const uint64_t c = __shfl_sync(0xFFFFFFFFu, src, q);
+      const uint32_t m = __shfl_sync(0xFFFFFFFFu, nb, q);
+      const uint32_t e = __shfl_sync(0xFFFFFFFFu, last, q);
+      for (uint32_t j = lane; j < m; j += 32) out[d + j] = segchars[c + j];
+      if (lane == 0 && e) out[d + m] = '\n';
+    }
   }
 }
 
@@ -1639,6 +1702,9 @@ int Env::reserve(int w, size_t bytes) {
   Arena& a = ar[w];
   bytes += size_t(16) << 20;
   if (bytes <= a.cap) return UC_OK;
+  if (pool)
+    return fail(UC_EBUDGET, "job needs " + std::to_string(bytes >> 20) + " MiB in arena " + std::to_string(w) +
+                                ", its pool slice holds " + std::to_string(a.cap >> 20) + " MiB");
   if (a.used) return fail(UC_EINTERNAL, "arena grown while in use");
   const size_t other = ar[1 - w].cap;
   if (bytes + other > budget)
@@ -1739,17 +1805,42 @@ struct FuseArgs {
   uint64_t M = 0;
 };
 
+template <int NW, bool FUSE, bool MULTI>
+static int pack_occupancy() {
+  static int o = 0;  // resident CTAs per SM (per template instance)
+  if (!o) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_pack<NW, FUSE, MULTI>, 256, 0);
+    if (o < 1) o = 1;
+  }
+  return o;
+}
+
+// one: the job of a single-job launch (host copy), or NULL for a batch
+// whose jobs the kernel finds in the table.
 template <int NW>
-static void launch_pack(Env& e, const JobTab* jobs, uint32_t njobs, uint64_t nblocks,
+static void launch_pack(Env& e, const JobTab* jobs, const JobTab* one, uint32_t njobs, uint64_t nblocks,
                         const unsigned long long* starts, int k, uint64_t* keys, const FuseArgs* fz) {
-  const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(nblocks, uint64_t(e.sm_count) * 8)));
+  // one wave of resident CTAs: blocks stride over equal-sized line blocks,
+  // so a partial second wave would double the time
+  const int o = fz ? (one ? pack_occupancy<NW, true, false>() : pack_occupancy<NW, true, true>())
+                   : (one ? pack_occupancy<NW, false, false>() : pack_occupancy<NW, false, true>());
+  const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(nblocks, uint64_t(e.sm_count) * o)));
+  const JobTab J = one ? *one : JobTab{};
   ++e.launches;
-  if (fz)
-    k_pack<NW, true><<<grid, 256, 0, e.stream>>>(jobs, njobs, nblocks, starts, k, keys, &e.ctr->err, fz->l,
-                                                 fz->seed, fz->jb, fz->b1, fz->b2, fz->counts, fz->jcross);
+  if (fz && one)
+    k_pack<NW, true, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
+                                                        fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
+                                                        fz->jcross);
+  else if (fz)
+    k_pack<NW, true, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
+                                                       fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
+                                                       fz->jcross);
+  else if (one)
+    k_pack<NW, false, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
+                                                         0, 0, nullptr, nullptr, nullptr, nullptr);
   else
-    k_pack<NW, false><<<grid, 256, 0, e.stream>>>(jobs, njobs, nblocks, starts, k, keys, &e.ctr->err, 0, 0, 0,
-                                                  nullptr, nullptr, nullptr, nullptr);
+    k_pack<NW, false, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
+                                                        0, 0, nullptr, nullptr, nullptr, nullptr);
 }
 
 // Grow-only device buffers for the job table and the per-job counters.
@@ -1805,8 +1896,8 @@ static int pack_single(Env& e, const char* d_text, size_t bytes, int k, uint64_t
   bool fixed = J.fixed != 0;
   int st;
   if (fixed) {
-    if (nw == 1) launch_pack<1>(e, jdev, 1, nblocks, nullptr, k, d_keys, fz);
-    else launch_pack<2>(e, jdev, 1, nblocks, nullptr, k, d_keys, fz);
+    if (nw == 1) launch_pack<1>(e, jdev, &J, 1, nblocks, nullptr, k, d_keys, fz);
+    else launch_pack<2>(e, jdev, &J, 1, nblocks, nullptr, k, d_keys, fz);
     UC_CK(cudaGetLastError());
     st = e.read_ctr();
     if (st) return st;
@@ -1841,8 +1932,8 @@ static int pack_single(Env& e, const char* d_text, size_t bytes, int k, uint64_t
     if (lines_m1 + 1 != n) return e.fail(UC_EINPUT, "header count differs from the number of lines");
     ++e.launches;
     k_write_starts<<<unsigned(nchunks), 256, 0, e.stream>>>(text, body, end, off, chunk, starts, n);
-    if (nw == 1) launch_pack<1>(e, jdev, 1, nblocks, starts, k, d_keys, fz);
-    else launch_pack<2>(e, jdev, 1, nblocks, starts, k, d_keys, fz);
+    if (nw == 1) launch_pack<1>(e, jdev, &J, 1, nblocks, starts, k, d_keys, fz);
+    else launch_pack<2>(e, jdev, &J, 1, nblocks, starts, k, d_keys, fz);
     UC_CK(cudaGetLastError());
     st = e.read_ctr();
     e.ar[1].used = 0;
@@ -1903,7 +1994,7 @@ int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
 // sizes jb, and njobs << jb buckets in all (rounded up to a power of two,
 // bits = log2 of that).
 struct Plan {
-  uint32_t bits, jb, cap, win, small, tslots, wcap, wts, wbytes;
+  uint32_t bits, jb, cap, win, small, tslots, wcap, wts, wbytes, lf;
   int l_used;
   uint64_t M;
 };
@@ -1930,15 +2021,18 @@ static Plan plan_buckets(const Env& e, uint64_t nmax, uint32_t njobs, int k, int
   if (e.tune.bucket_bits) {
     jb = e.tune.bucket_bits;
   } else {
-    while ((copies >> jb) > pack_cap / 8 && jb < 25) ++jb;  // ~capacity/8 copies per bucket
+    // about bucket_fill buckets per tile: small enough that tiles pack well,
+    // large enough that each bucket gathers several l-mers
+    const uint32_t fill = e.tune.bucket_fill ? e.tune.bucket_fill : 8;
+    while ((copies >> jb) > std::max<uint32_t>(1, pack_cap / fill) && jb < 25) ++jb;
   }
   jb = std::min(jb, jbits_max);
   // enough l-mers that each bucket gathers several of them
   const int lmin = int((jb + 2 + 1) / 2);
   int lu = std::max(l, lmin);
   lu = std::min(lu, std::min(16, k - 1));
-  uint32_t ts = pow2_at_least(uint64_t(cap) * std::max<uint32_t>(200, e.tune.load_factor_pct) / 100);
-  if (ts < 2 * cap) ts = pow2_at_least(2ull * cap);
+  const uint32_t lf = e.tune.load_factor_pct ? e.tune.load_factor_pct : 200;
+  uint32_t ts = big_slots(cap, lf);
   while (ts > pow2_at_least(2ull * cap) && tile_bytes(nw, cap, ts) > size_t(e.smem_optin)) ts >>= 1;
   P.jb = jb;
   P.bits = ceil_log2(uint64_t(njobs) << jb);
@@ -1947,7 +2041,12 @@ static Plan plan_buckets(const Env& e, uint64_t nmax, uint32_t njobs, int k, int
   P.small = pack_cap / 4;
   P.tslots = ts;
   P.wcap = warp_tier ? wcap : 0;
-  P.wts = warp_tier ? pow2_at_least(2ull * wcap) : 0;
+  uint32_t wts = warp_tier ? big_slots(wcap, lf) : 0;
+  // eight warp tiles share a CTA's shared memory
+  while (warp_tier && wts > pow2_at_least(2ull * wcap) && 8 * tile_bytes(nw, wcap, wts) > size_t(e.smem_optin))
+    wts >>= 1;
+  P.wts = wts;
+  P.lf = lf;
   P.wbytes = warp_tier ? uint32_t((tile_bytes(nw, wcap, P.wts) + 15) & ~size_t(15)) : 0;
   P.l_used = lu;
   P.M = 1ull << P.bits;
@@ -2004,6 +2103,19 @@ static int bucket_offsets(Env& e, const Front& f, uint64_t M, uint64_t& copies) 
   return UC_OK;
 }
 
+// Let a kernel take all the dynamic shared memory an SM offers a block.  The
+// attribute is process-wide, so it is always set to the same maximum: a
+// per-call size would let one host thread lower it under another thread's
+// launch (concurrent contexts and server lanes).
+template <class K>
+static int allow_max_smem(Env& e, K kernel) {
+  cudaFuncAttributes a{};
+  UC_CK(cudaFuncGetAttributes(&a, kernel));
+  UC_CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             e.smem_optin - int(a.sharedSizeBytes)));
+  return UC_OK;
+}
+
 // Level split of the scatter: 2^mcb coarse partitions of 2^fb buckets.
 static void scatter_split(uint32_t bbits, uint32_t& mcb, uint32_t& fb) {
   mcb = std::min<uint32_t>(bbits, 8);
@@ -2033,9 +2145,16 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
     e.launches += 1;
     k_coarse_init<<<grid_for(e, mc, 256), 256, 0, e.stream>>>(f.boff, fb, mc, f.cursor);
     const size_t sm1 = size_t(2 * SC_CHUNK) * (8 * nw + 8) + size_t(mc) * 16 + 16;
-    UC_CK(cudaFuncSetAttribute(k_scatter_coarse<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
-    UC_CK(cudaFuncSetAttribute(k_scatter_coarse<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm1)));
-    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + SC_CHUNK - 1) / SC_CHUNK, uint64_t(e.sm_count) * 6)));
+    int r0 = allow_max_smem(e, k_scatter_coarse<1>);
+    if (!r0) r0 = allow_max_smem(e, k_scatter_coarse<2>);
+    if (r0) return r0;
+    // one wave of resident CTAs (the chunks are strided statically)
+    int o1 = 0;
+    if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<1>, 256, sm1));
+    else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<2>, 256, sm1));
+    if (o1 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
+    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + SC_CHUNK - 1) / SC_CHUNK,
+                                                                uint64_t(e.sm_count) * uint64_t(o1))));
     UC_CK(cudaMemcpyAsync(f.fcur, f.boff, M * 8, cudaMemcpyDeviceToDevice, e.stream));
     UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
     const int g2 = e.sm_count * 8;
@@ -2051,7 +2170,7 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
   }
   ++e.launches;
   k_classify<<<grid_for(e, M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, P.wcap, P.cap, f.wlist, f.blist,
-                                                         f.big_list, f.big_size, nw);
+                                                         f.big_list, f.big_size, nw, P.lf);
   UC_CK(cudaGetLastError());
   return UC_OK;
 }
@@ -2060,24 +2179,32 @@ template <int NW>
 static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
   tp.wlist = f.wlist;
   tp.blist = f.blist;
+  const size_t wsm = size_t(tp.wbytes) * 8;
+  int wocc = 0;
   if (tp.wcap) {
-    const size_t wsm = size_t(tp.wbytes) * 8;
-    UC_CK(cudaFuncSetAttribute(k_tile_warp<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(wsm)));
-    int wocc = 0;
+    const int r0 = allow_max_smem(e, k_tile_warp<NW>);
+    if (r0) return r0;
     UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wocc, k_tile_warp<NW>, 256, wsm));
     if (wocc < 1) return e.fail(UC_EINTERNAL, "warp tile kernel does not fit an SM");
+  }
+  cudaEventRecord(e.ev[8], e.stream);
+  if (tp.wcap) {
     ++e.launches;
     k_tile_warp<NW><<<e.sm_count * wocc, 256, wsm, e.stream>>>(tp);
     UC_CK(cudaGetLastError());
   }
+  cudaEventRecord(e.ev[9], e.stream);
   const size_t smem = tile_bytes(NW, tp.cap, tp.tslots);
-  UC_CK(cudaFuncSetAttribute(k_tile<NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  const int r1 = allow_max_smem(e, k_tile<NW>);
+  if (r1) return r1;
   int occ = 0;
   UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<NW>, int(threads), smem));
   if (occ < 1) return e.fail(UC_EINTERNAL, "tile kernel does not fit an SM");
   ++e.launches;
   k_tile<NW><<<e.sm_count * occ, threads, smem, e.stream>>>(tp);
   UC_CK(cudaGetLastError());
+  cudaEventRecord(e.ev[5], e.stream);
+  e.tiles_timed = true;
   // oversized tiles: one CTA each in global scratch
   int st = e.read_ctr();
   if (st) return st;
@@ -2093,7 +2220,11 @@ static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
       tot += sz[i];
     }
     const size_t want = size_t(tot) + size_t(nbig) * 8 + 4096;
-    if (want > e.big_cap) {
+    char* big = nullptr;
+    if (e.pool) {
+      big = static_cast<char*>(e.take(1, want));
+      if (!big) return e.fail(UC_EBUDGET, "scratch for oversized buckets exceeds the pool slice");
+    } else if (want > e.big_cap) {
       if (e.big_buf) {
         cudaStreamSynchronize(e.stream);
         cudaFree(e.big_buf);
@@ -2108,8 +2239,9 @@ static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
       }
       e.big_cap = want;
     }
-    unsigned long long* d_off = reinterpret_cast<unsigned long long*>(e.big_buf);
-    char* scratch = e.big_buf + ((size_t(nbig) * 8 + 255) & ~size_t(255));
+    if (!big) big = e.big_buf;
+    unsigned long long* d_off = reinterpret_cast<unsigned long long*>(big);
+    char* scratch = big + ((size_t(nbig) * 8 + 255) & ~size_t(255));
     UC_CK(cudaMemcpyAsync(d_off, off.data(), nbig * 8, cudaMemcpyHostToDevice, e.stream));
     tp.big_list = f.big_list;
     tp.big_scratch = scratch;
@@ -2162,6 +2294,7 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   tp.k = k;
   tp.cap = P.cap;
   tp.tslots = P.tslots;
+  tp.lf = P.lf;
   tp.wcap = P.wcap;
   tp.wts = P.wts;
   tp.wbytes = P.wbytes;
@@ -2486,6 +2619,43 @@ uint64_t output_bound(size_t text_bytes, int k) {
   return uint64_t(text_bytes) + 64;
 }
 
+// Back arena bytes of the fused path: the bucketed copies and their staging,
+// the segment pool (Sp segments for X cross k-mers) and the stitch arrays.
+static size_t back_bytes(uint64_t copies, uint64_t X, uint64_t Sp, int nw, int k, bool want_hec) {
+  const uint64_t segchars = Sp * uint64_t(k) + copies + 64;
+  const uint32_t R = 64;
+  size_t back = 0;
+  auto add = [&](size_t b) { back += (b + 255) & ~size_t(255); };
+  add(copies * 8 * nw); add(copies * 4);                                  // copies
+  add(scatter_stage_bytes(copies, nw));                                   // level-1 staging
+  add(Sp * 8); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // seg_off, len, sx, ex, job
+  add((X + 1) * 4); add((X + 1) * 4);                                     // start_seg, end_seg
+  add(segchars);
+  add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // next, prev, w, act0, act1
+  add(Sp * 4); add(Sp * 4); add(Sp * 8); add((Sp + 1) * 8); add(Sp);     // llen, hlen, X, loff, oncyc
+  add(scan_tmp_elems(Sp) * 8); add(R * 4);
+  if (want_hec) add(hec_bytes(Sp, hec_rounds(Sp)));
+  return back;
+}
+
+void batch_footprint(const Env& e, uint32_t njobs, const size_t* bytes, int k, int l, size_t& front,
+                     size_t& back) {
+  const int nw = (k <= 31) ? 1 : 2;
+  uint64_t N = 0, nmax = 0, tb = 0;
+  for (uint32_t j = 0; j < njobs; ++j) {
+    const uint64_t n = (uint64_t(bytes[j]) + 1) / uint64_t(k + 1) + 1;
+    N += n;
+    nmax = std::max(nmax, n);
+    tb = std::max<uint64_t>(tb, bytes[j]);
+  }
+  const Plan P = plan_buckets(e, nmax, njobs, k, l);
+  const size_t slack = size_t(16) << 20;
+  front = front_bytes(N, nw, P.M, true) + slack + 4096;
+  const uint64_t X = N, copies = N + X, Sp = 2 * X + njobs;
+  back = std::max(back_bytes(copies, X, Sp, nw, k, e.tune.contract_method == UC_CONTRACT_HEC),
+                  line_index_bytes(tb, nmax)) + slack + 4096;
+}
+
 // The fused path.  Device memory: the front arena holds per-k-mer arrays
 // (keys, bucket ids) and per-bucket arrays; the back arena, sized once the
 // cross k-mers X are counted, holds the n+X bucketed copies and the segment
@@ -2567,8 +2737,8 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     r = pack_single(e, texts[0], bytes[0], k, f.keys, &fz, J[0], jd.tab);
     if (r) return r;
   } else if (N > 0) {
-    if (nw == 1) launch_pack<1>(e, jd.tab, njobs, lb, nullptr, k, f.keys, &fz);
-    else launch_pack<2>(e, jd.tab, njobs, lb, nullptr, k, f.keys, &fz);
+    if (nw == 1) launch_pack<1>(e, jd.tab, nullptr, njobs, lb, nullptr, k, f.keys, &fz);
+    else launch_pack<2>(e, jd.tab, nullptr, njobs, lb, nullptr, k, f.keys, &fz);
     UC_CK(cudaGetLastError());
   }
   cudaEventRecord(e.ev[1], e.stream);
@@ -2596,17 +2766,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   const uint32_t R = 64;
   const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
   const uint32_t RH = hec_rounds(Sp);
-  size_t back = 0;
-  auto add = [&](size_t b) { back += (b + 255) & ~size_t(255); };
-  add(copies * 8 * nw); add(copies * 4);                                  // copies
-  add(scatter_stage_bytes(copies, nw));                                   // level-1 staging
-  add(Sp * 8); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // seg_off, len, sx, ex, job
-  add((X + 1) * 4); add((X + 1) * 4);                                     // start_seg, end_seg
-  add(segchars);
-  add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // next, prev, w, act0, act1
-  add(Sp * 4); add(Sp * 4); add(Sp * 8); add((Sp + 1) * 8); add(Sp);     // llen, hlen, X, loff, oncyc
-  add(scan_tmp_elems(Sp) * 8); add(R * 4);
-  if (want_hec) add(hec_bytes(Sp, RH));
+  const size_t back = back_bytes(copies, X, Sp, nw, k, want_hec);
   r = e.reserve(1, back);
   if (r) return r;
   auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
@@ -2656,6 +2816,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   tp.k = k;
   tp.cap = P.cap;
   tp.tslots = P.tslots;
+  tp.lf = P.lf;
   tp.wcap = P.wcap;
   tp.wts = P.wts;
   tp.wbytes = P.wbytes;
@@ -2726,7 +2887,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   k_chain_len<<<gs, 256, 0, e.stream>>>(S, seg_len, Xr, next, wgt, oncyc, llen);
   k_head_len<<<gs, 256, 0, e.stream>>>(S, seg_len, prev, oncyc, llen, hlen);
   scan_excl<uint32_t, unsigned long long>(hlen, S, loff, stmp, e.stream);
-  k_seg_copy<<<grid_for(e, uint64_t(S) * 32, 256), 256, 0, e.stream>>>(S, seg_len, seg_job, jd.tab, jd.jclosed, Xr,
+  k_seg_copy<<<grid_for(e, S, 256), 256, 0, e.stream>>>(S, seg_len, seg_job, jd.tab, jd.jclosed, Xr,
                                                                         next, prev, wgt, oncyc, seg_off, loff, segc,
                                                                         out, k);
   k_job_finish<<<(njobs + 255) / 256, 256, 0, e.stream>>>(jd.tab, njobs, jd.jclosed, loff, jd.jout);
@@ -2744,8 +2905,9 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   }
   UC_CK(cudaGetLastError());
   cudaEventRecord(e.ev[4], e.stream);
-  std::vector<unsigned long long> jo(njobs);
+  std::vector<unsigned long long> jo(njobs), jc(st ? njobs : 0);
   UC_CK(cudaMemcpyAsync(jo.data(), jd.jout, njobs * 8, cudaMemcpyDeviceToHost, e.stream));
+  if (st) UC_CK(cudaMemcpyAsync(jc.data(), jd.jclosed, njobs * 8, cudaMemcpyDeviceToHost, e.stream));
   r = e.read_ctr();
   if (r) return r;
   if (e.h_ctr->err) return e.check_err(e.h_ctr);
@@ -2764,6 +2926,9 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     st->n_big_tiles = e.h_ctr->nbig;
     st->n_segments = Sp;
     st->n_cycles = e.h_ctr->cycles;
+    st->closed_bytes = 0;
+    for (uint32_t j = 0; j < njobs; ++j) st->closed_bytes += jc[j];
+    st->seg_chars = e.h_ctr->seg_char_cursor;
     st->out_bytes = total;
     st->stitch_rounds = rounds;
     st->l_used = uint32_t(P.l_used);
@@ -2781,6 +2946,10 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     st->ms_tiles = c;
     st->ms_stitch = d;
     st->ms_total = a + b + c + d;
+    if (e.tiles_timed) {
+      cudaEventElapsedTime(&st->ms_tile_warp, e.ev[8], e.ev[9]);
+      cudaEventElapsedTime(&st->ms_tile_block, e.ev[9], e.ev[5]);
+    }
   }
   e.reset();
   return UC_OK;

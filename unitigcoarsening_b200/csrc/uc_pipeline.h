@@ -32,7 +32,9 @@ struct Env {
   size_t jcap = 0;
   Counters* ctr = nullptr;    // device
   Counters* h_ctr = nullptr;  // pinned host mirror
-  cudaEvent_t ev[8] = {};
+  static constexpr int NEV = 10;
+  cudaEvent_t ev[NEV] = {};
+  bool tiles_timed = false;  // ev[8]/ev[9]/ev[5] bracket the warp and block tile kernels
   uc_tuning tune{};
   uint64_t seed = 0x00C0FFEE5EEDull;
   uint32_t launches = 0;    // kernels launched by the last call
@@ -43,6 +45,10 @@ struct Env {
   uint64_t gkey[2] = {0, 0};
   bool use_graphs = true;
   cudaStream_t gstream = nullptr;  // capture stream when the caller's stream is the legacy one
+  // pool mode (serving): the arenas are fixed slices of a device pool that a
+  // server owns; they never grow, and oversized-tile scratch comes from the
+  // back arena's free end
+  bool pool = false;
   std::string err;
 
   int fail(int code, const std::string& msg);
@@ -69,6 +75,11 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
 int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t* bytes, int k, int l, char* out,
                   uint64_t out_cap, uint64_t* out_off, uint64_t* out_len, uc_stats* st);
 uint64_t output_bound(size_t text_bytes, int k);
+// Upper bound of the front and back arena bytes (reserve slack included)
+// that compact_batch needs for these jobs under the current tuning, from the
+// text sizes alone: every line holds at least k+1 bytes and at most every
+// k-mer is a cross k-mer.
+void batch_footprint(const Env& e, uint32_t njobs, const size_t* bytes, int k, int l, size_t& front, size_t& back);
 // emit() over caller-provided device scratch of emit_scratch_bytes(n) bytes
 // (256-byte aligned) on stream s: the same kernels, no allocation.  Clears
 // the member counts it needs at zero itself.
