@@ -213,13 +213,15 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
-def measure_batched(args, comp):
+def measure_batched(args, device: int):
     """Many small jobs (log-normal lengths, median 3 Mbp, 0.5-8 Mbp, GC
-    30-70%, 0.2% SNPs, k=31): all of them in one batched pass against the
-    plain loop of one compaction per job, both device-resident on this GPU,
-    each the mean of the timed passes after warm-up."""
+    30-70%, 0.2% SNPs, k=31), device-resident: batched launches of
+    --batch-chunk jobs each (one tile queue per launch) against the plain
+    loop of one compaction per job, on a fresh context; each the mean of the
+    timed passes after warm-up."""
     import torch
-    from unitigcoarsening_b200 import synth
+    from unitigcoarsening_b200 import Compactor, synth
+    comp = Compactor(device)
     texts = []
     with torch.no_grad():
         for j in range(args.batch_jobs):
@@ -227,23 +229,28 @@ def measure_batched(args, comp):
     torch.cuda.synchronize()
     caps = [comp.output_bound(t.numel(), 31) for t in texts]
     one = torch.empty(max(caps), dtype=torch.uint8, device="cuda")  # the plain loop reuses one buffer
-    bout = torch.empty(sum((c + 15) // 16 * 16 for c in caps) + 64, dtype=torch.uint8, device="cuda")
+    C = max(1, args.batch_chunk)
+    chunks = [list(range(i, min(i + C, len(texts)))) for i in range(0, len(texts), C)]
+    bout = torch.empty(max(sum((caps[j] + 15) // 16 * 16 for j in ch) for ch in chunks) + 64, dtype=torch.uint8,
+                       device="cuda")
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
 
     def plain():
-        lens = []
-        for t in texts:
-            lens.append(comp.compact(t, 31, args.l, out=one).numel())
-        return lens
+        return [comp.compact(t, 31, args.l, out=one).numel() for t in texts]
 
     def batched():
-        res, st = comp.compact_batch(texts, 31, args.l, out=bout, stats=True)
-        return [r.numel() for r in res], st
+        lens, n, launches = [], 0, 0
+        for ch in chunks:
+            res, st = comp.compact_batch([texts[j] for j in ch], 31, args.l, out=bout, stats=True)
+            lens += [r.numel() for r in res]
+            n += int(st["n_kmers"])
+            launches += int(st["launches"])
+        return lens, n, launches
 
     for _ in range(2):
         plain_len = plain()
-        batch_len, bst = batched()
+        batch_len, n, launches = batched()
     reps = 2
     torch.cuda.synchronize()
     e0.record(stream)
@@ -258,12 +265,13 @@ def measure_batched(args, comp):
     e1.record(stream)
     torch.cuda.synchronize()
     batch_ms = e0.elapsed_time(e1) / reps
-    n = int(bst["n_kmers"])
-    del texts, one, bout
+    comp.close()
+    del texts, one, bout, comp
     torch.cuda.empty_cache()
     return {"workload": f"{args.batch_jobs} jobs: log-normal length (median 3 Mbp, 0.5-8 Mbp), GC 30-70%, "
-                        f"0.2% SNPs, k=31, device-resident", "jobs": args.batch_jobs, "n_kmers": n,
-            "batched": {"value": n / (batch_ms / 1e3), "ms": batch_ms, "launches": int(bst["launches"])},
+                        f"0.2% SNPs, k=31, device-resident; batched {C} jobs per launch sequence",
+            "jobs": args.batch_jobs, "n_kmers": n,
+            "batched": {"value": n / (batch_ms / 1e3), "ms": batch_ms, "launches": launches},
             "plain": {"value": n / (plain_ms / 1e3), "ms": plain_ms},
             "speedup": plain_ms / batch_ms, "out_bytes_equal": plain_len == batch_len, "unit": UNIT}
 
@@ -363,6 +371,7 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--tune-sample", type=float, default=2e8, help="genome length the autotuner times")
     ap.add_argument("--batch-jobs", type=int, default=256, help="jobs of the batched-vs-plain comparison (0: skip)")
+    ap.add_argument("--batch-chunk", type=int, default=64, help="jobs per batched launch sequence")
     ap.add_argument("--serve-jobs", type=int, default=400, help="arrivals of the serving measurement (0: skip)")
     ap.add_argument("--serve-pool", type=int, default=24, help="distinct jobs the arrivals draw from")
     args = ap.parse_args()
@@ -480,10 +489,10 @@ def main():
     text = out = None
     torch.cuda.empty_cache()
 
-    batched = measure_batched(args, comp) if args.batch_jobs > 0 else None
     comp.close()
     del comp
     torch.cuda.empty_cache()
+    batched = measure_batched(args, local) if args.batch_jobs > 0 else None
     serving = measure_serving(args, local) if args.serve_jobs > 0 else None
 
     cpu = None

@@ -165,6 +165,44 @@ __host__ __device__ __forceinline__ uint32_t bucket_of(uint32_t pr, uint32_t bit
   return bits ? (h >> (32u - bits)) : 0u;
 }
 
+// ASCII of the 4 codes in the low 8 bits of c (first char in the low byte):
+// spread the 2-bit codes into nibbles, then select bytes of "ACGT".
+__device__ __forceinline__ uint32_t ascii4(uint32_t c) {
+  uint32_t x = (c | (c << 4)) & 0x0F0Fu;
+  x = (x | (x << 2)) & 0x3333u;
+  return __byte_perm(0x54474341u, 0u, x);
+}
+
+// codes of chars ch..ch+3 of a packed key in the low 8 bits (chars past the
+// key read as 0)
+template <int NW>
+__device__ __forceinline__ uint32_t codes4(const Key<NW>& x, int ch) {
+  if constexpr (NW == 1) {
+    return uint32_t(x.w[0] >> (2 * ch)) & 0xFFu;
+  } else {
+    const uint64_t v = (ch < 32) ? ((x.w[0] >> (2 * ch)) | (ch > 0 ? (x.w[1] << (64 - 2 * ch)) : 0ull))
+                                 : (x.w[1] >> (2 * (ch - 32)));
+    return uint32_t(v) & 0xFFu;
+  }
+}
+
+// Write the k chars of a packed key at dst (any alignment): aligned 32-bit
+// stores for the middle, byte stores for the ragged ends.
+template <int NW>
+__device__ __forceinline__ void spell_key(char* dst, const Key<NW>& x, int k) {
+  int ch = int((4u - uint32_t(reinterpret_cast<uintptr_t>(dst) & 3u)) & 3u);
+  if (ch > k) ch = k;
+  if (ch) {
+    const uint32_t a = ascii4(codes4(x, 0));
+    for (int i = 0; i < ch; ++i) dst[i] = char(a >> (8 * i));
+  }
+  for (; ch + 4 <= k; ch += 4) *reinterpret_cast<uint32_t*>(dst + ch) = ascii4(codes4(x, ch));
+  if (ch < k) {
+    const uint32_t a = ascii4(codes4(x, ch));
+    for (int i = 0; ch + i < k; ++i) dst[ch + i] = char(a >> (8 * i));
+  }
+}
+
 // reverse the order of the 2-bit groups of a 64-bit word
 __device__ __forceinline__ uint64_t rev2(uint64_t x) {
   x = __brevll(x);

@@ -1032,7 +1032,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     const Key<NW> x = skey(m, i);
     char* dst = (sid == NONE_I) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
     if (r == 0) {
-      for (int ch = 0; ch < k; ++ch) dst[ch] = acgt(key_char(x, ch));
+      spell_key<NW>(dst, x, k);
     } else {
       dst[k - 1 + r] = acgt(key_char(x, k - 1));
     }
@@ -1663,7 +1663,7 @@ __global__ void k_spell(const uint64_t* __restrict__ keys, const uint32_t* __res
     const uint32_t h = head[v], r = rank[v];
     char* dst = out + loff[h];
     if (r == 0) {
-      for (int c = 0; c < k; ++c) dst[c] = acgt(key_char(x, c));
+      spell_key<NW>(dst, x, k);
     } else {
       dst[k - 1 + r] = acgt(key_char(x, k - 1));
     }
