@@ -466,7 +466,7 @@ __global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Co
 // every block taking the next chunk from a shared counter, and places each
 // record with its bucket's cursor.  All blocks therefore write into the same
 // one or two partitions at any time.
-constexpr int SC_CHUNK = 1024;   // k-mers per level-1 block pass (<= 2048 copies)
+constexpr int SC_CHUNK = 2048;   // k-mers per level-1 block pass (<= 4096 copies)
 constexpr int SC_FINE = 4096;    // staged records per level-2 work item
 
 __global__ void k_coarse_init(const unsigned long long* __restrict__ boff, uint32_t fb, uint32_t mc,
