@@ -118,9 +118,9 @@ def whole_path_bytes(st: dict, text_bytes: int, k: int) -> int:
 
 
 def traffic_per_copy(kernel: str):
-    """DRAM bytes per copy of a tile kernel from the committed ncu summary
-    (profiles/traffic.txt: kernel, bytes per copy, the capture it came
-    from), or None."""
+    """DRAM bytes per bucketed copy of the tile kernels from the committed
+    ncu capture (profiles/traffic.txt), or None.  Scaled by the run's copy
+    count it is the traffic of one launch pair at the bench's size."""
     p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
@@ -461,7 +461,7 @@ def main():
     alg = algorithmic_bytes(st, text_bytes, args.k)
     tile_ms = kern["tile_warp"] + kern["tile_block"]
     achieved = alg["tiles"] / (tile_ms / 1e3) / 1e9
-    tpc = traffic_per_copy("k_tile_warp")
+    tpc = traffic_per_copy("tiles")
     whole = whole_path_bytes(st, text_bytes, args.k) / (ms / 1e3) / 1e9
 
     # e2e: host text -> host lines through the C ABI
