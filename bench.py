@@ -213,6 +213,23 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def replica_totals(ms: float, n: int, dist=None, device: str = "cuda"):
+    """Whole-job figures over independent replicas (one job per rank, no
+    data-path collective): the step time is the slowest rank's, the value
+    the k-mers of all ranks over that time.  Every rank takes the same two
+    collectives and a barrier."""
+    if dist is None:
+        return ms, n / (ms / 1e3)
+    import torch
+    t = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    c = torch.tensor([n], dtype=torch.float64, device=device)
+    dist.all_reduce(c, op=dist.ReduceOp.SUM)
+    dist.barrier()
+    ms_max = float(t.item())
+    return ms_max, float(c.item()) / (ms_max / 1e3)
+
+
 def measure_batched(args, device: int):
     """Many small jobs (log-normal lengths, median 3 Mbp, 0.5-8 Mbp, GC
     30-70%, 0.2% SNPs, k=31), device-resident: batched launches of
@@ -442,17 +459,11 @@ def main():
                 kern[p] += st["ms_" + p]
         ev1.record(stream)
         torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
+    ms, value = replica_totals(ev0.elapsed_time(ev1) / args.steps, n, dist, "cuda")
     for p in phase:
         phase[p] /= args.steps
     for p in kern:
         kern[p] /= args.steps
-    value = world * n / (ms / 1e3)
 
     # roofline of the dominant kernels: the two tile kernels (warp tiles and
     # block tiles), timed by CUDA events on the library's stream around their
