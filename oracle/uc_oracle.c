@@ -87,12 +87,13 @@ int orc_parse(const char *text, size_t bytes, int k, uint32_t *words,
 /* ------------------------------------------------------------- minimizers */
 
 /* Seeded bijection of [0, 4^l) standing in for the reference's random l-mer
- * permutation (generate_permutation, driver.cpp:356-402): xor, odd multiplier
- * and addition modulo 4^l. */
+ * permutation (generate_permutation, driver.cpp:356-402): an odd multiplier
+ * and an addend drawn from the seed, modulo 4^l. */
 uint32_t orc_lmer_priority(uint32_t x, int l, uint64_t seed) {
     const uint32_t b = 2u * (uint32_t)l;
     const uint32_t mask = (b >= 32u) ? 0xFFFFFFFFu : ((1u << b) - 1u);
-    return ((x ^ (uint32_t)seed) * 0x9E3779B1u + (uint32_t)(seed >> 32)) & mask;
+    const uint32_t mult = (0x9E3779B1u ^ ((uint32_t)seed << 1)) | 1u;
+    return (x * mult + (uint32_t)(seed >> 32)) & mask;
 }
 
 static inline uint32_t get_char(const uint32_t *w, int x) {

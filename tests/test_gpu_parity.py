@@ -86,7 +86,8 @@ def test_fused_matches_oracle(comp, oracle, texts, cfg):
 
 @pytest.mark.parametrize("cap,bits,wcap,lf", [(256, 0, 0, 0), (256, 4, 0, 150), (1024, 12, 0, 0), (2048, 8, 1, 400),
                                               (8192, 9, 1, 0), (4096, 0, 64, 800), (4096, 14, 32, 0),
-                                              (4096, 0, 1024, 150), (1024, 0, 512, 300)])
+                                              (4096, 0, 1024, 150), (1024, 0, 512, 300),
+                                              (4096, 1, 0, 0)])  # 2 buckets of 300k copies: 16-bit counts wrap
 def test_fused_independent_of_tiling(comp, oracle, texts, cap, bits, wcap, lf):
     """Same lines whatever the bucketing, the hash load factor and whichever
     tier (warp tiles, block tiles, oversized tiles in global scratch) works

@@ -144,12 +144,16 @@ __device__ __forceinline__ char acgt(uint32_t c) {
 
 // Seeded bijection of [0, 4^l): the l-mer priority.  The reference draws a
 // random permutation of the 4^l l-mers (generate_permutation,
-// driver.cpp:356-402); any permutation gives the same unitigs.  An xor, an odd
-// multiplier and an addition modulo 4^l are each invertible.
+// driver.cpp:356-402); any permutation gives the same unitigs.  Multiplying
+// by an odd number and adding are each invertible modulo 4^l; both come from
+// the seed.
+__host__ __device__ __forceinline__ uint32_t lmer_mult(uint64_t seed) {
+  return (0x9E3779B1u ^ (static_cast<uint32_t>(seed) << 1)) | 1u;
+}
 __host__ __device__ __forceinline__ uint32_t lmer_priority(uint32_t x, int l, uint64_t seed) {
   const uint32_t b = 2u * static_cast<uint32_t>(l);
   const uint32_t mask = (b >= 32u) ? 0xFFFFFFFFu : ((1u << b) - 1u);
-  return ((x ^ static_cast<uint32_t>(seed)) * 0x9E3779B1u + static_cast<uint32_t>(seed >> 32)) & mask;
+  return (x * lmer_mult(seed) + static_cast<uint32_t>(seed >> 32)) & mask;
 }
 
 // Bucket of a minimizer priority.  Any function of the minimizer keeps every
@@ -213,6 +217,11 @@ __device__ __forceinline__ uint64_t rev2(uint64_t x) {
 // (get_double_lmin, lmin_buckets.h:67-94): l-mer ids are big-endian (first
 // char in the top bits); l1 covers the l-mers inside chars [0, k-1), l2 the
 // ones inside chars [1, k).  Requires 1 <= l <= min(16, k-1).
+//
+// Without a table the priority is computed in the top 2l bits of a 32-bit
+// word: (id * m + a) << (32 - 2l) equals id * (m << (32 - 2l)) + (a << ...)
+// modulo 2^32, and chars left of the l-mer in the id's upper bits drop out of
+// that product, so each l-mer costs one shift, one multiply-add and one min.
 template <int NW>
 __device__ __forceinline__ void lmins(const Key<NW>& key, int k, int l, uint64_t seed,
                                       const uint32_t* __restrict__ table, uint32_t& l1,
@@ -226,8 +235,36 @@ __device__ __forceinline__ void lmins(const Key<NW>& key, int k, int l, uint64_t
     lo = rev2(key.w[1] & ~ROLE_MASK);
   }
   const int w = k - l + 1;  // l-mers in the k-mer (>= 2)
+  if (table == nullptr) {
+    const uint32_t ps = 32u - 2u * uint32_t(l);
+    const uint32_t m = lmer_mult(seed) << ps, a = static_cast<uint32_t>(seed >> 32) << ps;
+    uint32_t first, mid = 0xFFFFFFFFu, last;
+    if constexpr (NW == 1) {
+      // l-mer p sits in bits [64 - 2p - 2l, 64 - 2p) of hi
+      int s = 64 - 2 * l;
+      first = static_cast<uint32_t>(hi >> s) * m + a;
+      for (int p = 1; p < w - 1; ++p) {
+        s -= 2;
+        mid = min(mid, static_cast<uint32_t>(hi >> s) * m + a);
+      }
+      last = static_cast<uint32_t>(hi >> (s - 2)) * m + a;
+    } else {
+      const int s = 64 - 2 * l;
+      first = static_cast<uint32_t>(hi >> s) * m + a;
+      for (int p = 1; p < w - 1; ++p) {
+        hi = (hi << 2) | (lo >> 62);
+        lo <<= 2;
+        mid = min(mid, static_cast<uint32_t>(hi >> s) * m + a);
+      }
+      hi = (hi << 2) | (lo >> 62);
+      last = static_cast<uint32_t>(hi >> s) * m + a;
+    }
+    l1 = min(first, mid) >> ps;
+    l2 = min(mid, last) >> ps;
+    return;
+  }
   const int sh = 64 - 2 * l;
-  auto pri = [&](uint32_t id) { return table ? __ldg(table + id) : lmer_priority(id, l, seed); };
+  auto pri = [&](uint32_t id) { return __ldg(table + id); };
   const uint32_t first = pri(static_cast<uint32_t>(hi >> sh));
   uint32_t mid = NONE;
   for (int p = 1; p < w - 1; ++p) {

@@ -25,6 +25,7 @@ struct Counters {
   uint32_t work_next;                // level-2 scatter work counter
   uint32_t nwarp, nblock;            // tiles per tier
   uint32_t wtile_next;
+  uint32_t count_ovf;                // a 16-bit bucket count wrapped in k_pack
 };
 
 // One job of a batch (a single call is a batch of one).  Its k-mers occupy

@@ -140,6 +140,30 @@ __device__ __forceinline__ uint32_t job_of_block(const JobTab* __restrict__ jobs
   return lo;
 }
 
+// Bucket counts while packing are 16-bit halves of 32-bit words, so that
+// 2^25 buckets take 64 MiB and the count atomics stay in L2; a half that
+// wraps raises *ovf, and the counts are then taken again at 32 bits
+// (k_count_buckets).  k_widen16 turns them into 32-bit counts.
+__device__ __forceinline__ void count16(uint32_t* c16, uint32_t b, uint32_t* ovf) {
+  const uint32_t sh = (b & 1u) * 16u;
+  const uint32_t old = atomicAdd(c16 + (b >> 1), 1u << sh);
+  if (((old >> sh) & 0xFFFFu) == 0xFFFFu) atomicOr(ovf, 1u);
+}
+
+__global__ void k_widen16(const uint32_t* __restrict__ c16, uint64_t M, uint32_t* __restrict__ counts) {
+  for (uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < M; b += uint64_t(gridDim.x) * blockDim.x)
+    counts[b] = (c16[b >> 1] >> ((b & 1u) * 16u)) & 0xFFFFu;
+}
+
+__global__ void k_count_buckets(const uint32_t* __restrict__ b1, const uint32_t* __restrict__ b2, uint64_t n,
+                                uint32_t* __restrict__ counts) {
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t a = b1[i], b = b2[i];
+    atomicAdd(counts + a, 1u);
+    if (a != b) atomicAdd(counts + b, 1u);
+  }
+}
+
 // MULTI: the block's job comes from the job table (batches); otherwise the
 // one job is a kernel parameter, read from the constant bank.
 template <int NW, bool FUSE, bool MULTI>
@@ -148,7 +172,8 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
                                               const unsigned long long* __restrict__ starts, int k,
                                               uint64_t* __restrict__ keys, uint32_t* err, int l, uint64_t seed,
                                               uint32_t jb, uint32_t* __restrict__ b1, uint32_t* __restrict__ b2,
-                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ jcross) {
+                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ jcross,
+                                              uint32_t* ovf) {
   __shared__ uint32_t buf[PACK_WORDS];
   __shared__ uint32_t s_cross;
   uint32_t bad = 0;
@@ -208,9 +233,46 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
       for (int w = 0; w < NW; ++w) key.w[w] = 0;
       bool lbad = false;
       const bool check_term = !starts && line + 1 < n;
+      bool fast = false;
       if (staged) {
         const uint32_t off = uint32_t((tb + s) - A0);     // line start in the staged span
         const uint32_t lim = uint32_t((tb + s1) - A0);    // end of the staged lines
+        lbad |= (off + uint32_t(k) > lim);
+        const uint32_t sh = 8u * (off & 3u);
+        const uint32_t base = off & ~3u;
+        // fast form: codes of 4 bytes in 3 operations, then one check that
+        // every byte is the letter its code spells ("ACGT"[code]); a line
+        // with any other byte among its k chars (a non-ACGT letter or a line
+        // break) is packed again by the exact form below
+        {
+          uint32_t cur = buf[pad_word(base)];
+          uint32_t mism = 0;
+          const int nfull = k / 4;
+#pragma unroll 4
+          for (int jw = 0; jw <= nfull; ++jw) {
+            const uint32_t nxt = buf[pad_word(base + 4u * (jw + 1))];
+            const uint32_t x = __funnelshift_r(cur, nxt, sh);
+            cur = nxt;
+            const int c0 = 4 * jw;
+            // the last word holds k % 4 chars and the line break
+            const uint32_t inmask = (jw < nfull) ? 0xFFFFFFFFu : ((1u << (8 * (k - c0))) - 1u);
+            const uint32_t g = gather_codes(((x >> 1) ^ (x >> 2)) & 0x03030303u);
+            mism |= (ascii4(g) ^ x) & inmask;
+            if (check_term && jw == nfull) lbad |= ((x >> (8 * (k - c0))) & 0xFFu) != '\n';
+            // codes past char k-1 fall under kmask_hi below; a word never
+            // straddles the two key words (32 is a multiple of 4)
+            const uint64_t gc = uint64_t(g);
+            if (NW == 1 || c0 < 32) key.w[0] |= gc << (2 * c0);
+            else key.w[NW - 1] |= gc << (2 * (c0 - 32));
+          }
+          fast = (mism == 0);
+        }
+      }
+      if (staged && !fast) {
+#pragma unroll
+        for (int w = 0; w < NW; ++w) key.w[w] = 0;
+        const uint32_t off = uint32_t((tb + s) - A0);
+        const uint32_t lim = uint32_t((tb + s1) - A0);
         lbad |= (off + uint32_t(k) > lim);
         const uint32_t sh = 8u * (off & 3u);
         const uint32_t base = off & ~3u;
@@ -234,7 +296,7 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
           if (NW == 1 || c0 < 32) key.w[0] |= gc << (2 * c0);
           else key.w[NW - 1] |= gc << (2 * (c0 - 32));
         }
-      } else {
+      } else if (!staged) {
         for (int c = 0; c <= k; ++c) {
           const uint64_t pos = s + c;
           const uint32_t ch = (pos < end) ? uint32_t(__ldg(text + pos)) : uint32_t('\n');
@@ -259,9 +321,9 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
         b = jp | bucket_of(b, jb);
         b1[koff + line] = a;
         b2[koff + line] = b;
-        atomicAdd(counts + a, 1u);
+        count16(counts, a, ovf);
         if (a != b) {
-          atomicAdd(counts + b, 1u);
+          count16(counts, b, ovf);
           mycross = 1;
         }
       }
@@ -1801,7 +1863,8 @@ struct FuseArgs {
   int l = 0;
   uint64_t seed = 0;
   uint32_t jb = 0;
-  uint32_t *b1 = nullptr, *b2 = nullptr, *counts = nullptr, *jcross = nullptr;
+  uint32_t *b1 = nullptr, *b2 = nullptr, *jcross = nullptr;
+  uint32_t* counts = nullptr;  // 16-bit counts, two per word ((M + 1) / 2 words)
   uint64_t M = 0;
 };
 
@@ -1830,17 +1893,17 @@ static void launch_pack(Env& e, const JobTab* jobs, const JobTab* one, uint32_t 
   if (fz && one)
     k_pack<NW, true, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
                                                         fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
-                                                        fz->jcross);
+                                                        fz->jcross, &e.ctr->count_ovf);
   else if (fz)
     k_pack<NW, true, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
                                                        fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
-                                                       fz->jcross);
+                                                       fz->jcross, &e.ctr->count_ovf);
   else if (one)
     k_pack<NW, false, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
-                                                         0, 0, nullptr, nullptr, nullptr, nullptr);
+                                                         0, 0, nullptr, nullptr, nullptr, nullptr, nullptr);
   else
     k_pack<NW, false, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
-                                                        0, 0, nullptr, nullptr, nullptr, nullptr);
+                                                        0, 0, nullptr, nullptr, nullptr, nullptr, nullptr);
 }
 
 // Grow-only device buffers for the job table and the per-job counters.
@@ -1905,7 +1968,7 @@ static int pack_single(Env& e, const char* d_text, size_t bytes, int k, uint64_t
       fixed = false;
       UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
       if (fz) {
-        UC_CK(cudaMemsetAsync(fz->counts, 0, fz->M * 4, e.stream));
+        UC_CK(cudaMemsetAsync(fz->counts, 0, (fz->M + 1) / 2 * 4, e.stream));
         UC_CK(cudaMemsetAsync(fz->jcross, 0, 4, e.stream));
       }
     } else if (e.h_ctr->err) {
@@ -2055,7 +2118,7 @@ static Plan plan_buckets(const Env& e, uint64_t nmax, uint32_t njobs, int k, int
 
 struct Front {
   uint64_t* keys;
-  uint32_t *b1, *b2, *counts;
+  uint32_t *b1, *b2, *counts, *c16;
   unsigned long long *boff, *cursor, *fcur, *tile_begin, *scan_tmp;
   uint32_t *flag, *fidx, *big_list, *wlist, *blist, *tile_job;
   unsigned long long* big_size;
@@ -2068,6 +2131,7 @@ static size_t front_bytes(uint64_t n, int nw, uint64_t M, bool own_keys) {
   add(n * 4); add(n * 4); add(M * 4); add((M + 1) * 8); add(M * 8); add(M * 8); add((M + 2) * 8);
   add(scan_tmp_elems(M) * 8); add(M * 4); add((M + 1) * 4); add(M * 4); add(M * 8);
   add(M * 4); add(M * 4); add(M * 4);
+  add((M + 1) / 2 * 4);
   return need;
 }
 
@@ -2088,7 +2152,8 @@ static int take_front(Env& e, uint64_t n, int nw, uint64_t M, bool own_keys, Fro
   f.wlist = static_cast<uint32_t*>(e.take(0, M * 4));
   f.blist = static_cast<uint32_t*>(e.take(0, M * 4));
   f.tile_job = static_cast<uint32_t*>(e.take(0, M * 4));
-  if (!f.tile_job) return e.fail(UC_EBUDGET, "front arena overflow");
+  f.c16 = static_cast<uint32_t*>(e.take(0, (M + 1) / 2 * 4));
+  if (!f.c16) return e.fail(UC_EBUDGET, "front arena overflow");
   return UC_OK;
 }
 
@@ -2720,7 +2785,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   r = take_front(e, N, nw, P.M, true, f);
   if (r) return r;
   UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
-  UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
+  UC_CK(cudaMemsetAsync(f.c16, 0, (P.M + 1) / 2 * 4, e.stream));
   UC_CK(cudaMemsetAsync(jd.jcross, 0, njobs * 4, e.stream));
   UC_CK(cudaMemcpyAsync(jd.tab, J.data(), njobs * sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
   cudaEventRecord(e.ev[0], e.stream);
@@ -2730,7 +2795,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   fz.jb = P.jb;
   fz.b1 = f.b1;
   fz.b2 = f.b2;
-  fz.counts = f.counts;
+  fz.counts = f.c16;
   fz.jcross = jd.jcross;
   fz.M = P.M;
   if (njobs == 1) {
@@ -2742,6 +2807,8 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     UC_CK(cudaGetLastError());
   }
   cudaEventRecord(e.ev[1], e.stream);
+  ++e.launches;
+  k_widen16<<<grid_for(e, P.M, 256), 256, 0, e.stream>>>(f.c16, P.M, f.counts);
   uint64_t copies = 0;
   r = bucket_offsets(e, f, P.M, copies);
   if (r) return r;
@@ -2749,6 +2816,14 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   UC_CK(cudaMemcpyAsync(xc.data(), jd.jcross, njobs * 4, cudaMemcpyDeviceToHost, e.stream));
   r = e.read_ctr();
   if (r) return r;
+  if (e.h_ctr->count_ovf && !e.h_ctr->err) {
+    // a bucket holds 65536 copies or more: count again at 32 bits
+    UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
+    e.launches += 1;
+    k_count_buckets<<<grid_for(e, N, 256), 256, 0, e.stream>>>(f.b1, f.b2, N, f.counts);
+    r = bucket_offsets(e, f, P.M, copies);
+    if (r) return r;
+  }
   if (e.h_ctr->err) {
     if (e.h_ctr->err & ERR_LAYOUT) return e.fail(UC_EINPUT, "a k-mer line is shorter than k");
     return e.check_err(e.h_ctr);
