@@ -118,14 +118,13 @@ __device__ __forceinline__ bool key_lt(const Key<NW>& a, const Key<NW>& b) {
   }
 }
 
+// Slot hash of a (k-1)-mer for the tile tables (at most 2^15 slots): the
+// high half of a multiplicative (Fibonacci) hash, which every key bit reaches.
 template <int NW>
 __device__ __forceinline__ uint32_t key_hash(const Key<NW>& p) {
   uint64_t h = p.w[0] * 0x9E3779B97F4A7C15ull;
-  if constexpr (NW == 2) h ^= p.w[1] * 0xC2B2AE3D27D4EB4Full;
-  h ^= h >> 29;
-  h *= 0xBF58476D1CE4E5B9ull;
-  h ^= h >> 32;
-  return static_cast<uint32_t>(h);
+  if constexpr (NW == 2) h += p.w[1] * 0xC2B2AE3D27D4EB4Full;
+  return static_cast<uint32_t>(h >> 32);
 }
 
 // 2-bit code of char x of a packed key

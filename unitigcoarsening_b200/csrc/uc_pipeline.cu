@@ -1045,10 +1045,11 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   IT* hi_a = (rnk == m.T) ? m.T + c : m.T;
   // ---- emission: closed segments (start has role P, end has role S) are
   // whole unitigs; the others are stitched across tiles
-  const uint32_t chunk = (c + G::size() - 1) / G::size();
-  const uint32_t lo = min(c, G::rank() * chunk), hi = min(c, lo + chunk);
+  // each thread takes copies rank, rank + size, ...: its lines are
+  // contiguous in the tile's output, in that order (the order of lines is
+  // free), and neighbouring threads read neighbouring shared words
   U3 mine{0, 0, 0};
-  for (uint32_t i = lo; i < hi; ++i) {
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     if (m.A[i] != NONE_I) continue;
     const uint32_t s = ptr[i];
     const uint32_t len = uint32_t(rnk[i]) + 1;
@@ -1061,7 +1062,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   unsigned long long s_base[3];
   if (!G::reserve(p, job, tot, s_base)) return;
   const unsigned long long cbase = s_base[0], obase = s_base[1], sbase = s_base[2];
-  for (uint32_t i = lo; i < hi; ++i) {
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
     if (m.A[i] != NONE_I) continue;
     const uint32_t s = ptr[i];
     const uint32_t len = uint32_t(rnk[i]) + 1;
@@ -1181,27 +1182,6 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
 // both hold x, so every later segment drops its first k chars
 // (write_unitigs4, compact.h:59-112).
 // Segment ids come from per-job pools; an unused id has length 0.
-__global__ void k_seg_link(uint32_t S, const uint32_t* __restrict__ seg_sx,
-                           const uint32_t* __restrict__ seg_ex, const uint32_t* __restrict__ seg_len,
-                           const uint32_t* __restrict__ start_seg, const uint32_t* __restrict__ end_seg,
-                           uint32_t* __restrict__ next, uint32_t* __restrict__ prev,
-                           uint32_t* __restrict__ w, int k) {
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
-    if (seg_len[s] == 0) {
-      next[s] = NONE;
-      prev[s] = NONE;
-      w[s] = 0;
-      continue;
-    }
-    const uint32_t ex = seg_ex[s], sx = seg_sx[s];
-    const uint32_t nx = (ex == NONE) ? NONE : start_seg[ex];
-    const uint32_t pv = (sx == NONE) ? NONE : end_seg[sx];
-    next[s] = nx;
-    prev[s] = pv;
-    w[s] = (pv == NONE) ? uint32_t(k) - 1u + seg_len[s] : seg_len[s] - 1u;
-  }
-}
-
 __device__ __forceinline__ unsigned long long pk(uint32_t p, uint32_t o) {
   return (static_cast<unsigned long long>(o) << 32) | p;
 }
@@ -1225,6 +1205,53 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool pred) {
   if (lane == leader) b = atomicAdd(count, uint32_t(__popc(m)));
   b = __shfl_sync(0xFFFFFFFFu, b, leader);
   return pred ? b + uint32_t(__popc(m & ((1u << lane) - 1u))) : NONE;
+}
+
+// Segment links: next/prev through the cross k-mer at each open end, and
+// each segment's weight (the chars it adds to the line).  With X, the list
+// ranking's first state is written too, from the predecessor's side: a
+// segment without a predecessor is a head, and every segment s with a
+// successor t sets X[t] = (s, w[s]) - every cross k-mer joins exactly one
+// segment ending there to one starting there, so each entry is written once.
+// Segments with a predecessor go to the active list.
+__global__ void k_seg_link(uint32_t S, const uint32_t* __restrict__ seg_sx,
+                           const uint32_t* __restrict__ seg_ex, const uint32_t* __restrict__ seg_len,
+                           const uint32_t* __restrict__ start_seg, const uint32_t* __restrict__ end_seg,
+                           uint32_t* __restrict__ next, uint32_t* __restrict__ prev,
+                           uint32_t* __restrict__ w, int k, unsigned long long* __restrict__ X,
+                           uint32_t* __restrict__ act, uint32_t* act_count) {
+  const uint32_t stride = gridDim.x * blockDim.x;
+  // whole warps iterate together (warp_append needs every lane)
+  for (uint32_t s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); s0 < S; s0 += stride) {
+    const uint32_t s = s0 + (threadIdx.x & 31);
+    bool tail = false;
+    if (s < S) {
+      const uint32_t len = seg_len[s];
+      if (len == 0) {  // an unused slot of the segment pool
+        next[s] = NONE;
+        prev[s] = NONE;
+        w[s] = 0;
+        if (X) X[s] = pk(s | HEAD_BIT, 0);
+      } else {
+        const uint32_t ex = seg_ex[s], sx = seg_sx[s];
+        const uint32_t nx = (ex == NONE) ? NONE : start_seg[ex];
+        const uint32_t pv = (sx == NONE) ? NONE : end_seg[sx];
+        const uint32_t ws = (pv == NONE) ? uint32_t(k) - 1u + len : len - 1u;
+        next[s] = nx;
+        prev[s] = pv;
+        w[s] = ws;
+        if (X) {
+          if (pv == NONE) X[s] = pk(s | HEAD_BIT, 0);
+          if (nx != NONE) X[nx] = pk(s, ws);
+          tail = pv != NONE;
+        }
+      }
+    }
+    if (X) {
+      const uint32_t slot = warp_append(act_count, tail);
+      if (tail) act[slot] = s;
+    }
+  }
 }
 
 // X[v] = (start pointer, weight distance); heads point at themselves.
@@ -2432,15 +2459,20 @@ static int run_graph(Env& e, int slot, uint64_t key, F&& body) {
   return UC_OK;
 }
 
+// prefilled: X, act0 and cnt[0] were written by k_seg_link.
 static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t nmax, bool count_on_device,
                       unsigned long long* X, uint32_t* act0, uint32_t* act1, uint32_t* cnt, uint32_t& rounds,
-                      uint32_t*& act_final, uint32_t*& cnt_final) {
+                      uint32_t*& act_final, uint32_t*& cnt_final, bool prefilled = false) {
   rounds = 2;
   for (uint64_t t = 1; t < nmax; t <<= 1) ++rounds;
-  UC_CK(cudaMemsetAsync(cnt, 0, (rounds + 1) * 4, e.stream));
   const int grid = grid_for(e, nmax ? nmax : 1, 256);
-  ++e.launches;
-  k_rank_init<<<grid, 256, 0, e.stream>>>(prev, w, nmax, count_on_device ? e.ctr : nullptr, X, act0, cnt);
+  if (prefilled) {
+    UC_CK(cudaMemsetAsync(cnt + 1, 0, rounds * 4, e.stream));
+  } else {
+    UC_CK(cudaMemsetAsync(cnt, 0, (rounds + 1) * 4, e.stream));
+    ++e.launches;
+    k_rank_init<<<grid, 256, 0, e.stream>>>(prev, w, nmax, count_on_device ? e.ctr : nullptr, X, act0, cnt);
+  }
   uint32_t* lists[2] = {act0, act1};
   for (uint32_t r = 0; r < rounds; ++r) {
     ++e.launches;
@@ -2921,7 +2953,11 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   const uint32_t S = uint32_t(Sp);
   const int gs = grid_for(e, S, 256);
   ++e.launches;
-  k_seg_link<<<gs, 256, 0, e.stream>>>(S, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k);
+  // pointer jumping takes its first state from the link pass
+  const bool link_ranks = !want_hec;
+  if (link_ranks) UC_CK(cudaMemsetAsync(rcnt, 0, 4, e.stream));
+  k_seg_link<<<gs, 256, 0, e.stream>>>(S, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k,
+                                       link_ranks ? Xr : nullptr, act0, rcnt);
   uint32_t *act = nullptr, *left = nullptr;
   bool hec = want_hec;
   if (hec) {
@@ -2949,8 +2985,8 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     uint32_t rr = 2;
     for (uint64_t t = 1; t < S; t <<= 1) ++rr;
     int rl = UC_OK;
-    r = run_graph(e, 0, (uint64_t(rr) << 32) | uint32_t(gs), [&] {
-      rl = rank_lists(e, prev, wgt, S, false, Xr, act0, act1, rcnt, rounds, act, left);
+    r = run_graph(e, 0, (uint64_t(rr) << 33) | (uint64_t(link_ranks) << 32) | uint32_t(gs), [&] {
+      rl = rank_lists(e, prev, wgt, S, false, Xr, act0, act1, rcnt, rounds, act, left, link_ranks);
       cudaMemsetAsync(oncyc, 0, S, e.stream);
       ++e.launches;
       k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
