@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
         const uintptr_t a = A0 + 16u * c;
         uint4 v;
         if (a >= tb && a + 16 <= tb + tbytes) {
-          v = __ldg(reinterpret_cast<const uint4*>(a));
+          v = __ldcs(reinterpret_cast<const uint4*>(a));  // read once: evict first
         } else {
           uint32_t w[4] = {0x0A0A0A0Au, 0x0A0A0A0Au, 0x0A0A0A0Au, 0x0A0A0A0Au};
           for (int q = 0; q < 16; ++q) {
@@ -312,15 +312,19 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
       }
       key.w[NW - 1] &= kmask_hi;
       if (lbad) bad = 1;
-      st_key<NW>(keys, koff + line, key);
+      // keys and bucket ids stream out with evict-first stores, so that the
+      // text and them do not push the bucket counts out of L2
+      if constexpr (NW == 1) __stcs(reinterpret_cast<unsigned long long*>(keys) + koff + line,
+                                    static_cast<unsigned long long>(key.w[0]));
+      else st_key<NW>(keys, koff + line, key);
       if constexpr (FUSE) {
         uint32_t a, b;
         lmins<NW>(key, k, l, seed, nullptr, a, b);
         const uint32_t jp = j << jb;
         a = jp | bucket_of(a, jb);
         b = jp | bucket_of(b, jb);
-        b1[koff + line] = a;
-        b2[koff + line] = b;
+        __stcs(b1 + koff + line, a);
+        __stcs(b2 + koff + line, b);
         count16(counts, a, ovf);
         if (a != b) {
           count16(counts, b, ovf);
