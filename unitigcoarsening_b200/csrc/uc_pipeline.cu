@@ -560,13 +560,29 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
   const int lane = threadIdx.x & 31;
   for (uint64_t c0 = uint64_t(blockIdx.x) * SC_CHUNK; c0 < n; c0 += uint64_t(gridDim.x) * SC_CHUNK) {
     const uint32_t cn = uint32_t((n - c0) < uint64_t(SC_CHUNK) ? (n - c0) : uint64_t(SC_CHUNK));
+    // every load of the chunk is issued at once; the values stay in registers
+    constexpr int PT = SC_CHUNK / 256;
+    Key<NW> kk[PT];
+    uint32_t aa[PT], bb[PT];
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const uint32_t t = uint32_t(q) * 256u + threadIdx.x;
+      if (t < cn) {
+        kk[q] = ld_key<NW>(keys, c0 + t);
+        aa[q] = b1[c0 + t];
+        bb[q] = b2[c0 + t];
+      }
+    }
     for (uint32_t j = threadIdx.x; j < mc; j += blockDim.x) hist[j] = 0;
     __syncthreads();
     // count copies per coarse partition
-    for (uint32_t t = threadIdx.x; t < cn; t += blockDim.x) {
-      const uint32_t a = b1[c0 + t], b = b2[c0 + t];
-      atomicAdd(hist + (a >> fb), 1u);
-      if (a != b) atomicAdd(hist + (b >> fb), 1u);
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const uint32_t t = uint32_t(q) * 256u + threadIdx.x;
+      if (t < cn) {
+        atomicAdd(hist + (aa[q] >> fb), 1u);
+        if (aa[q] != bb[q]) atomicAdd(hist + (bb[q] >> fb), 1u);
+      }
     }
     __syncthreads();
     // local offsets (scan over the partitions) and global reservations
@@ -588,15 +604,18 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
     }
     __syncthreads();
     // place every copy in its partition's run of the staging area
-    for (uint32_t t0 = 0; t0 < cn; t0 += blockDim.x) {
-      const uint32_t t = t0 + threadIdx.x;
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const uint32_t t = uint32_t(q) * 256u + threadIdx.x;
       const bool live = t < cn;
       uint32_t a = 0, b = 0;
       Key<NW> key;
+#pragma unroll
+      for (int w = 0; w < NW; ++w) key.w[w] = 0;
       if (live) {
-        key = ld_key<NW>(keys, c0 + t);
-        a = b1[c0 + t];
-        b = b2[c0 + t];
+        key = kk[q];
+        a = aa[q];
+        b = bb[q];
       }
       const bool cross = live && (a != b);
       uint32_t x = NONE;
