@@ -74,6 +74,13 @@ uc_status uc_ctx_create(int device, size_t hbm_budget, uc_ctx **out);
 uc_status uc_ctx_destroy(uc_ctx *ctx);
 uc_status uc_ctx_set_stream(uc_ctx *ctx, void *cuda_stream);
 uc_status uc_ctx_sync(uc_ctx *ctx);
+/* Deterministic output: with on != 0, uc_compact_device, uc_compact_host,
+ * uc_job_* and uc_compact_file leave the lines in byte order, so equal input
+ * gives byte-equal output.  The reference appends lines in an order that
+ * varies from run to run (compact.h:7-37); sorting costs one radix sort of
+ * the lines by their first k-mer and one copy of the output.  Batches
+ * (uc_compact_batch) are not reordered. */
+uc_status uc_ctx_set_sorted_output(uc_ctx *ctx, int on);
 uc_status uc_ctx_set_tuning(uc_ctx *ctx, const uc_tuning *t);
 uc_status uc_ctx_get_tuning(const uc_ctx *ctx, uc_tuning *t);
 const char *uc_last_error(const uc_ctx *ctx);

@@ -183,6 +183,37 @@ def test_host_path_and_file(comp, oracle, texts, tmp_path):
     assert sorted_lines(data) == sorted(sorted_lines(want) * 2)
 
 
+@pytest.mark.parametrize("cfg", ["small_plain", "wide_k63", "k47", "k15", "scale_sample"])
+def test_sorted_output_is_byte_exact(comp, oracle, texts, cfg):
+    """Sorted output: the whole output equals the oracle's lines in byte
+    order, byte for byte, on repeated calls and on the host path."""
+    text, k = texts[cfg]
+    want, _, _ = oracle.compact(text, k)
+    expect = b"".join(x + b"\n" for x in sorted_lines(want))
+    comp.set_sorted_output(True)
+    try:
+        a = comp.compact(dev(text), k, min(8, k - 1)).cpu().numpy().tobytes()
+        b = comp.compact(dev(text), k, min(8, k - 1)).cpu().numpy().tobytes()
+        h = bytes(comp.compact_host(text, k, min(8, k - 1)).numpy())
+    finally:
+        comp.set_sorted_output(False)
+    assert a == expect
+    assert b == expect and h == expect
+
+
+def test_sorted_output_cli(comp, oracle, texts, tmp_path):
+    import subprocess
+    from unitigcoarsening_b200 import build as B
+    text, k = texts["small_plain"]
+    want, _, _ = oracle.compact(text, k)
+    inp = tmp_path / "in.txt"
+    outp = tmp_path / "out.txt"
+    inp.write_bytes(text)
+    r = subprocess.run([B.CLI, str(inp), str(k), "8", str(outp), "--sorted"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert outp.read_bytes() == b"".join(x + b"\n" for x in sorted_lines(want))
+
+
 def _golden():
     from tests.test_oracle import _checksum_cases, _golden_cases
     return _golden_cases(), _checksum_cases()

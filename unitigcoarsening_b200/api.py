@@ -102,6 +102,7 @@ def lib():
             "uc_ctx_set_stream": ([vp, vp], i),
             "uc_ctx_sync": ([vp], i),
             "uc_ctx_set_tuning": ([vp, ctypes.POINTER(Tuning)], i),
+            "uc_ctx_set_sorted_output": ([vp, i], i),
             "uc_ctx_get_tuning": ([vp, ctypes.POINTER(Tuning)], i),
             "uc_last_error": ([vp], ctypes.c_char_p),
             "uc_status_str": ([i], ctypes.c_char_p),
@@ -199,6 +200,11 @@ class Compactor:
         for k, v in kw.items():
             setattr(t, k, int(v))
         self._check(self._L.uc_ctx_set_tuning(self._h, ctypes.byref(t)))
+
+    def set_sorted_output(self, on: bool = True):
+        """Whole-job calls leave the lines in byte order (deterministic
+        output; uc_ctx_set_sorted_output)."""
+        self._check(self._L.uc_ctx_set_sorted_output(self._h, 1 if on else 0))
 
     def get_tuning(self) -> dict:
         t = Tuning()

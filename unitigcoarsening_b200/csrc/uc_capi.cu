@@ -187,6 +187,12 @@ uc_status uc_ctx_sync(uc_ctx* c) {
   return e == cudaSuccess ? UC_OK : cuda_fail(c, e, "cudaStreamSynchronize");
 }
 
+uc_status uc_ctx_set_sorted_output(uc_ctx* c, int on) {
+  if (!c) return UC_EINPUT;
+  c->env.sorted = on != 0;
+  return UC_OK;
+}
+
 uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
   if (!c || !t) return UC_EINPUT;
   if (t->tile_capacity && (t->tile_capacity < 256 || t->tile_capacity > 8192)) {

@@ -1,6 +1,6 @@
 // uc_main — command-line driver with the reference's interface:
 //
-//   uc_main <k-mer file> k l <output file> [--config <file>] [--device N]
+//   uc_main <k-mer file> k l <output file> [--config <file>] [--device N] [--sorted]
 //
 // (driver.cpp:422-432: exactly four positional arguments, no defaults).  The
 // unitig lines are appended to the output file as the reference does
@@ -8,7 +8,8 @@
 // cond_config.txt, fourpart_config.txt) that none of its code reads; --config
 // accepts them, checks that they parse (seven lines of numbers and a final
 // word), and changes nothing.  Phase times are printed like the reference's
-// timers (driver.cpp:641-657).
+// timers (driver.cpp:641-657).  --sorted writes the lines in byte order, so
+// that equal input gives byte-equal output.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -37,18 +38,21 @@ int main(int argc, char** argv) {
   std::vector<const char*> pos;
   const char* config = nullptr;
   int device = 0;
+  bool sorted = false;
   for (int i = 1; i < argc; ++i) {
     if (!std::strcmp(argv[i], "--config") && i + 1 < argc) {
       config = argv[++i];
     } else if (!std::strcmp(argv[i], "--device") && i + 1 < argc) {
       device = std::atoi(argv[++i]);
+    } else if (!std::strcmp(argv[i], "--sorted")) {
+      sorted = true;
     } else {
       pos.push_back(argv[i]);
     }
   }
   if (pos.size() != 4) {
     std::printf("You input %d args\n", argc);
-    std::fprintf(stderr, "Usage: %s <k-mer file> k l <output file> [--config <file>] [--device N]\n", argv[0]);
+    std::fprintf(stderr, "Usage: %s <k-mer file> k l <output file> [--config <file>] [--device N] [--sorted]\n", argv[0]);
     return EXIT_FAILURE;
   }
   if (config && !check_config(config)) {
@@ -63,6 +67,7 @@ int main(int argc, char** argv) {
     std::fprintf(stderr, "Error: %s\n", uc_status_str(s));
     return EXIT_FAILURE;
   }
+  if (sorted) uc_ctx_set_sorted_output(ctx, 1);
   uc_stats st{};
   s = uc_compact_file(ctx, pos[0], k, l, pos[3], &st);
   if (s != UC_OK) {

@@ -17,6 +17,7 @@
 #include "uc_pipeline.h"
 
 #include <cuda_pipeline.h>
+#include <cub/device/device_radix_sort.cuh>
 
 namespace uc {
 
@@ -3092,9 +3093,153 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
 int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char* out, uint64_t cap,
                    uint64_t& out_bytes, uc_stats* st) {
   uint64_t off = 0, len = 0;
-  const int r = compact_batch(e, 1, &d_text, &bytes, k, l, out, cap, &off, &len, st);
+  int r = compact_batch(e, 1, &d_text, &bytes, k, l, out, cap, &off, &len, st);
   out_bytes = len;
+  if (r == UC_OK && e.sorted && len) r = sort_lines(e, out, len, k);
   return r;
+}
+
+// ============================================================ sorted output
+
+// Each line's first k chars, packed big-endian (first char in the top bits
+// of hi, chars 32.. in lo), so that numeric order is byte order.  Every
+// k-mer begins at most one line, so these keys order the lines completely.
+__global__ void k_line_keys(const char* __restrict__ out, const unsigned long long* __restrict__ starts, uint64_t L,
+                            int k, unsigned long long* __restrict__ khi, unsigned long long* __restrict__ klo,
+                            uint32_t* __restrict__ idx) {
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < L; j += uint64_t(gridDim.x) * blockDim.x) {
+    const char* p = out + starts[j];
+    unsigned long long hi = 0, lo = 0;
+    for (int c = 0; c < k; ++c) {
+      const uint32_t b = uint8_t(p[c]);
+      const unsigned long long code = ((b >> 1) ^ (b >> 2)) & 3u;  // A C G T -> 0 1 2 3
+      if (c < 32) hi |= code << (62 - 2 * c);
+      else lo |= code << (62 - 2 * (c - 32));
+    }
+    khi[j] = hi;
+    klo[j] = lo;
+    idx[j] = uint32_t(j);
+  }
+}
+
+__global__ void k_gather_u64(const unsigned long long* __restrict__ src, const uint32_t* __restrict__ idx,
+                             uint64_t L, unsigned long long* __restrict__ dst) {
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < L; j += uint64_t(gridDim.x) * blockDim.x)
+    dst[j] = src[idx[j]];
+}
+
+__global__ void k_sorted_len(const unsigned long long* __restrict__ starts, const uint32_t* __restrict__ idx,
+                             uint64_t L, uint32_t* __restrict__ len) {
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < L; j += uint64_t(gridDim.x) * blockDim.x) {
+    const uint32_t i = idx[j];
+    len[j] = uint32_t(starts[i + 1] - starts[i]);
+  }
+}
+
+// Lines to their sorted places: a warp resolves 32 lines, then copies them.
+__global__ void k_line_copy(const char* __restrict__ src, const unsigned long long* __restrict__ starts,
+                            const uint32_t* __restrict__ idx, const unsigned long long* __restrict__ dsto,
+                            uint64_t L, char* __restrict__ dst) {
+  const int lane = threadIdx.x & 31;
+  const uint64_t warp = (uint64_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nwarps = (uint64_t(gridDim.x) * blockDim.x) >> 5;
+  for (uint64_t base = warp * 32u; base < L; base += nwarps * 32u) {
+    const uint64_t j = base + uint64_t(lane);
+    uint64_t so = 0, d = 0;
+    uint32_t m = 0;
+    if (j < L) {
+      const uint32_t i = idx[j];
+      so = starts[i];
+      m = uint32_t(starts[i + 1] - so);
+      d = dsto[j];
+    }
+    uint32_t todo = __ballot_sync(0xFFFFFFFFu, j < L);
+    while (todo) {
+      const int q = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const uint64_t a = __shfl_sync(0xFFFFFFFFu, so, q);
+      const uint64_t b = __shfl_sync(0xFFFFFFFFu, d, q);
+      const uint32_t n = __shfl_sync(0xFFFFFFFFu, m, q);
+      for (uint32_t x = lane; x < n; x += 32) dst[b + x] = src[a + x];
+    }
+  }
+}
+
+int sort_lines(Env& e, char* out, uint64_t bytes, int k) {
+  if (bytes == 0) return UC_OK;
+  e.reset();
+  const uint32_t chunk = 1 << 16;
+  const uint64_t nchunks = std::max<uint64_t>(1, (bytes - 1 + chunk - 1) / chunk);
+  // lines end with '\n'; the last one at bytes - 1
+  const uint64_t Lmax = bytes / uint64_t(k + 1) + 1;
+  size_t cub_bytes = 0;
+  cub::DeviceRadixSort::SortPairs(nullptr, cub_bytes, static_cast<const unsigned long long*>(nullptr),
+                                  static_cast<unsigned long long*>(nullptr), static_cast<const uint32_t*>(nullptr),
+                                  static_cast<uint32_t*>(nullptr), int(Lmax), 0, 64, e.stream);
+  size_t need = 0;
+  auto add = [&](size_t b) { need += (b + 255) & ~size_t(255); };
+  add(bytes); add(nchunks * 4); add((nchunks + 1) * 8); add(scan_tmp_elems(nchunks) * 8);
+  add((Lmax + 1) * 8);                         // starts
+  add(Lmax * 8); add(Lmax * 8); add(Lmax * 8); // khi, klo, sorted keys
+  add(Lmax * 4); add(Lmax * 4);                // idx, sorted idx
+  add(Lmax * 4); add((Lmax + 1) * 8); add(scan_tmp_elems(Lmax) * 8);
+  add(cub_bytes);
+  int r = e.reserve(1, need);
+  if (r) return r;
+  char* tmp = static_cast<char*>(e.take(1, bytes));
+  uint32_t* cnt = static_cast<uint32_t*>(e.take(1, nchunks * 4));
+  auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
+  auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(1, c * 4)); };
+  unsigned long long* coff = T64(nchunks + 1);
+  unsigned long long* ctmp = T64(scan_tmp_elems(nchunks));
+  unsigned long long* starts = T64(Lmax + 1);
+  unsigned long long* khi = T64(Lmax);
+  unsigned long long* klo = T64(Lmax);
+  unsigned long long* ks = T64(Lmax);
+  uint32_t* idx = T32(Lmax);
+  uint32_t* idx2 = T32(Lmax);
+  uint32_t* len = T32(Lmax);
+  unsigned long long* dsto = T64(Lmax + 1);
+  unsigned long long* stmp = T64(scan_tmp_elems(Lmax));
+  void* cub_tmp = e.take(1, cub_bytes);
+  if (!cub_tmp) return e.fail(UC_EBUDGET, "arena overflow (sorted output)");
+  const uint8_t* ob = reinterpret_cast<const uint8_t*>(out);
+  e.launches += 1 + 6 + 1;
+  k_count_nl<<<unsigned(nchunks), 256, 0, e.stream>>>(ob, 0, bytes - 1, cnt, chunk);
+  scan_excl<uint32_t, unsigned long long>(cnt, nchunks, coff, ctmp, e.stream);
+  unsigned long long nl = 0;
+  UC_CK(cudaMemcpyAsync(&nl, coff + nchunks, 8, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  const uint64_t L = nl + 1;
+  if (L > Lmax || L >= 0x7FFFFFFFull) return e.fail(UC_EINTERNAL, "line count of the output out of range");
+  k_write_starts<<<unsigned(nchunks), 256, 0, e.stream>>>(ob, 0, bytes - 1, coff, chunk, starts, L);
+  UC_CK(cudaMemcpyAsync(starts + L, &bytes, 8, cudaMemcpyHostToDevice, e.stream));
+  const int g = grid_for(e, L, 256);
+  e.launches += 1;
+  k_line_keys<<<g, 256, 0, e.stream>>>(out, starts, L, k, khi, klo, idx);
+  // least significant part first; radix sort is stable
+  uint32_t* order = idx;
+  if (k > 32) {
+    UC_CK(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_bytes, klo, ks, idx, idx2, int(L), 128 - 2 * k, 64,
+                                          e.stream));
+    ++e.launches;
+    k_gather_u64<<<g, 256, 0, e.stream>>>(khi, idx2, L, klo);
+    UC_CK(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_bytes, klo, ks, idx2, idx, int(L), 0, 64, e.stream));
+    order = idx;
+  } else {
+    UC_CK(cub::DeviceRadixSort::SortPairs(cub_tmp, cub_bytes, khi, ks, idx, idx2, int(L), 64 - 2 * k, 64,
+                                          e.stream));
+    order = idx2;
+  }
+  e.launches += 2 + 6;
+  k_sorted_len<<<g, 256, 0, e.stream>>>(starts, order, L, len);
+  scan_excl<uint32_t, unsigned long long>(len, L, dsto, stmp, e.stream);
+  k_line_copy<<<g, 256, 0, e.stream>>>(out, starts, order, dsto, L, tmp);
+  UC_CK(cudaGetLastError());
+  UC_CK(cudaMemcpyAsync(out, tmp, bytes, cudaMemcpyDeviceToDevice, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  e.reset();
+  return UC_OK;
 }
 
 }  // namespace uc

@@ -49,6 +49,9 @@ struct Env {
   // server owns; they never grow, and oversized-tile scratch comes from the
   // back arena's free end
   bool pool = false;
+  // whole-job calls (compact_device and the paths built on it) leave the
+  // lines in byte order
+  bool sorted = false;
   std::string err;
 
   int fail(int code, const std::string& msg);
@@ -75,6 +78,9 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
 int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t* bytes, int k, int l, char* out,
                   uint64_t out_cap, uint64_t* out_off, uint64_t* out_len, uc_stats* st);
 uint64_t output_bound(size_t text_bytes, int k);
+// Reorder the lines of out[0, bytes) into byte order in place (scratch from
+// the back arena).
+int sort_lines(Env& e, char* out, uint64_t bytes, int k);
 // Upper bound of the front and back arena bytes (reserve slack included)
 // that compact_batch needs for these jobs under the current tuning, from the
 // text sizes alone: every line holds at least k+1 bytes and at most every
