@@ -200,6 +200,20 @@ uint64_t uc_batch_output_bound(int njobs, const size_t *bytes, int k);
 
 /* ---- host-memory jobs ------------------------------------------------- */
 
+/* A sequence of host jobs, each from host memory (text) to host memory
+ * (outs[j], caps[j] bytes; out_lens[j] receives the length), with the
+ * uploads overlapped: job j+1's text goes to the device while job j runs its
+ * bucketing, tiles, stitch and result copy (a job's text is not read after
+ * its pack phase, so one device text buffer serves all).  Equivalent to
+ * uc_compact_host per job.  The reference reads and writes one file per run
+ * (driver.cpp:257-354, compact.h:7-37); with pinned buffers the host link
+ * carries both directions at once.  stats (may be NULL) sums k-mers, output
+ * bytes, device time and launches. */
+uc_status uc_compact_host_many(uc_ctx *ctx, int njobs, const char *const *texts,
+                               const size_t *bytes, int k, int l,
+                               char *const *outs, const size_t *caps,
+                               size_t *out_lens, uc_stats *stats);
+
 /* Submit host text (pageable or pinned); the job copies it to the device,
  * runs the fused path and copies the lines back.  main, driver.cpp:422-662,
  * without the file I/O. */

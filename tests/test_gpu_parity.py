@@ -214,6 +214,25 @@ def test_sorted_output_cli(comp, oracle, texts, tmp_path):
     assert outp.read_bytes() == b"".join(x + b"\n" for x in sorted_lines(want))
 
 
+def test_host_many_overlapped_uploads(comp, oracle, texts):
+    """A sequence of host jobs with the next text uploading during the job
+    before it: each job's lines equal the oracle's and the job alone,
+    including a repeated text and one larger job between smaller ones."""
+    seq = [texts["small_plain"], texts["scale_sample"], texts["batched_job"], texts["small_plain"]]
+    k = 31
+    assert all(kk == k for _, kk in seq)
+    want = [sorted_lines(oracle.compact(t, k)[0]) for t, _ in seq]
+    outs = [torch.empty(comp.output_bound(len(t), k), dtype=torch.uint8) for t, _ in seq]
+    res, st = comp.compact_host_many([t for t, _ in seq], k, 8, outs=outs, stats=True)
+    for r, w in zip(res, want):
+        assert sorted_lines(bytes(r.numpy())) == w
+    assert st["n_kmers"] == sum(int(t[: t.index(b"\n")]) for t, _ in seq)
+    # one shared output buffer for every job: each result is read before the next
+    one = torch.empty(max(o.numel() for o in outs), dtype=torch.uint8)
+    shared = comp.compact_host_many([t for t, _ in seq], k, 8, outs=[one] * len(seq))
+    assert sorted_lines(bytes(shared[-1].numpy())) == want[-1]
+
+
 def _golden():
     from tests.test_oracle import _checksum_cases, _golden_cases
     return _golden_cases(), _checksum_cases()

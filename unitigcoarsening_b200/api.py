@@ -115,6 +115,9 @@ def lib():
             "uc_compact_device": ([vp, vp, sz, i, i, vp, u64, pu64, ctypes.POINTER(Stats)], i),
             "uc_output_bound": ([sz, i], u64),
             "uc_compact_host": ([vp, vp, sz, i, i, vp, sz, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(Stats)], i),
+            "uc_compact_host_many": ([vp, i, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t), i, i,
+                                      ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t),
+                                      ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(Stats)], i),
             "uc_compact_batch": ([vp, i, ctypes.POINTER(vp), ctypes.POINTER(ctypes.c_size_t), i, i, vp, u64,
                                   pu64, pu64, ctypes.POINTER(Stats)], i),
             "uc_batch_output_bound": ([i, ctypes.POINTER(ctypes.c_size_t), i], u64),
@@ -345,6 +348,39 @@ class Compactor:
         if cache:
             store_tuning(cache, key, res, ms.value)
         return dict(res, ms=ms.value, trials=n.value, cached=False)
+
+    def compact_host_many(self, texts, k: int, l: int, outs=None, stats: bool = False):
+        """A sequence of host jobs with overlapped uploads (uc_compact_host_many):
+        each text (bytes, numpy uint8 or CPU tensor; pinned for full link
+        speed) goes to the device while the job before it finishes.  ``outs``
+        (CPU uint8 tensors, one per job, may repeat) receive the lines;
+        returns one view per job."""
+        nj = len(texts)
+        keep, tp, tn = [], [], []
+        for t in texts:
+            if isinstance(t, (bytes, bytearray)):
+                a = np.frombuffer(t, dtype=np.uint8)
+                keep.append(a)
+                tp.append(a.ctypes.data)
+                tn.append(a.nbytes)
+            elif isinstance(t, np.ndarray):
+                tp.append(t.ctypes.data)
+                tn.append(t.nbytes)
+            else:
+                tp.append(t.data_ptr())
+                tn.append(t.numel())
+        if outs is None:
+            outs = [torch.empty(self.output_bound(n, k), dtype=torch.uint8) for n in tn]
+        ptrs = (ctypes.c_void_p * max(nj, 1))(*tp)
+        sizes = (ctypes.c_size_t * max(nj, 1))(*tn)
+        optr = (ctypes.c_void_p * max(nj, 1))(*[o.data_ptr() for o in outs])
+        ocap = (ctypes.c_size_t * max(nj, 1))(*[o.numel() for o in outs])
+        olen = (ctypes.c_size_t * max(nj, 1))()
+        st = Stats()
+        self._bind_stream()
+        self._check(self._L.uc_compact_host_many(self._h, nj, ptrs, sizes, k, l, optr, ocap, olen, ctypes.byref(st)))
+        res = [outs[j][: olen[j]] for j in range(nj)]
+        return (res, st.as_dict()) if stats else res
 
     def compact_file(self, in_path: str, k: int, l: int, out_path: str) -> dict:
         st = Stats()

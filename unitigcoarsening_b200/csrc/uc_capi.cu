@@ -16,6 +16,9 @@ struct uc_ctx {
   size_t io_text_cap = 0;
   char* io_out = nullptr;
   size_t io_out_cap = 0;
+  // uc_compact_host_many: the upload stream and its completion event
+  cudaStream_t up_stream = nullptr;
+  cudaEvent_t up_done = nullptr;
 };
 
 struct uc_job {
@@ -161,6 +164,8 @@ uc_status uc_ctx_destroy(uc_ctx* c) {
   if (c->env.gstream) cudaStreamDestroy(c->env.gstream);
   if (c->io_text) cudaFree(c->io_text);
   if (c->io_out) cudaFree(c->io_out);
+  if (c->up_done) cudaEventDestroy(c->up_done);
+  if (c->up_stream) cudaStreamDestroy(c->up_stream);
   if (c->env.ctr) cudaFree(c->env.ctr);
   if (c->env.h_ctr) cudaFreeHost(c->env.h_ctr);
   for (int i = 0; i < uc::Env::NEV; ++i)
@@ -472,6 +477,91 @@ uc_status uc_compact_host(uc_ctx* c, const char* text, size_t bytes, int k, int 
   if (!c || !text || !out || !out_bytes) return UC_EINPUT;
   if (stats) std::memset(stats, 0, sizeof(*stats));
   return run_host(c, text, bytes, k, l, nullptr, out, cap, out_bytes, stats);
+}
+
+uc_status uc_compact_host_many(uc_ctx* c, int njobs, const char* const* texts, const size_t* bytes, int k, int l,
+                               char* const* outs, const size_t* caps, size_t* out_lens, uc_stats* stats) {
+  if (!c || njobs < 0 || (njobs > 0 && (!texts || !bytes || !outs || !caps || !out_lens))) return UC_EINPUT;
+  if (njobs == 0) return UC_OK;
+  uc_status s = set_device(c);
+  if (s) return s;
+  size_t tmax = 0;
+  uint64_t omax = 0;
+  for (int j = 0; j < njobs; ++j) {
+    if (!texts[j] && bytes[j]) return UC_EINPUT;
+    tmax = std::max(tmax, bytes[j]);
+    omax = std::max<uint64_t>(omax, uc::output_bound(bytes[j], k));
+  }
+  s = grow(c, &c->io_text, &c->io_text_cap, tmax + 64);
+  if (s) return s;
+  s = grow(c, &c->io_out, &c->io_out_cap, omax);
+  if (s) return s;
+  cudaError_t e = cudaSuccess;
+  if (!c->up_stream) e = cudaStreamCreateWithFlags(&c->up_stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess && !c->up_done) e = cudaEventCreateWithFlags(&c->up_done, cudaEventDisableTiming);
+  if (e != cudaSuccess) return cuda_fail(c, e, "upload stream");
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  // job 0's text goes up first; every later one goes up while the job before
+  // it is past its pack phase (its text is dead then), on the upload stream
+  e = cudaMemcpyAsync(c->io_text, texts[0], bytes[0], cudaMemcpyHostToDevice, c->up_stream);
+  if (e == cudaSuccess) e = cudaEventRecord(c->up_done, c->up_stream);
+  if (e != cudaSuccess) return cuda_fail(c, e, "cudaMemcpyAsync H2D");
+  uc_status result = UC_OK;
+  cudaError_t hook_err = cudaSuccess;
+  for (int j = 0; j < njobs && result == UC_OK; ++j) {
+    e = cudaStreamWaitEvent(c->env.stream, c->up_done, 0);
+    if (e != cudaSuccess) {
+      result = cuda_fail(c, e, "cudaStreamWaitEvent");
+      break;
+    }
+    const int nxt = j + 1;
+    c->env.after_pack = [&, nxt] {
+      if (nxt >= njobs) return;
+      cudaError_t he = cudaStreamWaitEvent(c->up_stream, c->env.ev[1], 0);
+      if (he == cudaSuccess)
+        he = cudaMemcpyAsync(c->io_text, texts[nxt], bytes[nxt], cudaMemcpyHostToDevice, c->up_stream);
+      if (he == cudaSuccess) he = cudaEventRecord(c->up_done, c->up_stream);
+      if (he != cudaSuccess && hook_err == cudaSuccess) hook_err = he;
+    };
+    uint64_t ob = 0;
+    uc_stats one{};
+    const int r = uc::compact_device(c->env, c->io_text, bytes[j], k, l, c->io_out, omax, ob, &one);
+    c->env.after_pack = nullptr;
+    if (r) {
+      result = as_status(r);
+      break;
+    }
+    if (hook_err != cudaSuccess) {
+      result = cuda_fail(c, hook_err, "cudaMemcpyAsync H2D (next job)");
+      break;
+    }
+    if (ob > caps[j]) {
+      c->env.err = "result buffer of job " + std::to_string(j) + " too small";
+      result = UC_EINPUT;
+      break;
+    }
+    if (ob) {
+      // stream order keeps the next job from writing io_out before this copy
+      e = cudaMemcpyAsync(outs[j], c->io_out, ob, cudaMemcpyDeviceToHost, c->env.stream);
+      if (e != cudaSuccess) {
+        result = cuda_fail(c, e, "cudaMemcpyAsync D2H");
+        break;
+      }
+    }
+    out_lens[j] = ob;
+    if (stats) {
+      stats->n_kmers += one.n_kmers;
+      stats->out_bytes += ob;
+      stats->ms_total += one.ms_total;
+      stats->launches += one.launches;
+    }
+  }
+  // the uploads and copies still in flight finish before return
+  const cudaError_t e1 = cudaStreamSynchronize(c->up_stream);
+  const cudaError_t e2 = cudaStreamSynchronize(c->env.stream);
+  if (result == UC_OK && e1 != cudaSuccess) result = cuda_fail(c, e1, "cudaStreamSynchronize");
+  if (result == UC_OK && e2 != cudaSuccess) result = cuda_fail(c, e2, "cudaStreamSynchronize");
+  return result;
 }
 
 uc_status uc_job_submit(uc_ctx* c, const char* text, size_t bytes, int k, int l, uc_job** job) {

@@ -2863,6 +2863,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     UC_CK(cudaGetLastError());
   }
   cudaEventRecord(e.ev[1], e.stream);
+  if (e.after_pack) e.after_pack();
   ++e.launches;
   k_widen16<<<grid_for(e, P.M, 256), 256, 0, e.stream>>>(f.c16, P.M, f.counts);
   uint64_t copies = 0;

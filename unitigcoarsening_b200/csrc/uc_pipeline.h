@@ -1,6 +1,7 @@
 // uc_pipeline.h — host-side pipeline entry points used by the C ABI.
 #pragma once
 #include <cstdint>
+#include <functional>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -52,6 +53,10 @@ struct Env {
   // whole-job calls (compact_device and the paths built on it) leave the
   // lines in byte order
   bool sorted = false;
+  // called by the fused path once the pack kernels are enqueued and ev[1]
+  // recorded after them: from then on the job's text is no longer read, so
+  // a host pipeline can upload the next job's text into the same buffer
+  std::function<void()> after_pack;
   std::string err;
 
   int fail(int code, const std::string& msg);
