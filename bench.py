@@ -293,6 +293,43 @@ def measure_batched(args, device: int):
             "speedup": plain_ms / batch_ms, "out_bytes_equal": plain_len == batch_len, "unit": UNIT}
 
 
+def measure_configs(args, device: int):
+    """The two other single-job shapes, device-resident, each on a fresh
+    context: the small plain job (1 Mbp, uniform ACGT, 200 SNP bubbles,
+    k=31) and the wide-k job (200 Mbp, 50% GC, 3% tandem repeats, 0.05% SNPs,
+    k=63, 128-bit keys).  Mean of 3 timed steps after 2 warm-up steps."""
+    import torch
+    from unitigcoarsening_b200 import Compactor, synth
+    res = {}
+    for name, spec, k in [("small_plain_1Mbp_k31", synth.small_plain(), 31),
+                          ("wide_k63_200Mbp", synth.wide_k(), 63)]:
+        with torch.no_grad():
+            text = synth.make_text(spec, k, device="cuda")
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        comp = Compactor(device)
+        out = torch.empty(comp.output_bound(text.numel(), k), dtype=torch.uint8, device="cuda")
+        l = min(args.l, k - 1)
+        for _ in range(2):
+            comp.compact(text, k, l, out=out)
+        stream = torch.cuda.current_stream()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(3):
+            r, st = comp.compact(text, k, l, out=out, stats=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 3
+        res[name] = {"value": st["n_kmers"] / (ms / 1e3), "unit": UNIT, "ms": ms, "n_kmers": int(st["n_kmers"]),
+                     "k": k, "text_bytes": int(text.numel()),
+                     "phase_ms": {p: round(st["ms_" + p], 3) for p in ("pack", "bucket", "tiles", "stitch")}}
+        comp.close()
+        del comp, text, out
+        torch.cuda.empty_cache()
+    return res
+
+
 def measure_serving(args, device: int):
     """Serving loop: a pool of distinct jobs (k-mer counts log-uniform in
     [10k, 50M], k = 31 with p 0.7 else 63) in pinned host memory; capacity =
@@ -389,6 +426,7 @@ def main():
     ap.add_argument("--tune-sample", type=float, default=2e8, help="genome length the autotuner times")
     ap.add_argument("--batch-jobs", type=int, default=256, help="jobs of the batched-vs-plain comparison (0: skip)")
     ap.add_argument("--batch-chunk", type=int, default=64, help="jobs per batched launch sequence")
+    ap.add_argument("--no-configs", action="store_true", help="skip the small and wide-k single-job shapes")
     ap.add_argument("--serve-jobs", type=int, default=400, help="arrivals of the serving measurement (0: skip)")
     ap.add_argument("--serve-pool", type=int, default=24, help="distinct jobs the arrivals draw from")
     args = ap.parse_args()
@@ -514,6 +552,7 @@ def main():
     del comp
     torch.cuda.empty_cache()
     batched = measure_batched(args, local) if args.batch_jobs > 0 else None
+    configs = measure_configs(args, local) if not args.no_configs else None
     serving = measure_serving(args, local) if args.serve_jobs > 0 else None
 
     cpu = None
@@ -537,7 +576,7 @@ def main():
             "phase_ms": phase, "kernel_ms": kern, "algorithmic_bytes": alg,
             "stats": {k2: (float(v) if isinstance(v, float) else int(v)) for k2, v in st.items()},
             "tuning": tuning,
-            "batched_vs_plain": batched, "serving": serving,
+            "batched_vs_plain": batched, "serving": serving, "other_configs": configs,
             "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
             "gpu_launches": int(st["launches"]) * args.steps,
             "gen_seconds": gen_s,
