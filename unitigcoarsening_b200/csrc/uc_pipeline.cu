@@ -1,11 +1,15 @@
 // uc_pipeline.cu — CUDA kernels of the unitig compactor and the host code
 // that sequences them.
 //
-// Data flow of the fused path (all device resident):
-//   text --k_pack--> keys[n] --k_lmin_count--> (b1,b2)[n] + bucket counts
-//   --scan/plan--> tiles of whole buckets --k_scatter--> copies in bucket order
-//   --k_tile (persistent, one tile per CTA in shared memory)--> finished lines
-//   + open segments --stitch (list ranking over segments)--> cross lines.
+// Data flow of the fused path (all device resident; a batch of jobs shares
+// every launch):
+//   text --k_pack (fused minimizers)--> keys[n], (b1,b2)[n], bucket counts
+//   --scan/plan--> tiles of whole buckets --k_scatter_coarse/fine--> copies
+//   in bucket order --k_tile_warp / k_tile / k_tile_big (persistent; a warp,
+//   a CTA, or global scratch per tile)--> finished lines + open segments
+//   --stitch (k_seg_link, list ranking, k_seg_copy)--> cross-tile lines.
+// The phase-by-phase entry points (pack, minimizers, find_edges, contract,
+// emit) run the same kernels separately.
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
@@ -1244,36 +1248,51 @@ __global__ void k_seg_link(uint32_t S, const uint32_t* __restrict__ seg_sx,
                            uint32_t* __restrict__ next, uint32_t* __restrict__ prev,
                            uint32_t* __restrict__ w, int k, unsigned long long* __restrict__ X,
                            uint32_t* __restrict__ act, uint32_t* act_count) {
-  const uint32_t stride = gridDim.x * blockDim.x;
+  constexpr int PER = 4;  // segments per thread and pass: their gathers are in flight together
+  const uint32_t span = gridDim.x * blockDim.x;
   // whole warps iterate together (warp_append needs every lane)
-  for (uint32_t s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); s0 < S; s0 += stride) {
-    const uint32_t s = s0 + (threadIdx.x & 31);
-    bool tail = false;
-    if (s < S) {
-      const uint32_t len = seg_len[s];
-      if (len == 0) {  // an unused slot of the segment pool
-        next[s] = NONE;
-        prev[s] = NONE;
-        w[s] = 0;
-        if (X) X[s] = pk(s | HEAD_BIT, 0);
-      } else {
-        const uint32_t ex = seg_ex[s], sx = seg_sx[s];
-        const uint32_t nx = (ex == NONE) ? NONE : start_seg[ex];
-        const uint32_t pv = (sx == NONE) ? NONE : end_seg[sx];
-        const uint32_t ws = (pv == NONE) ? uint32_t(k) - 1u + len : len - 1u;
-        next[s] = nx;
-        prev[s] = pv;
-        w[s] = ws;
-        if (X) {
-          if (pv == NONE) X[s] = pk(s | HEAD_BIT, 0);
-          if (nx != NONE) X[nx] = pk(s, ws);
-          tail = pv != NONE;
+  for (uint32_t s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); s0 < S; s0 += span * PER) {
+    uint32_t sid[PER], len[PER], ex[PER], sx[PER], nx[PER], pv[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      sid[q] = s0 + uint32_t(q) * span + (threadIdx.x & 31);
+      const bool in = sid[q] < S && (s0 + uint32_t(q) * span) >= s0;
+      len[q] = in ? seg_len[sid[q]] : 0u;
+      ex[q] = (in && len[q]) ? seg_ex[sid[q]] : NONE;
+      sx[q] = (in && len[q]) ? seg_sx[sid[q]] : NONE;
+      if (!in) sid[q] = NONE;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      nx[q] = (ex[q] == NONE) ? NONE : start_seg[ex[q]];
+      pv[q] = (sx[q] == NONE) ? NONE : end_seg[sx[q]];
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const uint32_t s = sid[q];
+      bool tail = false;
+      if (s != NONE) {
+        if (len[q] == 0) {  // an unused slot of the segment pool
+          next[s] = NONE;
+          prev[s] = NONE;
+          w[s] = 0;
+          if (X) X[s] = pk(s | HEAD_BIT, 0);
+        } else {
+          const uint32_t ws = (pv[q] == NONE) ? uint32_t(k) - 1u + len[q] : len[q] - 1u;
+          next[s] = nx[q];
+          prev[s] = pv[q];
+          w[s] = ws;
+          if (X) {
+            if (pv[q] == NONE) X[s] = pk(s | HEAD_BIT, 0);
+            if (nx[q] != NONE) X[nx[q]] = pk(s, ws);
+            tail = pv[q] != NONE;
+          }
         }
       }
-    }
-    if (X) {
-      const uint32_t slot = warp_append(act_count, tail);
-      if (tail) act[slot] = s;
+      if (X) {
+        const uint32_t slot = warp_append(act_count, tail);
+        if (tail) act[slot] = s;
+      }
     }
   }
 }
