@@ -189,9 +189,11 @@ uc_status uc_compact_host(uc_ctx *ctx, const char *text, size_t bytes, int k,
 /* Many independent jobs in one pass (same k and l): all their buckets form
  * one tile queue worked by one persistent launch per tier.  Job j's lines land
  * in d_out[out_offsets[j], out_offsets[j] + out_lengths[j]).  d_out needs
- * uc_batch_output_bound bytes.  Jobs whose lines are not exactly k chars +
- * '\n' are compacted one by one.  (No reference counterpart: the reference
- * runs one job per process; this is the batched form of its main.) */
+ * uc_batch_output_bound bytes.  When a job's lines are not exactly k chars +
+ * '\n', or any job is malformed, the jobs are compacted one by one, and a
+ * malformed job fails the call with UC_EINPUT and its index in
+ * uc_last_error.  (No reference counterpart: the reference runs one job per
+ * process; this is the batched form of its main.) */
 uc_status uc_compact_batch(uc_ctx *ctx, int njobs, const char *const *d_texts,
                            const size_t *bytes, int k, int l, char *d_out,
                            uint64_t out_cap, uint64_t *out_offsets,

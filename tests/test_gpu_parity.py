@@ -337,6 +337,21 @@ def test_batch_k63_and_mixed_layouts(comp, oracle):
         assert sorted_lines(o.cpu().numpy().tobytes()) == sorted_lines(want)
 
 
+def test_batch_names_a_malformed_job(comp, texts):
+    """A batch with a job whose count line is wrong fails with UC_EINPUT and
+    the job's index in the error; without it the same batch succeeds."""
+    from unitigcoarsening_b200 import UCError
+    good = texts["batched_job"][0]
+    head, body = good.split(b"\n", 1)
+    bad = str(int(head) - 1).encode() + b"\n" + body
+    jobs = [dev(good), dev(good), dev(bad), dev(good)]
+    with pytest.raises(UCError) as ei:
+        comp.compact_batch(jobs, 31, 8)
+    assert ei.value.status == 1 and "job 2" in str(ei.value)
+    res = comp.compact_batch([dev(good)] * 3, 31, 8)
+    assert len(res) == 3 and res[0].numel() == res[2].numel() > 0
+
+
 def test_batch_with_tiers_and_hec(comp, oracle):
     from unitigcoarsening_b200 import CONTRACT_HEC, synth
     jobs = [synth.make_text(synth.scale_plain(length=40_000 + 9_000 * j, seed=60 + j), 31).numpy().tobytes()

@@ -82,3 +82,29 @@ def test_admission_under_a_small_pool(comp, mix):
     for (data, _), want in zip(res, alone):
         assert sorted_lines(data) == want
     assert st["pool_peak_bytes"] <= budget
+
+
+def test_bad_job_fails_alone(comp, mix):
+    """A job whose count line disagrees with its lines, and one with a line
+    shorter than k, fail with UC_EINPUT; the jobs around them (batched or
+    not) complete with their own lines."""
+    from unitigcoarsening_b200 import Server, UCError
+    good = [(t, k) for t, k in mix if k == 31][:6]
+    alone = [sorted_lines(bytes(comp.compact_host(t, k, 8).numpy())) for t, k in good]
+    t0 = good[0][0]
+    head, body = t0.split(b"\n", 1)
+    wrong_count = str(int(head) + 5).encode() + b"\n" + body
+    short_line = b"2\n" + b"A" * 31 + b"\nACGT\n"
+    jobs = [good[0], (wrong_count, 31), good[1], good[2], (short_line, 31), good[3], good[4], good[5]]
+    with Server(lanes=2, max_batch=4, hbm_budget=2 << 30) as srv:
+        tickets = [srv.submit(t, k, 8) for t, k in jobs]
+        results = []
+        for t in tickets:
+            try:
+                results.append(srv.wait(t, timeout=120)[0])
+            except UCError as e:
+                results.append(e.status)
+    assert results[1] == 1 and results[4] == 1  # UC_EINPUT
+    got = [r for i, r in enumerate(results) if i not in (1, 4)]
+    for g, w in zip(got, alone):
+        assert sorted_lines(g) == w

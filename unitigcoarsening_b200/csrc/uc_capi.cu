@@ -448,8 +448,9 @@ uc_status uc_compact_batch(uc_ctx* c, int njobs, const char* const* d_texts, con
   if (stats) std::memset(stats, 0, sizeof(*stats));
   int r = uc::compact_batch(c->env, uint32_t(njobs), d_texts, bytes, k, l, d_out, out_cap, out_off, out_len, stats);
   c->env.reset();
-  if (r == UC_EINPUT && c->env.err.find("batched jobs need") != std::string::npos) {
-    // a job with another line layout: compact the jobs one by one
+  if (r == UC_EINPUT) {
+    // a job with another line layout, or a malformed one: compact the jobs
+    // one by one, so that a malformed job is named
     uint64_t base = 0;
     for (int j = 0; j < njobs; ++j) {
       const uint64_t cap = uc::output_bound(bytes[j], k);
@@ -457,7 +458,10 @@ uc_status uc_compact_batch(uc_ctx* c, int njobs, const char* const* d_texts, con
       uc_stats one{};
       r = uc::compact_device(c->env, d_texts[j], bytes[j], k, l, d_out + base, cap, ob, stats ? &one : nullptr);
       c->env.reset();
-      if (r) return as_status(r);
+      if (r) {
+        c->env.err = "job " + std::to_string(j) + ": " + c->env.err;
+        return as_status(r);
+      }
       out_off[j] = base;
       out_len[j] = ob;
       if (stats) {

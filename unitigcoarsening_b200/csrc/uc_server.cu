@@ -241,14 +241,17 @@ void run_work(uc_server* s, Lane& ln) {
       e.reset();
       if (r == UC_OK) {
         for (uint32_t i = 0; i < nj; ++i) jst[i] = bs;
-      } else if (r != UC_EINPUT || e.err.find("batched jobs need") == std::string::npos) {
+      } else if (r != UC_EINPUT) {
         st = static_cast<uc_status>(r);
         err = e.err;
       }
+      // an input the batched path does not take (a layout other than k
+      // chars and '\n' per line) or a malformed job: every job runs alone
+      // below, so that only a malformed one fails
     }
     if (st == UC_OK && (nj == 1 || r != UC_OK)) {
-      // one job, or a batch whose layout the batched path does not take:
-      // each job alone, one after another, in the same slice
+      // one job, or a batch that the batched path refused: each job alone,
+      // one after another, in the same slice
       uint64_t pos = 0;
       for (uint32_t i = 0; i < nj; ++i) {
         uint64_t ob = 0;
