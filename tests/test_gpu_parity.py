@@ -195,10 +195,13 @@ def test_sorted_output_is_byte_exact(comp, oracle, texts, cfg):
         a = comp.compact(dev(text), k, min(8, k - 1)).cpu().numpy().tobytes()
         b = comp.compact(dev(text), k, min(8, k - 1)).cpu().numpy().tobytes()
         h = bytes(comp.compact_host(text, k, min(8, k - 1)).numpy())
+        # an output buffer that is not 16-byte aligned takes the byte-wise line scan
+        buf = torch.empty(comp.output_bound(len(text), k) + 16, dtype=torch.uint8, device="cuda")
+        u = comp.compact(dev(text), k, min(8, k - 1), out=buf[3:]).cpu().numpy().tobytes()
     finally:
         comp.set_sorted_output(False)
     assert a == expect
-    assert b == expect and h == expect
+    assert b == expect and h == expect and u == expect
 
 
 def test_sorted_output_cli(comp, oracle, texts, tmp_path):

@@ -3121,23 +3121,117 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
 
 // ============================================================ sorted output
 
-// Each line's first k chars, packed big-endian (first char in the top bits
-// of hi, chars 32.. in lo), so that numeric order is byte order.  Every
-// k-mer begins at most one line, so these keys order the lines completely.
-__global__ void k_line_keys(const char* __restrict__ out, const unsigned long long* __restrict__ starts, uint64_t L,
-                            int k, unsigned long long* __restrict__ khi, unsigned long long* __restrict__ klo,
-                            uint32_t* __restrict__ idx) {
-  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < L; j += uint64_t(gridDim.x) * blockDim.x) {
-    const char* p = out + starts[j];
-    unsigned long long hi = 0, lo = 0;
-    for (int c = 0; c < k; ++c) {
-      const uint32_t b = uint8_t(p[c]);
-      const unsigned long long code = ((b >> 1) ^ (b >> 2)) & 3u;  // A C G T -> 0 1 2 3
-      if (c < 32) hi |= code << (62 - 2 * c);
-      else lo |= code << (62 - 2 * (c - 32));
+// 0x80 in every byte of w that is a line break.
+__device__ __forceinline__ uint32_t nl_bytes(uint32_t w) {
+  const uint32_t z = w ^ 0x0A0A0A0Au;
+  return ~(((z & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | z) & 0x80808080u;
+}
+
+// Line breaks in each 64 KiB chunk of out[0, n), 16-byte loads (out is
+// 16-byte aligned; the tail of a chunk that ends inside a word is read
+// byte by byte).
+constexpr uint32_t NL_CHUNK = 1u << 16;
+__global__ void __launch_bounds__(256) k_nl_count16(const char* __restrict__ out, uint64_t n,
+                                                    uint32_t* __restrict__ cnt) {
+  const uint64_t c0 = uint64_t(blockIdx.x) * NL_CHUNK;
+  uint32_t acc = 0;
+#pragma unroll 4
+  for (uint32_t j = 0; j < NL_CHUNK / (16 * 256); ++j) {
+    const uint64_t off = c0 + 16ull * (threadIdx.x + 256u * j);
+    if (off + 16 <= n) {
+      const uint4 v = __ldcs(reinterpret_cast<const uint4*>(out + off));
+      acc += __popc(nl_bytes(v.x)) + __popc(nl_bytes(v.y)) + __popc(nl_bytes(v.z)) + __popc(nl_bytes(v.w));
+    } else {
+      for (uint64_t i = off; i < n && i < off + 16; ++i) acc += (out[i] == '\n');
     }
-    khi[j] = hi;
-    klo[j] = lo;
+  }
+  acc = __reduce_add_sync(0xFFFFFFFFu, acc);
+  __shared__ uint32_t sh[8];
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t t = 0;
+    for (int w = 0; w < 8; ++w) t += sh[w];
+    cnt[blockIdx.x] = t;
+  }
+}
+
+// Line starts: starts[0] = 0 and starts[r + 1] = 1 + the position of the
+// r-th line break in out[0, n).  Each thread owns 256 contiguous bytes of its
+// block's chunk: a count pass, a block scan, then a pass that writes.
+__global__ void __launch_bounds__(256) k_nl_starts16(const char* __restrict__ out, uint64_t n,
+                                                     const unsigned long long* __restrict__ coff,
+                                                     unsigned long long* __restrict__ starts, uint64_t nlines) {
+  const uint64_t t0 = uint64_t(blockIdx.x) * NL_CHUNK + 256ull * threadIdx.x;
+  if (blockIdx.x == 0 && threadIdx.x == 0) starts[0] = 0;
+  uint32_t mine = 0;
+  for (uint32_t j = 0; j < 16; ++j) {
+    const uint64_t off = t0 + 16ull * j;
+    if (off + 16 <= n) {
+      const uint4 v = *reinterpret_cast<const uint4*>(out + off);
+      mine += __popc(nl_bytes(v.x)) + __popc(nl_bytes(v.y)) + __popc(nl_bytes(v.z)) + __popc(nl_bytes(v.w));
+    } else {
+      for (uint64_t i = off; i < n && i < off + 16; ++i) mine += (out[i] == '\n');
+    }
+  }
+  __shared__ uint32_t sc[33];
+  uint32_t tot;
+  uint64_t r = coff[blockIdx.x] + block_excl_scan(mine, sc, &tot);
+  for (uint32_t j = 0; j < 16; ++j) {
+    const uint64_t off = t0 + 16ull * j;
+    if (off + 16 <= n) {
+      const uint4 v = *reinterpret_cast<const uint4*>(out + off);
+      const uint32_t wv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        uint32_t m = nl_bytes(wv[q]);
+        while (m) {
+          const int b = (__ffs(m) - 1) >> 3;
+          m &= m - 1;
+          ++r;
+          if (r < nlines) starts[r] = off + 4u * q + b + 1;
+        }
+      }
+    } else {
+      for (uint64_t i = off; i < n && i < off + 16; ++i) {
+        if (out[i] == '\n') {
+          ++r;
+          if (r < nlines) starts[r] = i + 1;
+        }
+      }
+    }
+  }
+}
+
+// Line keys: each line's first k chars, packed big-endian (first char in the
+// top bits of hi, chars 32.. in lo), so that numeric order is byte order.
+// Every k-mer begins at most one line, so these keys order the lines
+// completely.  The k chars are read as 4-byte words
+// (funnel-shifted to the line's byte offset) and converted 4 codes at a time;
+// the little-endian codes are then reversed into big-endian keys.  Reads up
+// to 12 bytes past a line's k chars (inside the output buffer's bound).
+__global__ void k_line_keys4(const char* __restrict__ out, const unsigned long long* __restrict__ starts,
+                             uint64_t L, int k, unsigned long long* __restrict__ khi,
+                             unsigned long long* __restrict__ klo, uint32_t* __restrict__ idx) {
+  const int nw = (k + 3) / 4;
+  const uint64_t m0 = (k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull);
+  const uint64_t m1 = (k <= 32) ? 0ull : ((k - 32 >= 32) ? ~0ull : ((1ull << (2 * (k - 32))) - 1ull));
+  for (uint64_t j = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; j < L; j += uint64_t(gridDim.x) * blockDim.x) {
+    const uintptr_t a = reinterpret_cast<uintptr_t>(out + starts[j]);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+    const uint32_t sh = 8u * uint32_t(a & 3u);
+    uint64_t w0 = 0, w1 = 0;
+    uint32_t cur = w[0];
+    for (int q = 0; q < nw; ++q) {
+      const uint32_t nxt = w[q + 1];
+      const uint32_t x = __funnelshift_r(cur, nxt, sh);
+      cur = nxt;
+      const uint64_t g = gather_codes(((x >> 1) ^ (x >> 2)) & 0x03030303u);
+      if (q < 8) w0 |= g << (8 * q);
+      else w1 |= g << (8 * (q - 8));
+    }
+    khi[j] = rev2(w0 & m0);
+    klo[j] = rev2(w1 & m1);
     idx[j] = uint32_t(j);
   }
 }
@@ -3188,8 +3282,9 @@ __global__ void k_line_copy(const char* __restrict__ src, const unsigned long lo
 int sort_lines(Env& e, char* out, uint64_t bytes, int k) {
   if (bytes == 0) return UC_OK;
   e.reset();
-  const uint32_t chunk = 1 << 16;
+  const uint32_t chunk = NL_CHUNK;
   const uint64_t nchunks = std::max<uint64_t>(1, (bytes - 1 + chunk - 1) / chunk);
+  const bool aligned = (reinterpret_cast<uintptr_t>(out) & 15u) == 0;  // else byte-wise line scan
   // lines end with '\n'; the last one at bytes - 1
   const uint64_t Lmax = bytes / uint64_t(k + 1) + 1;
   size_t cub_bytes = 0;
@@ -3225,18 +3320,20 @@ int sort_lines(Env& e, char* out, uint64_t bytes, int k) {
   if (!cub_tmp) return e.fail(UC_EBUDGET, "arena overflow (sorted output)");
   const uint8_t* ob = reinterpret_cast<const uint8_t*>(out);
   e.launches += 1 + 6 + 1;
-  k_count_nl<<<unsigned(nchunks), 256, 0, e.stream>>>(ob, 0, bytes - 1, cnt, chunk);
+  if (aligned) k_nl_count16<<<unsigned(nchunks), 256, 0, e.stream>>>(out, bytes - 1, cnt);
+  else k_count_nl<<<unsigned(nchunks), 256, 0, e.stream>>>(ob, 0, bytes - 1, cnt, chunk);
   scan_excl<uint32_t, unsigned long long>(cnt, nchunks, coff, ctmp, e.stream);
   unsigned long long nl = 0;
   UC_CK(cudaMemcpyAsync(&nl, coff + nchunks, 8, cudaMemcpyDeviceToHost, e.stream));
   UC_CK(cudaStreamSynchronize(e.stream));
   const uint64_t L = nl + 1;
   if (L > Lmax || L >= 0x7FFFFFFFull) return e.fail(UC_EINTERNAL, "line count of the output out of range");
-  k_write_starts<<<unsigned(nchunks), 256, 0, e.stream>>>(ob, 0, bytes - 1, coff, chunk, starts, L);
+  if (aligned) k_nl_starts16<<<unsigned(nchunks), 256, 0, e.stream>>>(out, bytes - 1, coff, starts, L);
+  else k_write_starts<<<unsigned(nchunks), 256, 0, e.stream>>>(ob, 0, bytes - 1, coff, chunk, starts, L);
   UC_CK(cudaMemcpyAsync(starts + L, &bytes, 8, cudaMemcpyHostToDevice, e.stream));
   const int g = grid_for(e, L, 256);
   e.launches += 1;
-  k_line_keys<<<g, 256, 0, e.stream>>>(out, starts, L, k, khi, klo, idx);
+  k_line_keys4<<<g, 256, 0, e.stream>>>(out, starts, L, k, khi, klo, idx);
   // least significant part first; radix sort is stable
   uint32_t* order = idx;
   if (k > 32) {
