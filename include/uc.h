@@ -217,8 +217,10 @@ uc_status uc_compact_host_many(uc_ctx *ctx, int njobs, const char *const *texts,
                                size_t *out_lens, uc_stats *stats);
 
 /* Submit host text (pageable or pinned); the job copies it to the device,
- * runs the fused path and copies the lines back.  main, driver.cpp:422-662,
- * without the file I/O. */
+ * runs the fused path and copies the lines back into a buffer the library
+ * allocates, all before uc_job_submit returns (poll and wait then report it
+ * done; the serving loop below is the asynchronous form).  main,
+ * driver.cpp:422-662, without the file I/O. */
 uc_status uc_job_submit(uc_ctx *ctx, const char *text, size_t bytes, int k,
                         int l, uc_job **job);
 uc_status uc_job_poll(uc_job *job, int *done);
