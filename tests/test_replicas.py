@@ -33,7 +33,7 @@ def _rank(rank, world, port, out):
 def test_replica_totals_two_gloo_ranks():
     world = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:  # no fork of a threaded process
         out = mgr.dict()
         mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
