@@ -562,7 +562,6 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
   uint32_t* hist = reinterpret_cast<uint32_t*>(gbase + mc);                     // [mc]
   uint32_t* lofs = hist + mc;                                                   // [mc + 1]
   __shared__ uint32_t sc[33];
-  const int lane = threadIdx.x & 31;
   for (uint64_t c0 = uint64_t(blockIdx.x) * SC_CHUNK; c0 < n; c0 += uint64_t(gridDim.x) * SC_CHUNK) {
     const uint32_t cn = uint32_t((n - c0) < uint64_t(SC_CHUNK) ? (n - c0) : uint64_t(SC_CHUNK));
     // every load of the chunk is issued at once; the values stay in registers
@@ -580,24 +579,36 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
     }
     for (uint32_t j = threadIdx.x; j < mc; j += blockDim.x) hist[j] = 0;
     __syncthreads();
-    // count copies per coarse partition
+    // count copies per coarse partition; bit q of cmask marks a cross k-mer
+    uint32_t cmask = 0;
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
       const uint32_t t = uint32_t(q) * 256u + threadIdx.x;
       if (t < cn) {
         atomicAdd(hist + (aa[q] >> fb), 1u);
-        if (aa[q] != bb[q]) atomicAdd(hist + (bb[q] >> fb), 1u);
+        if (aa[q] != bb[q]) {
+          atomicAdd(hist + (bb[q] >> fb), 1u);
+          cmask |= 1u << q;
+        }
       }
     }
     __syncthreads();
-    // local offsets (scan over the partitions) and global reservations
+    // local offsets (scan over the partitions), this thread's first cross
+    // index within the chunk, and global reservations.  One scan carries both
+    // sums: the copy count in the low half (<= 4096) and the cross count in
+    // the high half (<= 2048).  The chunk's cross indices are reserved with a
+    // single atomic: a counter shared by every block of the grid serialises
+    // in L2, so one reservation per warp and k-mer slot would bound the kernel.
+    uint32_t xpre;
     {
       const uint32_t per = (mc + blockDim.x - 1) / blockDim.x;
       const uint32_t j0 = min(mc, threadIdx.x * per), j1 = min(mc, j0 + per);
       uint32_t acc = 0;
       for (uint32_t j = j0; j < j1; ++j) acc += hist[j];
       uint32_t tot;
-      uint32_t pre = block_excl_scan(acc, sc, &tot);
+      const uint32_t both = block_excl_scan(acc | (uint32_t(__popc(cmask)) << 16), sc, &tot);
+      uint32_t pre = both & 0xFFFFu;
+      xpre = both >> 16;
       for (uint32_t j = j0; j < j1; ++j) {
         const uint32_t h = hist[j];
         lofs[j] = pre;
@@ -605,9 +616,14 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
         pre += h;
         hist[j] = 0;
       }
-      if (threadIdx.x == 0) lofs[mc] = tot;
+      if (threadIdx.x == 0) {
+        lofs[mc] = tot & 0xFFFFu;
+        const uint32_t xt = tot >> 16;
+        sc[32] = (!ids_mode && xt) ? atomicAdd(&ctr->cross_count, xt) : 0u;
+      }
     }
     __syncthreads();
+    xpre += sc[32];
     // place every copy in its partition's run of the staging area
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
@@ -622,17 +638,8 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
         a = aa[q];
         b = bb[q];
       }
-      const bool cross = live && (a != b);
-      uint32_t x = NONE;
-      if (!ids_mode) {
-        const uint32_t m = __ballot_sync(0xFFFFFFFFu, cross);
-        uint32_t bx = 0;
-        if (m) {
-          if (lane == __ffs(m) - 1) bx = atomicAdd(&ctr->cross_count, uint32_t(__popc(m)));
-          bx = __shfl_sync(0xFFFFFFFFu, bx, __ffs(m) - 1);
-        }
-        if (cross) x = bx + __popc(m & ((1u << lane) - 1u));
-      }
+      const bool cross = (cmask >> q) & 1u;
+      const uint32_t x = (!ids_mode && cross) ? xpre + __popc(cmask & ((1u << q) - 1u)) : NONE;
       if (live) {
         const uint32_t link = ids_mode ? uint32_t(c0 + t) : x;
         Key<NW> kp = key;
@@ -1222,17 +1229,19 @@ constexpr uint32_t HEAD_BIT = 0x80000000u;
 __device__ __forceinline__ uint32_t ptr_of(unsigned long long v) { return pk_p(v) & ~HEAD_BIT; }
 __device__ __forceinline__ bool is_head_entry(unsigned long long v) { return (pk_p(v) & HEAD_BIT) != 0; }
 
-// Slot for a lane that appends to a shared list: one atomic per warp.
-// Every lane of the warp must call it (pred false = no slot).
-__device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool pred) {
-  const uint32_t m = __ballot_sync(0xFFFFFFFFu, pred);
-  if (!m) return NONE;
-  const int lane = threadIdx.x & 31;
-  const int leader = __ffs(m) - 1;
-  uint32_t b = 0;
-  if (lane == leader) b = atomicAdd(count, uint32_t(__popc(m)));
-  b = __shfl_sync(0xFFFFFFFFu, b, leader);
-  return pred ? b + uint32_t(__popc(m & ((1u << lane) - 1u))) : NONE;
+// First of c consecutive slots for each thread of a block that appends to a
+// shared list: one atomic per block.  A list counter that every block of the
+// grid bumps serialises in L2, so per-warp appends would bound a pass that
+// appends most of its elements.  Every thread of the block must call it;
+// sc holds 33 values.
+__device__ __forceinline__ uint32_t block_append(uint32_t* count, uint32_t c, uint32_t* sc) {
+  uint32_t tot;
+  const uint32_t pre = block_excl_scan(c, sc, &tot);  // ends with a barrier after every read of sc
+  if (threadIdx.x == 0) sc[32] = tot ? atomicAdd(count, tot) : 0u;
+  __syncthreads();
+  const uint32_t b = sc[32] + pre;
+  __syncthreads();  // sc is reused by the next call
+  return b;
 }
 
 // Segment links: next/prev through the cross k-mer at each open end, and
@@ -1242,70 +1251,73 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* count, bool pred) {
 // successor t sets X[t] = (s, w[s]) - every cross k-mer joins exactly one
 // segment ending there to one starting there, so each entry is written once.
 // Segments with a predecessor go to the active list.
-__global__ void k_seg_link(uint32_t S, const uint32_t* __restrict__ seg_sx,
+__global__ void __launch_bounds__(256) k_seg_link(uint32_t S, const uint32_t* __restrict__ seg_sx,
                            const uint32_t* __restrict__ seg_ex, const uint32_t* __restrict__ seg_len,
                            const uint32_t* __restrict__ start_seg, const uint32_t* __restrict__ end_seg,
                            uint32_t* __restrict__ next, uint32_t* __restrict__ prev,
                            uint32_t* __restrict__ w, int k, unsigned long long* __restrict__ X,
                            uint32_t* __restrict__ act, uint32_t* act_count) {
   constexpr int PER = 4;  // segments per thread and pass: their gathers are in flight together
-  const uint32_t span = gridDim.x * blockDim.x;
-  // whole warps iterate together (warp_append needs every lane)
-  for (uint32_t s0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); s0 < S; s0 += span * PER) {
+  __shared__ uint32_t sc[33];
+  const uint64_t B = blockDim.x;
+  // whole blocks iterate together (block_append needs every thread)
+  for (uint64_t b0 = uint64_t(blockIdx.x) * B * PER; b0 < S; b0 += uint64_t(gridDim.x) * B * PER) {
     uint32_t sid[PER], len[PER], ex[PER], sx[PER], nx[PER], pv[PER];
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
-      sid[q] = s0 + uint32_t(q) * span + (threadIdx.x & 31);
-      const bool in = sid[q] < S && (s0 + uint32_t(q) * span) >= s0;
-      len[q] = in ? seg_len[sid[q]] : 0u;
-      ex[q] = (in && len[q]) ? seg_ex[sid[q]] : NONE;
-      sx[q] = (in && len[q]) ? seg_sx[sid[q]] : NONE;
-      if (!in) sid[q] = NONE;
+      const uint64_t i = b0 + uint64_t(q) * B + threadIdx.x;
+      const bool in = i < S;
+      sid[q] = in ? uint32_t(i) : NONE;
+      len[q] = in ? seg_len[i] : 0u;
+      ex[q] = (in && len[q]) ? seg_ex[i] : NONE;
+      sx[q] = (in && len[q]) ? seg_sx[i] : NONE;
     }
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
       nx[q] = (ex[q] == NONE) ? NONE : start_seg[ex[q]];
       pv[q] = (sx[q] == NONE) ? NONE : end_seg[sx[q]];
     }
+    uint32_t tails = 0;  // bit q: segment q has a predecessor
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
       const uint32_t s = sid[q];
-      bool tail = false;
-      if (s != NONE) {
-        if (len[q] == 0) {  // an unused slot of the segment pool
-          next[s] = NONE;
-          prev[s] = NONE;
-          w[s] = 0;
-          if (X) X[s] = pk(s | HEAD_BIT, 0);
-        } else {
-          const uint32_t ws = (pv[q] == NONE) ? uint32_t(k) - 1u + len[q] : len[q] - 1u;
-          next[s] = nx[q];
-          prev[s] = pv[q];
-          w[s] = ws;
-          if (X) {
-            if (pv[q] == NONE) X[s] = pk(s | HEAD_BIT, 0);
-            if (nx[q] != NONE) X[nx[q]] = pk(s, ws);
-            tail = pv[q] != NONE;
-          }
+      if (s == NONE) continue;
+      if (len[q] == 0) {  // an unused slot of the segment pool
+        next[s] = NONE;
+        prev[s] = NONE;
+        w[s] = 0;
+        if (X) X[s] = pk(s | HEAD_BIT, 0);
+      } else {
+        const uint32_t ws = (pv[q] == NONE) ? uint32_t(k) - 1u + len[q] : len[q] - 1u;
+        next[s] = nx[q];
+        prev[s] = pv[q];
+        w[s] = ws;
+        if (X) {
+          if (pv[q] == NONE) X[s] = pk(s | HEAD_BIT, 0);
+          if (nx[q] != NONE) X[nx[q]] = pk(s, ws);
+          if (pv[q] != NONE) tails |= 1u << q;
         }
       }
-      if (X) {
-        const uint32_t slot = warp_append(act_count, tail);
-        if (tail) act[slot] = s;
-      }
+    }
+    if (X) {
+      uint32_t slot = block_append(act_count, uint32_t(__popc(tails)), sc);
+#pragma unroll
+      for (int q = 0; q < PER; ++q)
+        if ((tails >> q) & 1u) act[slot++] = sid[q];
     }
   }
 }
 
 // X[v] = (start pointer, weight distance); heads point at themselves.
-__global__ void k_rank_init(const uint32_t* __restrict__ prev, const uint32_t* __restrict__ w,
+__global__ void __launch_bounds__(256) k_rank_init(const uint32_t* __restrict__ prev, const uint32_t* __restrict__ w,
                             uint64_t n, const Counters* ctr, unsigned long long* __restrict__ X,
                             uint32_t* __restrict__ act, uint32_t* act_count) {
+  __shared__ uint32_t sc[33];
   const uint64_t N = ctr ? uint64_t(ctr->seg_count) : n;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
-  // whole warps iterate together (warp_append needs every lane)
-  for (uint64_t s0 = uint64_t(blockIdx.x) * blockDim.x + (threadIdx.x & ~31u); s0 < N; s0 += stride) {
-    const uint64_t s = s0 + (threadIdx.x & 31);
+  // whole blocks iterate together (block_append needs every thread)
+  for (uint64_t s0 = uint64_t(blockIdx.x) * blockDim.x; s0 < N; s0 += stride) {
+    const uint64_t s = s0 + threadIdx.x;
     bool tail = false;
     if (s < N) {
       const uint32_t pv = prev[s];
@@ -1316,7 +1328,7 @@ __global__ void k_rank_init(const uint32_t* __restrict__ prev, const uint32_t* _
         tail = true;
       }
     }
-    const uint32_t slot = warp_append(act_count, tail);
+    const uint32_t slot = block_append(act_count, tail ? 1u : 0u, sc);
     if (tail) act[slot] = uint32_t(s);
   }
 }
@@ -1325,13 +1337,15 @@ __global__ void k_rank_init(const uint32_t* __restrict__ prev, const uint32_t* _
 // are (pointer, distance) pairs in one 64-bit word, so a concurrent reader
 // always sees a consistent pair; the list keeps the entries whose pointer
 // does not yet reach a head.
-__global__ void k_rank_round(unsigned long long* __restrict__ X, const uint32_t* __restrict__ act,
+__global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restrict__ X, const uint32_t* __restrict__ act,
                              const uint32_t* act_count, uint32_t* __restrict__ act_out,
                              uint32_t* act_out_count) {
+  __shared__ uint32_t sc[33];
   const uint32_t na = *act_count;
-  const uint32_t stride = gridDim.x * blockDim.x;
-  for (uint32_t j0 = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); j0 < na; j0 += stride) {
-    const uint32_t j = j0 + (threadIdx.x & 31);
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  // whole blocks iterate together (block_append needs every thread)
+  for (uint64_t j0 = uint64_t(blockIdx.x) * blockDim.x; j0 < na; j0 += stride) {
+    const uint64_t j = j0 + threadIdx.x;
     bool keep = false;
     uint32_t s = 0;
     if (j < na) {
@@ -1345,7 +1359,7 @@ __global__ void k_rank_round(unsigned long long* __restrict__ X, const uint32_t*
         keep = !is_head_entry(z);
       }
     }
-    const uint32_t slot = warp_append(act_out_count, keep);
+    const uint32_t slot = block_append(act_out_count, keep ? 1u : 0u, sc);
     if (keep) act_out[slot] = s;
   }
 }
