@@ -1166,16 +1166,18 @@ __global__ void __launch_bounds__(256) k_tile_warp(TileParams p) {
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const TileMem<NW, uint16_t> m = carve<NW, uint16_t>(smem + size_t(wid) * p.wbytes, p.wcap, p.wts);
   const uint32_t nt = p.ctr->nwarp;
-  for (;;) {
-    uint32_t j = 0;
-    if (lane == 0) j = atomicAdd(&p.ctr->wtile_next, 1u);
-    j = __shfl_sync(0xFFFFFFFFu, j, 0);
-    if (j >= nt) break;
+  uint32_t j = 0;
+  if (lane == 0) j = atomicAdd(&p.ctr->wtile_next, 1u);
+  j = __shfl_sync(0xFFFFFFFFu, j, 0);
+  while (j < nt) {
+    uint32_t jn = 0;  // the next tile's index is in flight while this tile is worked
+    if (lane == 0) jn = atomicAdd(&p.ctr->wtile_next, 1u);
     const uint32_t t = p.wlist[j];
     const uint64_t beg = p.tile_begin[t];
     const uint32_t c = uint32_t(p.tile_begin[t + 1] - beg);
     process_tile<NW, uint16_t, WarpGroup>(p, m, beg, c, p.tile_job[t]);
     __syncwarp();
+    j = __shfl_sync(0xFFFFFFFFu, jn, 0);
   }
 }
 
@@ -1385,8 +1387,8 @@ __global__ void k_head_len(uint32_t S, const uint32_t* __restrict__ seg_len, con
 
 // Copy each segment's chars into its line.  A warp takes 32 consecutive
 // segments: each lane resolves one segment's source, destination and length
-// (independent loads, issued together), then the warp copies the 32
-// segments one after another, 32 bytes per step.
+// (independent loads, issued together), then the warp copies the segments,
+// a group of four at a time, 32 bytes per step.
 __global__ void __launch_bounds__(256) k_seg_copy(
     uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
     const JobTab* __restrict__ jobs, const unsigned long long* __restrict__ jclosed,
@@ -1415,14 +1417,36 @@ __global__ void __launch_bounds__(256) k_seg_copy(
     }
     uint32_t todo = __ballot_sync(0xFFFFFFFFu, live);
     while (todo) {
-      const int q = __ffs(todo) - 1;
-      todo &= todo - 1;
-      const uint64_t d = __shfl_sync(0xFFFFFFFFu, dst, q);
-      const uint64_t c = __shfl_sync(0xFFFFFFFFu, src, q);
-      const uint32_t m = __shfl_sync(0xFFFFFFFFu, nb, q);
-      const uint32_t e = __shfl_sync(0xFFFFFFFFu, last, q);
-      for (uint32_t j = lane; j < m; j += 32) out[d + j] = segchars[c + j];
-      if (lane == 0 && e) out[d + m] = '\n';
+      // SG segments at a time: the first 64 bytes of each are loaded before
+      // any of them is stored, so the warp waits for one round trip per
+      // group instead of one per segment
+      constexpr int SG = 4;
+      uint64_t d[SG], c[SG];
+      uint32_t m[SG], e[SG];
+      char v[SG][2];
+#pragma unroll
+      for (int u = 0; u < SG; ++u) {
+        const int q = todo ? __ffs(todo) - 1 : 0;  // warp-uniform
+        const bool has = todo != 0;
+        todo &= todo - 1;
+        d[u] = __shfl_sync(0xFFFFFFFFu, dst, q);
+        c[u] = __shfl_sync(0xFFFFFFFFu, src, q);
+        m[u] = __shfl_sync(0xFFFFFFFFu, nb, q);
+        e[u] = __shfl_sync(0xFFFFFFFFu, last, q);
+        if (!has) m[u] = e[u] = 0;
+      }
+#pragma unroll
+      for (int u = 0; u < SG; ++u) {
+        v[u][0] = (uint32_t(lane) < m[u]) ? segchars[c[u] + lane] : 0;
+        v[u][1] = (uint32_t(lane) + 32u < m[u]) ? segchars[c[u] + lane + 32] : 0;
+      }
+#pragma unroll
+      for (int u = 0; u < SG; ++u) {
+        if (uint32_t(lane) < m[u]) out[d[u] + lane] = v[u][0];
+        if (uint32_t(lane) + 32u < m[u]) out[d[u] + lane + 32] = v[u][1];
+        for (uint32_t j = lane + 64; j < m[u]; j += 32) out[d[u] + j] = segchars[c[u] + j];
+        if (lane == 0 && e[u]) out[d[u] + m[u]] = '\n';
+      }
     }
   }
 }
