@@ -204,6 +204,21 @@ def test_sorted_output_is_byte_exact(comp, oracle, texts, cfg):
     assert b == expect and h == expect and u == expect
 
 
+@pytest.mark.parametrize("cfg", ["small_plain", "wide_k63", "k47"])
+@pytest.mark.parametrize("shift", [1, 2, 3])
+def test_output_buffer_at_any_byte(comp, oracle, texts, cfg, shift):
+    """An output buffer that starts at any byte gets the same lines: the
+    cross-tile copy stores aligned words in the middle of each segment and
+    single bytes at its ends."""
+    text, k = texts[cfg]
+    want = sorted_lines(oracle.compact(text, k)[0])
+    buf = torch.full((comp.output_bound(len(text), k) + 16,), 0x55, dtype=torch.uint8, device="cuda")
+    got = comp.compact(dev(text), k, min(8, k - 1), out=buf[shift:])
+    nb = got.numel()
+    assert sorted_lines(got.cpu().numpy().tobytes()) == want
+    assert bool((buf[:shift] == 0x55).all()) and bool((buf[shift + nb:] == 0x55).all())
+
+
 def test_sorted_output_cli(comp, oracle, texts, tmp_path):
     import subprocess
     from unitigcoarsening_b200 import build as B

@@ -1270,10 +1270,15 @@ __global__ void __launch_bounds__(256) k_seg_link(uint32_t S, const uint32_t* __
       const uint64_t i = b0 + uint64_t(q) * B + threadIdx.x;
       const bool in = i < S;
       sid[q] = in ? uint32_t(i) : NONE;
+      // the three slot loads are issued together; an unused slot's ends are
+      // not used
       len[q] = in ? seg_len[i] : 0u;
-      ex[q] = (in && len[q]) ? seg_ex[i] : NONE;
-      sx[q] = (in && len[q]) ? seg_sx[i] : NONE;
+      ex[q] = in ? seg_ex[i] : NONE;
+      sx[q] = in ? seg_sx[i] : NONE;
     }
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+      if (!len[q]) ex[q] = sx[q] = NONE;
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
       nx[q] = (ex[q] == NONE) ? NONE : start_seg[ex[q]];
@@ -1371,24 +1376,28 @@ __global__ void k_chain_len(uint32_t S, const uint32_t* __restrict__ seg_len, co
                             const uint32_t* __restrict__ next, const uint32_t* __restrict__ w,
                             const uint8_t* __restrict__ oncycle, uint32_t* __restrict__ linelen) {
   for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
-    if (seg_len[s] && next[s] == NONE && !oncycle[s]) {
-      const unsigned long long v = X[s];
-      linelen[ptr_of(v)] = pk_o(v) + w[s] + 1u;
-    }
+    // every per-slot load is issued before any test
+    const uint32_t len = seg_len[s], nx = next[s], ws = w[s];
+    const uint8_t cyc = oncycle[s];
+    const unsigned long long v = X[s];
+    if (len && nx == NONE && !cyc) linelen[ptr_of(v)] = pk_o(v) + ws + 1u;
   }
 }
 
 __global__ void k_head_len(uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ prev,
                            const uint8_t* __restrict__ oncycle, const uint32_t* __restrict__ linelen,
                            uint32_t* __restrict__ v) {
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x)
-    v[s] = (seg_len[s] && prev[s] == NONE && !oncycle[s]) ? linelen[s] : 0u;
+  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
+    const uint32_t len = seg_len[s], pv = prev[s], ll = linelen[s];  // issued together
+    const uint8_t cyc = oncycle[s];
+    v[s] = (len && pv == NONE && !cyc) ? ll : 0u;
+  }
 }
 
 // Copy each segment's chars into its line.  A warp takes 32 consecutive
 // segments: each lane resolves one segment's source, destination and length
-// (independent loads, issued together), then the warp copies the segments,
-// a group of four at a time, 32 bytes per step.
+// (independent loads, issued together), then groups of 8 lanes copy the
+// segments word by word.
 __global__ void __launch_bounds__(256) k_seg_copy(
     uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
     const JobTab* __restrict__ jobs, const unsigned long long* __restrict__ jclosed,
@@ -1404,49 +1413,54 @@ __global__ void __launch_bounds__(256) k_seg_copy(
     bool live = s < S;
     uint64_t dst = 0, src = 0;
     uint32_t nb = 0, last = 0;
-    if (live) live = seg_len[s] != 0 && !oncycle[s];
     if (live) {
+      // every per-slot load is issued before the test; the gathers that
+      // depend on them only for live segments
+      const uint32_t len = seg_len[s], job = seg_job[s], pv = prev[s], ws = w[s], nx = next[s];
+      const uint8_t cyc = oncycle[s];
       const unsigned long long v = X[s];
-      const uint32_t job = seg_job[s];
-      const uint64_t obase = jobs[job].obase;
-      const uint32_t sb = jobs[job].seg_base;
-      dst = obase + jclosed[job] + (loff[ptr_of(v)] - loff[sb]) + pk_o(v);
-      src = seg_off[s] + ((prev[s] == NONE) ? 0u : uint32_t(k));
-      nb = w[s];
-      last = next[s] == NONE;
+      const unsigned long long so = seg_off[s];
+      live = len != 0 && !cyc;
+      if (live) {
+        const uint64_t obase = jobs[job].obase;
+        const uint32_t sb = jobs[job].seg_base;
+        dst = obase + jclosed[job] + (loff[ptr_of(v)] - loff[sb]) + pk_o(v);
+        src = so + ((pv == NONE) ? 0u : uint32_t(k));
+        nb = ws;
+        last = nx == NONE;
+      }
     }
-    uint32_t todo = __ballot_sync(0xFFFFFFFFu, live);
-    while (todo) {
-      // SG segments at a time: the first 64 bytes of each are loaded before
-      // any of them is stored, so the warp waits for one round trip per
-      // group instead of one per segment
-      constexpr int SG = 4;
-      uint64_t d[SG], c[SG];
-      uint32_t m[SG], e[SG];
-      char v[SG][2];
-#pragma unroll
-      for (int u = 0; u < SG; ++u) {
-        const int q = todo ? __ffs(todo) - 1 : 0;  // warp-uniform
-        const bool has = todo != 0;
-        todo &= todo - 1;
-        d[u] = __shfl_sync(0xFFFFFFFFu, dst, q);
-        c[u] = __shfl_sync(0xFFFFFFFFu, src, q);
-        m[u] = __shfl_sync(0xFFFFFFFFu, nb, q);
-        e[u] = __shfl_sync(0xFFFFFFFFu, last, q);
-        if (!has) m[u] = e[u] = 0;
+    // groups of 8 lanes: group g copies, one after another, the segments
+    // resolved by its own 8 lanes.  Each lane of the group stores aligned
+    // 4-byte words of the destination, funnel-shifted from the two aligned
+    // source words that hold them; the up to 3 bytes before the first
+    // aligned word and after the last one go byte by byte.  Source words
+    // are read only where they hold a byte of the segment, so they stay in
+    // the segment chars' allocation.
+    const uint32_t gl = uint32_t(lane) & 7u;
+#pragma unroll 1
+    for (int i = 0; i < 8; ++i) {
+      const uint64_t d = __shfl_sync(0xFFFFFFFFu, dst, i, 8);
+      const uint64_t c = __shfl_sync(0xFFFFFFFFu, src, i, 8);
+      const uint32_t m = __shfl_sync(0xFFFFFFFFu, nb, i, 8);
+      const uint32_t e = __shfl_sync(0xFFFFFFFFu, last, i, 8);
+      // bytes before the first aligned word of the destination (the output
+      // buffer itself may start at any byte)
+      const uint32_t hb = min((4u - uint32_t(reinterpret_cast<uintptr_t>(out + d) & 3u)) & 3u, m);
+      const uint32_t nbody = (m - hb) >> 2;
+      const uint32_t tb = (m - hb) & 3u;
+      const char* sp = segchars + c + hb;
+      char* dp = out + d + hb;
+      const uint32_t sh = 8u * uint32_t(reinterpret_cast<uintptr_t>(sp) & 3u);
+      const uint32_t* sw = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(sp) & ~uintptr_t(3));
+      for (uint32_t wi = gl; wi < nbody; wi += 8) {
+        const uint32_t w0 = sw[wi];
+        const uint32_t v = sh ? __funnelshift_r(w0, sw[wi + 1], sh) : w0;
+        reinterpret_cast<uint32_t*>(dp)[wi] = v;
       }
-#pragma unroll
-      for (int u = 0; u < SG; ++u) {
-        v[u][0] = (uint32_t(lane) < m[u]) ? segchars[c[u] + lane] : 0;
-        v[u][1] = (uint32_t(lane) + 32u < m[u]) ? segchars[c[u] + lane + 32] : 0;
-      }
-#pragma unroll
-      for (int u = 0; u < SG; ++u) {
-        if (uint32_t(lane) < m[u]) out[d[u] + lane] = v[u][0];
-        if (uint32_t(lane) + 32u < m[u]) out[d[u] + lane + 32] = v[u][1];
-        for (uint32_t j = lane + 64; j < m[u]; j += 32) out[d[u] + j] = segchars[c[u] + j];
-        if (lane == 0 && e[u]) out[d[u] + m[u]] = '\n';
-      }
+      if (gl < hb) out[d + gl] = segchars[c + gl];
+      if (gl >= 4 && gl - 4 < tb) dp[4 * nbody + (gl - 4)] = sp[4 * nbody + (gl - 4)];
+      if (gl == 7 && e) out[d + m] = '\n';
     }
   }
 }
