@@ -869,17 +869,22 @@ struct WarpGroup {
   static __device__ __forceinline__ uint32_t size() { return 32u; }
   static __device__ __forceinline__ void sync() { __syncwarp(); }
   static __device__ __forceinline__ int sync_or(int v) { return __any_sync(0xFFFFFFFFu, v); }
+  // a warp tile's totals fit 32 bits (at most 256 copies)
   static __device__ __forceinline__ U3 scan3(U3 v, U3* total) {
     const int lane = threadIdx.x & 31;
-    U3 inc = v;
+    uint32_t a = uint32_t(v.a), b = uint32_t(v.b), c = uint32_t(v.c);
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const U3 t = u3_shfl_up(inc, o);
-      if (lane >= o) inc = u3_add(inc, t);
+      const uint32_t ta = __shfl_up_sync(0xFFFFFFFFu, a, o), tb = __shfl_up_sync(0xFFFFFFFFu, b, o),
+                     tc = __shfl_up_sync(0xFFFFFFFFu, c, o);
+      if (lane >= o) {
+        a += ta;
+        b += tb;
+        c += tc;
+      }
     }
-    *total = U3{__shfl_sync(0xFFFFFFFFu, inc.a, 31), __shfl_sync(0xFFFFFFFFu, inc.b, 31),
-                __shfl_sync(0xFFFFFFFFu, inc.c, 31)};
-    return U3{inc.a - v.a, inc.b - v.b, inc.c - v.c};
+    *total = U3{__shfl_sync(0xFFFFFFFFu, a, 31), __shfl_sync(0xFFFFFFFFu, b, 31), __shfl_sync(0xFFFFFFFFu, c, 31)};
+    return U3{a - uint32_t(v.a), b - uint32_t(v.b), c - uint32_t(v.c)};
   }
   static __device__ __forceinline__ bool reserve(const TileParams& p, uint32_t job, const U3& tot,
                                                  unsigned long long* base) {
@@ -1371,7 +1376,8 @@ __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restri
   }
 }
 
-// Line length of each chain, stored at its head.
+// Line length of each chain, stored at its head (every live chain has one
+// tail, which writes it; the array is zeroed before).
 __global__ void k_chain_len(uint32_t S, const uint32_t* __restrict__ seg_len, const unsigned long long* __restrict__ X,
                             const uint32_t* __restrict__ next, const uint32_t* __restrict__ w,
                             const uint8_t* __restrict__ oncycle, uint32_t* __restrict__ linelen) {
@@ -1381,16 +1387,6 @@ __global__ void k_chain_len(uint32_t S, const uint32_t* __restrict__ seg_len, co
     const uint8_t cyc = oncycle[s];
     const unsigned long long v = X[s];
     if (len && nx == NONE && !cyc) linelen[ptr_of(v)] = pk_o(v) + ws + 1u;
-  }
-}
-
-__global__ void k_head_len(uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ prev,
-                           const uint8_t* __restrict__ oncycle, const uint32_t* __restrict__ linelen,
-                           uint32_t* __restrict__ v) {
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
-    const uint32_t len = seg_len[s], pv = prev[s], ll = linelen[s];  // issued together
-    const uint8_t cyc = oncycle[s];
-    v[s] = (len && pv == NONE && !cyc) ? ll : 0u;
   }
 }
 
@@ -2824,7 +2820,7 @@ static size_t back_bytes(uint64_t copies, uint64_t X, uint64_t Sp, int nw, int k
   add((X + 1) * 4); add((X + 1) * 4);                                     // start_seg, end_seg
   add(segchars);
   add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // next, prev, w, act0, act1
-  add(Sp * 4); add(Sp * 4); add(Sp * 8); add((Sp + 1) * 8); add(Sp);     // llen, hlen, X, loff, oncyc
+  add(Sp * 4); add(Sp * 8); add((Sp + 1) * 8); add(Sp);                  // hlen, X, loff, oncyc
   add(scan_tmp_elems(Sp) * 8); add(R * 4);
   if (want_hec) add(hec_bytes(Sp, hec_rounds(Sp)));
   return back;
@@ -2990,7 +2986,6 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   uint32_t* wgt = T32(Sp);
   uint32_t* act0 = T32(Sp);
   uint32_t* act1 = T32(Sp);
-  uint32_t* llen = T32(Sp);
   uint32_t* hlen = T32(Sp);
   unsigned long long* Xr = T64(Sp);
   unsigned long long* loff = T64(Sp + 1);
@@ -3090,9 +3085,10 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     if (r) return r;
     if (rl) return rl;
   }
-  e.launches += 2 + 6 + 2;
-  k_chain_len<<<gs, 256, 0, e.stream>>>(S, seg_len, Xr, next, wgt, oncyc, llen);
-  k_head_len<<<gs, 256, 0, e.stream>>>(S, seg_len, prev, oncyc, llen, hlen);
+  e.launches += 1 + 6 + 2;
+  // line length at each head, 0 at every other slot
+  UC_CK(cudaMemsetAsync(hlen, 0, size_t(S) * 4, e.stream));
+  k_chain_len<<<gs, 256, 0, e.stream>>>(S, seg_len, Xr, next, wgt, oncyc, hlen);
   scan_excl<uint32_t, unsigned long long>(hlen, S, loff, stmp, e.stream);
   k_seg_copy<<<grid_for(e, S, 256), 256, 0, e.stream>>>(S, seg_len, seg_job, jd.tab, jd.jclosed, Xr,
                                                                         next, prev, wgt, oncyc, seg_off, loff, segc,
