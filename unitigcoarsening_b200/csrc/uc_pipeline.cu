@@ -457,20 +457,24 @@ __global__ void __launch_bounds__(256) k_lmin_count(const uint64_t* __restrict__
 
 // ============================================================ tile planning
 
-// A bucket starts a new tile when its offset enters a new window of `win`
-// copies, or when it or its predecessor is larger than `small` (such buckets
-// sit alone).  Every packed tile then holds < win + small <= capacity copies.
-__global__ void k_tile_flags(const uint32_t* __restrict__ counts, const unsigned long long* __restrict__ off,
-                             uint32_t m, uint32_t win, uint32_t small, uint32_t jb, uint32_t* __restrict__ flag) {
-  for (uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < m; b += gridDim.x * blockDim.x) {
-    uint32_t f = (b == 0);
-    if (b > 0) {
-      f |= (off[b] / win) != (off[b - 1] / win);
-      f |= counts[b] > small;
-      f |= counts[b - 1] > small;
-      f |= (b >> jb) != ((b - 1) >> jb);  // tiles never mix jobs
+// Tiles pack consecutive whole buckets, next fit: each thread walks a run of
+// TF_RUN buckets and starts a new tile at the run's first bucket, at a job's
+// first bucket, and wherever the next bucket would take the tile past
+// `cap` copies.  A tile of several buckets therefore holds at most `cap`
+// copies; a bucket larger than `cap` sits alone.
+constexpr uint32_t TF_RUN = 512;
+__global__ void k_tile_flags(const uint32_t* __restrict__ counts, uint32_t m, uint32_t cap, uint32_t jb,
+                             uint32_t* __restrict__ flag) {
+  const uint32_t nruns = (m + TF_RUN - 1) / TF_RUN;
+  for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nruns; r += gridDim.x * blockDim.x) {
+    const uint32_t b0 = r * TF_RUN, b1 = min(m, b0 + TF_RUN);
+    uint32_t run = 0;
+    for (uint32_t b = b0; b < b1; ++b) {
+      const uint32_t c = counts[b];
+      const bool f = (b == b0) || ((b >> jb) != ((b - 1) >> jb)) || (run + c > cap);
+      flag[b] = f;
+      run = f ? c : run + c;
     }
-    flag[b] = f;
   }
 }
 
@@ -2175,7 +2179,7 @@ int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
 // sizes jb, and njobs << jb buckets in all (rounded up to a power of two,
 // bits = log2 of that).
 struct Plan {
-  uint32_t bits, jb, cap, win, small, tslots, wcap, wts, wbytes, lf;
+  uint32_t bits, jb, cap, pack, tslots, wcap, wts, wbytes, lf;
   int l_used;
   uint64_t M;
 };
@@ -2218,8 +2222,7 @@ static Plan plan_buckets(const Env& e, uint64_t nmax, uint32_t njobs, int k, int
   P.jb = jb;
   P.bits = ceil_log2(uint64_t(njobs) << jb);
   P.cap = cap;
-  P.win = pack_cap - pack_cap / 4;
-  P.small = pack_cap / 4;
+  P.pack = pack_cap;
   P.tslots = ts;
   P.wcap = warp_tier ? wcap : 0;
   uint32_t wts = warp_tier ? big_slots(wcap, lf) : 0;
@@ -2314,7 +2317,8 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
   const uint64_t M = P.M;
   const int gm = grid_for(e, M, 256);
   e.launches += 2 + 6;
-  k_tile_flags<<<gm, 256, 0, e.stream>>>(f.counts, f.boff, uint32_t(M), P.win, P.small, P.jb, f.flag);
+  k_tile_flags<<<grid_for(e, (M + TF_RUN - 1) / TF_RUN, 256), 256, 0, e.stream>>>(f.counts, uint32_t(M), P.pack, P.jb,
+                                                                                 f.flag);
   scan_excl<uint32_t, uint32_t>(f.flag, M, f.fidx, reinterpret_cast<uint32_t*>(f.scan_tmp), e.stream);
   k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), P.jb, f.tile_begin, f.tile_job, e.ctr);
   UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
