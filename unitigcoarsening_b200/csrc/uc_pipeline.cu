@@ -458,22 +458,50 @@ __global__ void __launch_bounds__(256) k_lmin_count(const uint64_t* __restrict__
 // ============================================================ tile planning
 
 // Tiles pack consecutive whole buckets, next fit: each thread walks a run of
-// TF_RUN buckets and starts a new tile at the run's first bucket, at a job's
-// first bucket, and wherever the next bucket would take the tile past
-// `cap` copies.  A tile of several buckets therefore holds at most `cap`
-// copies; a bucket larger than `cap` sits alone.
-constexpr uint32_t TF_RUN = 512;
+// `runlen` buckets (a multiple of 16) and starts a new tile at the run's
+// first bucket, at a job's first bucket, and wherever the next bucket would
+// take the tile past `cap` copies.  A tile of several buckets therefore
+// holds at most `cap` copies; a bucket larger than `cap` sits alone.  Counts
+// and flags move 16 at a time (the arrays start 256-byte aligned).
 __global__ void k_tile_flags(const uint32_t* __restrict__ counts, uint32_t m, uint32_t cap, uint32_t jb,
-                             uint32_t* __restrict__ flag) {
-  const uint32_t nruns = (m + TF_RUN - 1) / TF_RUN;
+                             uint32_t runlen, uint32_t* __restrict__ flag) {
+  const uint32_t nruns = (m + runlen - 1) / runlen;
   for (uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < nruns; r += gridDim.x * blockDim.x) {
-    const uint32_t b0 = r * TF_RUN, b1 = min(m, b0 + TF_RUN);
+    const uint32_t b0 = r * runlen, b1 = min(m, b0 + runlen);
     uint32_t run = 0;
-    for (uint32_t b = b0; b < b1; ++b) {
-      const uint32_t c = counts[b];
-      const bool f = (b == b0) || ((b >> jb) != ((b - 1) >> jb)) || (run + c > cap);
-      flag[b] = f;
-      run = f ? c : run + c;
+    for (uint32_t c0 = b0; c0 < b1; c0 += 16) {
+      const bool full = c0 + 16 <= b1;
+      uint32_t c[16], f[16];
+      if (full) {
+        const uint4* src = reinterpret_cast<const uint4*>(counts + c0);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+          const uint4 x = src[v];
+          c[4 * v] = x.x;
+          c[4 * v + 1] = x.y;
+          c[4 * v + 2] = x.z;
+          c[4 * v + 3] = x.w;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) c[q] = (c0 + q < b1) ? counts[c0 + q] : 0u;
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const uint32_t b = c0 + uint32_t(q);
+        const bool st = (b == b0) || ((b >> jb) != ((b - 1) >> jb)) || (run + c[q] > cap);
+        f[q] = st;
+        run = st ? c[q] : run + c[q];
+      }
+      if (full) {
+        uint4* dst = reinterpret_cast<uint4*>(flag + c0);
+#pragma unroll
+        for (int v = 0; v < 4; ++v) dst[v] = make_uint4(f[4 * v], f[4 * v + 1], f[4 * v + 2], f[4 * v + 3]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q)
+          if (c0 + q < b1) flag[c0 + q] = f[q];
+      }
     }
   }
 }
@@ -2317,8 +2345,14 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
   const uint64_t M = P.M;
   const int gm = grid_for(e, M, 256);
   e.launches += 2 + 6;
-  k_tile_flags<<<grid_for(e, (M + TF_RUN - 1) / TF_RUN, 256), 256, 0, e.stream>>>(f.counts, uint32_t(M), P.pack, P.jb,
-                                                                                 f.flag);
+  {
+    // about 256 threads per SM; each run ends a tile, so runs stay long
+    // where there are enough buckets
+    const uint64_t want = (M + uint64_t(e.sm_count) * 256 - 1) / (uint64_t(e.sm_count) * 256);
+    const uint32_t runlen = uint32_t(std::min<uint64_t>(512, std::max<uint64_t>(16, (want + 15) & ~uint64_t(15))));
+    k_tile_flags<<<grid_for(e, (M + runlen - 1) / runlen, 256), 256, 0, e.stream>>>(f.counts, uint32_t(M), P.pack,
+                                                                                     P.jb, runlen, f.flag);
+  }
   scan_excl<uint32_t, uint32_t>(f.flag, M, f.fidx, reinterpret_cast<uint32_t*>(f.scan_tmp), e.stream);
   k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), P.jb, f.tile_begin, f.tile_job, e.ctr);
   UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
