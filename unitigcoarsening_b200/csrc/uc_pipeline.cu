@@ -1413,12 +1413,25 @@ __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restri
 __global__ void k_chain_len(uint32_t S, const uint32_t* __restrict__ seg_len, const unsigned long long* __restrict__ X,
                             const uint32_t* __restrict__ next, const uint32_t* __restrict__ w,
                             const uint8_t* __restrict__ oncycle, uint32_t* __restrict__ linelen) {
-  for (uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < S; s += gridDim.x * blockDim.x) {
-    // every per-slot load is issued before any test
-    const uint32_t len = seg_len[s], nx = next[s], ws = w[s];
-    const uint8_t cyc = oncycle[s];
-    const unsigned long long v = X[s];
-    if (len && nx == NONE && !cyc) linelen[ptr_of(v)] = pk_o(v) + ws + 1u;
+  constexpr int PER = 4;  // slots per thread and pass: their loads are in flight together
+  const uint64_t span = uint64_t(gridDim.x) * blockDim.x;
+  for (uint64_t s0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s0 < S; s0 += span * PER) {
+    uint32_t len[PER], nx[PER], ws[PER];
+    uint8_t cyc[PER];
+    unsigned long long v[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const uint64_t s = s0 + uint64_t(q) * span;
+      const bool in = s < S;
+      len[q] = in ? seg_len[s] : 0u;
+      nx[q] = in ? next[s] : NONE;
+      ws[q] = in ? w[s] : 0u;
+      cyc[q] = in ? oncycle[s] : uint8_t(1);
+      v[q] = in ? X[s] : 0ull;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+      if (len[q] && nx[q] == NONE && !cyc[q]) linelen[ptr_of(v[q])] = pk_o(v[q]) + ws[q] + 1u;
   }
 }
 
