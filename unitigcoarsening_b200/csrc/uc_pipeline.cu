@@ -569,7 +569,15 @@ __global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Co
 // every block taking the next chunk from a shared counter, and places each
 // record with its bucket's cursor.  All blocks therefore write into the same
 // one or two partitions at any time.
-constexpr int SC_CHUNK = 2048;   // k-mers per level-1 block pass (<= 4096 copies)
+// k-mers per level-1 block pass (at most twice as many copies): large chunks
+// spread the per-chunk reservations and barriers over more copies; 3072
+// 64-bit keys (100 KB of staging, 2 CTAs per SM) beat 2048 (3 CTAs per SM)
+// by 6% at 1 Gbp, and 128-bit keys keep 2048 (98 KB)
+template <int NW>
+__host__ __device__ constexpr int sc_chunk() {
+  return NW == 1 ? 3072 : 2048;
+}
+static_assert(2 * sc_chunk<1>() < 65536 && 2 * sc_chunk<2>() < 65536, "chunk copy counts share a 32-bit scan");
 constexpr int SC_FINE = 4096;    // staged records per level-2 work item
 
 __global__ void k_coarse_init(const unsigned long long* __restrict__ boff, uint32_t fb, uint32_t mc,
@@ -588,6 +596,7 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
                                                         uint32_t* __restrict__ rbkt, int ids_mode, Counters* ctr) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);                         // [2*CHUNK*NW]
+  constexpr int SC_CHUNK = sc_chunk<NW>();
   uint32_t* slink = reinterpret_cast<uint32_t*>(skey + 2 * SC_CHUNK * NW);      // [2*CHUNK]
   uint32_t* sbkt = slink + 2 * SC_CHUNK;                                        // [2*CHUNK]
   unsigned long long* gbase = reinterpret_cast<unsigned long long*>(sbkt + 2 * SC_CHUNK);  // [mc]
@@ -627,8 +636,8 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
     __syncthreads();
     // local offsets (scan over the partitions), this thread's first cross
     // index within the chunk, and global reservations.  One scan carries both
-    // sums: the copy count in the low half (<= 4096) and the cross count in
-    // the high half (<= 2048).  The chunk's cross indices are reserved with a
+    // sums: the copy count in the low half (<= 2 * chunk < 2^16) and the
+    // cross count in the high half (<= chunk).  The chunk's cross indices are reserved with a
     // single atomic: a counter shared by every block of the grid serialises
     // in L2, so one reservation per warp and k-mer slot would bound the kernel.
     uint32_t xpre;
@@ -2378,7 +2387,8 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
     uint32_t* rbkt = rlink + copies;
     e.launches += 1;
     k_coarse_init<<<grid_for(e, mc, 256), 256, 0, e.stream>>>(f.boff, fb, mc, f.cursor);
-    const size_t sm1 = size_t(2 * SC_CHUNK) * (8 * nw + 8) + size_t(mc) * 16 + 16;
+    const uint64_t chunk = (nw == 1) ? sc_chunk<1>() : sc_chunk<2>();
+    const size_t sm1 = size_t(2 * chunk) * (8 * nw + 8) + size_t(mc) * 16 + 16;
     int r0 = allow_max_smem(e, k_scatter_coarse<1>);
     if (!r0) r0 = allow_max_smem(e, k_scatter_coarse<2>);
     if (r0) return r0;
@@ -2387,7 +2397,7 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
     if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<1>, 256, sm1));
     else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<2>, 256, sm1));
     if (o1 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
-    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + SC_CHUNK - 1) / SC_CHUNK,
+    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + chunk - 1) / chunk,
                                                                 uint64_t(e.sm_count) * uint64_t(o1))));
     UC_CK(cudaMemcpyAsync(f.fcur, f.boff, M * 8, cudaMemcpyDeviceToDevice, e.stream));
     UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
