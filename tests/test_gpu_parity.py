@@ -249,6 +249,16 @@ def test_host_many_overlapped_uploads(comp, oracle, texts):
     one = torch.empty(max(o.numel() for o in outs), dtype=torch.uint8)
     shared = comp.compact_host_many([t for t, _ in seq], k, 8, outs=[one] * len(seq))
     assert sorted_lines(bytes(shared[-1].numpy())) == want[-1]
+    # the largest job first and none larger after it, twice in a row on the
+    # same context
+    order = sorted(range(len(seq)), key=lambda i: -len(seq[i][0]))
+    seq2 = [seq[i] for i in order] + [seq[order[0]]]
+    want2 = [want[i] for i in order] + [want[order[0]]]
+    for _ in range(2):
+        outs2 = [torch.empty(comp.output_bound(len(t), k), dtype=torch.uint8) for t, _ in seq2]
+        res2 = comp.compact_host_many([t for t, _ in seq2], k, 8, outs=outs2)
+        for r, w in zip(res2, want2):
+            assert sorted_lines(bytes(r.numpy())) == w
 
 
 def _golden():
