@@ -131,16 +131,60 @@ def traffic_per_copy(kernel: str):
     return None
 
 
+def lines_digest(buf) -> int:
+    """Order-independent digest of the '\\n'-terminated lines of a uint8
+    CUDA tensor: every byte weighted by a mix of its position in its line,
+    summed per line, each line's sum mixed, and the mixes summed (mod 2^64).
+    Equal multisets of lines give equal digests whatever their order, so a
+    job's lines from the batched path and from the plain path compare
+    without sorting; a line split, merged or changed changes it."""
+    import torch
+    from unitigcoarsening_b200 import synth
+    n = buf.numel()
+    if n == 0:
+        return 0
+    nl = buf == 10
+    ends = torch.nonzero(nl).flatten()
+    starts = torch.cat([torch.zeros(1, dtype=ends.dtype, device=buf.device), ends[:-1] + 1])
+    line = torch.cumsum(nl.to(torch.int64), 0) - nl.to(torch.int64)
+    if int(line[-1]) >= ends.numel():  # bytes after the last newline form a line of their own
+        starts = torch.cat([starts, (ends[-1:] + 1) if ends.numel() else starts[:1]])
+    rel = torch.arange(n, device=buf.device, dtype=torch.int64) - starts[line]
+    v = (buf.to(torch.int64) + 1) * synth._mix(rel * -7046029254386353131 + 0x632BE59BD9B4E019)
+    per = torch.zeros(starts.numel(), dtype=torch.int64, device=buf.device).index_add_(0, line, v)
+    return int(synth._mix(per).sum().item()) & ((1 << 64) - 1)
+
+
+def cpu_model() -> str:
+    """lscpu's model name of the host cores (or /proc/cpuinfo's)."""
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for ln in out.splitlines():
+            if ln.startswith("Model name:"):
+                return ln.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("model name"):
+                return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "uc_ref_large")
 
 
-def _cpu_sample(args):
-    """Bounded sample of the workload: the same genome model, shorter."""
+def _cpu_sample(args, spec=None, k=None):
+    """Bounded sample of the workload: the same genome model, shorter (or
+    the given spec)."""
     import torch
     from unitigcoarsening_b200 import synth
-    spec = synth.scale_plain(length=int(args.cpu_sample), seed=2)
+    if spec is None:
+        spec = synth.scale_plain(length=int(args.cpu_sample), seed=2)
     with torch.no_grad():
-        return synth.make_text(spec, args.k, device="cpu").numpy().tobytes()
+        return synth.make_text(spec, k or args.k, device="cpu").numpy().tobytes()
 
 
 def _run_reference_binary(text: bytes, k: int, l: int, threads: int):
@@ -165,10 +209,13 @@ def _run_reference_binary(text: bytes, k: int, l: int, threads: int):
         return (float(m.group(1)) if m else wall), wall
 
 
-def cpu_baseline(args, steps: int = 1):
+def cpu_baseline(args, steps: int = 1, text: bytes | None = None, sample: str | None = None):
     """Reference CPU path (or, without its binary, the oracle port) timed on
     the host over a bounded sample; returns the cpu_baseline object."""
-    text = _cpu_sample(args)
+    if text is None:
+        text = _cpu_sample(args)
+        sample = (f"{args.cpu_sample / 1e6:g} Mbp genome of the same model (seed 2), {{n}} k-mers, "
+                  f"k={args.k}, l={args.l}, text in a file, lines to a file")
     n = int(text[: text.index(b"\n")])
     if os.path.exists(REF_BIN):
         threads = os.cpu_count() or 1
@@ -185,9 +232,8 @@ def cpu_baseline(args, steps: int = 1):
             ts.append(time.perf_counter() - t0)
         sec = sum(ts) / len(ts)
         kind, cores = "port", 1
-    return {"value": n / sec, "unit": UNIT, "cores": cores, "kind": kind, "seconds": sec,
-            "sample": f"{args.cpu_sample / 1e6:g} Mbp genome of the same model (seed 2), {n} k-mers, "
-                      f"k={args.k}, l={args.l}, text in a file, lines to a file"}
+    return {"value": n / sec, "unit": UNIT, "cores": cores, "kind": kind, "seconds": sec, "n_kmers": n,
+            "cpu_model": cpu_model(), "nproc": os.cpu_count(), "sample": sample.format(n=n)}
 
 
 def reference_throughput(args):
@@ -195,7 +241,10 @@ def reference_throughput(args):
         cpu_baseline(args, steps=1)
     cb = cpu_baseline(args, steps=max(1, args.steps))
     cfg = {"workload": f"plain single job (bounded CPU sample): {args.cpu_sample / 1e6:g} Mbp genome, 41% GC, "
-                       f"5% repeat families, 0.1% SNPs, k={args.k}", "k": args.k, "l": args.l}
+                       f"5% repeat families, 0.1% SNPs, k={args.k}", "k": args.k, "l": args.l,
+           "n_kmers": cb["n_kmers"],
+           "sample_of": f"the GPU arm's {args.genome / 1e9:g} Gbp job of the same model (~1.0B k-mers); "
+                        f"this arm times {cb['n_kmers']} k-mers of it per step"}
     return {"value": cb["value"], "ms_per_step": cb["seconds"] * 1e3, "config": cfg, "cpu_baseline": cb}
 
 
@@ -232,65 +281,86 @@ def replica_totals(ms: float, n: int, dist=None, device: str = "cuda"):
 
 def measure_batched(args, device: int):
     """Many small jobs (log-normal lengths, median 3 Mbp, 0.5-8 Mbp, GC
-    30-70%, 0.2% SNPs, k=31), device-resident: batched launches of
-    --batch-chunk jobs each (one tile queue per launch) against the plain
-    loop of one compaction per job, on a fresh context; each the mean of the
-    timed passes after warm-up."""
+    30-70%, 0.2% SNPs, k=31), device-resident.  The jobs are generated on
+    the GPU in chunks of --batch-gen-chunk (untimed; all 4096 texts would not
+    fit in HBM at once).  For each chunk, one timed pass of the plain loop
+    (one compaction per job) and one timed pass of the batched form
+    (--batch-chunk jobs per launch sequence, one tile queue each), then an
+    untimed check that every job's lines are the same in both (order-free
+    line digests).  Times are summed over the chunks."""
     import torch
     from unitigcoarsening_b200 import Compactor, synth
     comp = Compactor(device)
-    texts = []
-    with torch.no_grad():
-        for j in range(args.batch_jobs):
-            texts.append(synth.make_text(synth.batched_job(j, seed=4), 31, device="cuda"))
-    torch.cuda.synchronize()
-    caps = [comp.output_bound(t.numel(), 31) for t in texts]
-    one = torch.empty(max(caps), dtype=torch.uint8, device="cuda")  # the plain loop reuses one buffer
     C = max(1, args.batch_chunk)
-    chunks = [list(range(i, min(i + C, len(texts)))) for i in range(0, len(texts), C)]
-    bout = torch.empty(max(sum((caps[j] + 15) // 16 * 16 for j in ch) for ch in chunks) + 64, dtype=torch.uint8,
-                       device="cuda")
+    G = max(C, args.batch_gen_chunk // C * C)
     stream = torch.cuda.current_stream()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    plain_ms = batch_ms = gen_s = 0.0
+    n_total, launches, mismatched, warm = 0, 0, [], False
+    for g0 in range(0, args.batch_jobs, G):
+        ids = list(range(g0, min(args.batch_jobs, g0 + G)))
+        t0 = time.perf_counter()
+        with torch.no_grad():
+            texts = [synth.make_text(synth.batched_job(j, seed=4), 31, device="cuda") for j in ids]
+        torch.cuda.synchronize()
+        gen_s += time.perf_counter() - t0
+        caps = [comp.output_bound(t.numel(), 31) for t in texts]
+        one = torch.empty(max(caps), dtype=torch.uint8, device="cuda")  # the plain loop reuses one buffer
+        chunks = [list(range(i, min(i + C, len(texts)))) for i in range(0, len(texts), C)]
+        bout = torch.empty(max(sum((caps[j] + 15) // 16 * 16 for j in ch) for ch in chunks) + 64,
+                           dtype=torch.uint8, device="cuda")
 
-    def plain():
-        return [comp.compact(t, 31, args.l, out=one).numel() for t in texts]
+        def plain(check=None):
+            for i, t in enumerate(texts):
+                r = comp.compact(t, 31, args.l, out=one)
+                if check is not None:
+                    check.append(lines_digest(r))
 
-    def batched():
-        lens, n, launches = [], 0, 0
-        for ch in chunks:
-            res, st = comp.compact_batch([texts[j] for j in ch], 31, args.l, out=bout, stats=True)
-            lens += [r.numel() for r in res]
-            n += int(st["n_kmers"])
-            launches += int(st["launches"])
-        return lens, n, launches
+        def batched(check=None):
+            n, nl = 0, 0
+            for ch in chunks:
+                res, st = comp.compact_batch([texts[j] for j in ch], 31, args.l, out=bout, stats=True)
+                n += int(st["n_kmers"])
+                nl += int(st["launches"])
+                if check is not None:
+                    check += [lines_digest(r) for r in res]
+            return n, nl
 
-    for _ in range(2):
-        plain_len = plain()
-        batch_len, n, launches = batched()
-    reps = 2
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(reps):
+        if not warm:
+            plain()
+            batched()
+            warm = True
+        torch.cuda.synchronize()
+        e0.record(stream)
         plain()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    plain_ms = e0.elapsed_time(e1) / reps
-    e0.record(stream)
-    for _ in range(reps):
-        batched()
-    e1.record(stream)
-    torch.cuda.synchronize()
-    batch_ms = e0.elapsed_time(e1) / reps
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms += e0.elapsed_time(e1)
+        e0.record(stream)
+        n, nl = batched()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        batch_ms += e0.elapsed_time(e1)
+        n_total += n
+        launches += nl
+        dp, db = [], []
+        plain(dp)
+        batched(db)
+        mismatched += [ids[i] for i in range(len(ids)) if dp[i] != db[i]]
+        del texts, one, bout
+        torch.cuda.empty_cache()
     comp.close()
-    del texts, one, bout, comp
+    del comp
     torch.cuda.empty_cache()
     return {"workload": f"{args.batch_jobs} jobs: log-normal length (median 3 Mbp, 0.5-8 Mbp), GC 30-70%, "
-                        f"0.2% SNPs, k=31, device-resident; batched {C} jobs per launch sequence",
-            "jobs": args.batch_jobs, "n_kmers": n,
-            "batched": {"value": n / (batch_ms / 1e3), "ms": batch_ms, "launches": launches},
-            "plain": {"value": n / (plain_ms / 1e3), "ms": plain_ms},
-            "speedup": plain_ms / batch_ms, "out_bytes_equal": plain_len == batch_len, "unit": UNIT}
+                        f"0.2% SNPs, k=31, device-resident; batched {C} jobs per launch sequence; generated "
+                        f"{G} jobs at a time (untimed)",
+            "jobs": args.batch_jobs, "n_kmers": n_total,
+            "batched": {"value": n_total / (batch_ms / 1e3), "ms": batch_ms, "launches": launches},
+            "plain": {"value": n_total / (plain_ms / 1e3), "ms": plain_ms},
+            "speedup": plain_ms / batch_ms, "per_job_lines_equal": not mismatched,
+            "mismatched_jobs": mismatched[:16], "check": "order-free digest of each job's lines, plain vs batched",
+            "gen_seconds": gen_s, "unit": UNIT}
 
 
 def measure_configs(args, device: int):
@@ -322,8 +392,22 @@ def measure_configs(args, device: int):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / 3
         res[name] = {"value": st["n_kmers"] / (ms / 1e3), "unit": UNIT, "ms": ms, "n_kmers": int(st["n_kmers"]),
-                     "k": k, "text_bytes": int(text.numel()),
+                     "k": k, "l_used": int(st["l_used"]), "text_bytes": int(text.numel()),
                      "phase_ms": {p: round(st["ms_" + p], 3) for p in ("pack", "bucket", "tiles", "stitch")}}
+        if text.numel() < (1 << 30):
+            # host memory to host memory through uc_compact_host (pinned), the
+            # form comparable with the reference's file-to-file run
+            htext = torch.empty(text.numel(), dtype=torch.uint8, pin_memory=True)
+            htext.copy_(text)
+            hout = torch.empty(comp.output_bound(text.numel(), k), dtype=torch.uint8, pin_memory=True)
+            for _ in range(2):
+                comp.compact_host(htext, k, l, out=hout)
+            t0 = time.perf_counter()
+            for _ in range(5):
+                comp.compact_host(htext, k, l, out=hout)
+            hs = (time.perf_counter() - t0) / 5
+            res[name]["host_to_host"] = {"value": st["n_kmers"] / hs, "ms": hs * 1e3, "api": "uc_compact_host"}
+            del htext, hout
         comp.close()
         del comp, text, out
         torch.cuda.empty_cache()
@@ -333,80 +417,111 @@ def measure_configs(args, device: int):
 def measure_serving(args, device: int):
     """Serving loop: a pool of distinct jobs (k-mer counts log-uniform in
     [10k, 50M], k = 31 with p 0.7 else 63) in pinned host memory; capacity =
-    the plain sequential host-to-host path over the pool; then Poisson
+    the plain sequential host-to-host path over the pool.  Then (1) Poisson
     arrivals at 80% of that capacity, each a job drawn from the pool, served
-    by uc_server (footprint admission, batching, overlapping lanes)."""
+    by uc_server (footprint admission, batching, overlapping lanes), with
+    latency percentiles; (2) a saturation run: --serve-burst jobs submitted
+    at once, whose completion rate is the server's sustained capacity."""
+    import psutil
     import random
     import threading
     import torch
-    from unitigcoarsening_b200 import Compactor, Server, synth
-    pool = []
+    from unitigcoarsening_b200 import Compactor, Server, UCError, synth
+    pool, pool_bytes = [], 0
+    host_cap = psutil.virtual_memory().available // 3  # the pool, its outputs, and headroom
+    t0 = time.perf_counter()
     with torch.no_grad():
         for j in range(args.serve_pool):
             spec, k = synth.served_job(j, seed=5)
             t = synth.make_text(spec, k, device="cuda")
+            if pool and pool_bytes + t.numel() > host_cap:
+                break
             h = torch.empty(t.numel(), dtype=torch.uint8, pin_memory=True)
             h.copy_(t)
             del t
+            pool_bytes += h.numel()
             pool.append((h, k, int(bytes(h[:24].numpy()).split(b"\n")[0])))
+    gen_s = time.perf_counter() - t0
     torch.cuda.empty_cache()
     # capacity: plain sequential path, host text to host lines (pinned both
-    # ways, like the server's lanes)
+    # ways, like the server's lanes); one output buffer of the largest size
     comp = Compactor(device)
-    houts = [torch.empty(comp.output_bound(h.numel(), k), dtype=torch.uint8, pin_memory=True) for h, k, _ in pool]
+    hout = torch.empty(max(comp.output_bound(h.numel(), k) for h, k, _ in pool), dtype=torch.uint8,
+                       pin_memory=True)
     seq_s = 0.0
     for rep in range(2):
         t0 = time.perf_counter()
-        for (h, k, n), o in zip(pool, houts):
-            comp.compact_host(h, k, min(args.l, k - 1), out=o)
+        for h, k, n in pool:
+            comp.compact_host(h, k, min(args.l, k - 1), out=hout)
         if rep:
             seq_s = time.perf_counter() - t0
     comp.close()
-    del comp, houts
+    del comp, hout
     torch.cuda.empty_cache()
     pool_kmers = sum(n for _, _, n in pool)
     capacity = pool_kmers / seq_s
     mean_n = pool_kmers / len(pool)
+
+    def serve(arrivals):
+        results = [None] * len(arrivals)
+        with Server(device=device, lanes=4, max_batch=32) as srv:
+            tickets = [None] * len(arrivals)
+            ready = threading.Semaphore(0)
+
+            def waiter():
+                for i in range(len(arrivals)):
+                    ready.acquire()
+                    try:
+                        results[i] = srv.wait(tickets[i], timeout=600, fetch=False)[1]
+                    except UCError as ex:
+                        results[i] = {"status": ex.status, "latency_ms": 0.0}
+
+            wt = threading.Thread(target=waiter)
+            wt.start()
+            t0 = time.perf_counter()
+            for i, (ta, j) in enumerate(arrivals):
+                d = ta - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                h, k, _ = pool[j]
+                tickets[i] = srv.submit(h, k, min(args.l, k - 1))
+                ready.release()
+            wt.join()
+            wall = time.perf_counter() - t0
+            tot = srv.stats()
+        bad = sum(1 for r in results if r["status"] != 0)
+        served = sum(pool[j][2] for _, j in arrivals)
+        lat = sorted(r["latency_ms"] for r in results)
+        pct = lambda q: lat[min(len(lat) - 1, int(q * (len(lat) - 1) + 0.5))]
+        return {"jobs": len(arrivals), "n_kmers": served, "wall_s": wall,
+                "sustained": {"value": served / wall, "unit": UNIT}, "failed_jobs": bad,
+                "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": lat[-1], "mean": sum(lat) / len(lat)},
+                "batches": int(tot["batches"]), "batched_jobs": int(tot["batched_jobs"]),
+                "pool_gb": tot["pool_bytes"] / 1e9, "pool_peak_gb": tot["pool_peak_bytes"] / 1e9}
+
     rate = 0.8 * capacity / mean_n  # jobs per second
     rnd = random.Random(7)
     arrivals, t = [], 0.0
     for _ in range(args.serve_jobs):
         t += rnd.expovariate(rate)
         arrivals.append((t, rnd.randrange(len(pool))))
-    results = [None] * len(arrivals)
-    with Server(device=device, lanes=4, max_batch=32) as srv:
-        tickets = [None] * len(arrivals)
-        ready = threading.Semaphore(0)
-
-        def waiter():
-            for i in range(len(arrivals)):
-                ready.acquire()
-                results[i] = srv.wait(tickets[i], timeout=600, fetch=False)[1]
-
-        wt = threading.Thread(target=waiter)
-        wt.start()
-        t0 = time.perf_counter()
-        for i, (ta, j) in enumerate(arrivals):
-            d = ta - (time.perf_counter() - t0)
-            if d > 0:
-                time.sleep(d)
-            h, k, _ = pool[j]
-            tickets[i] = srv.submit(h, k, min(args.l, k - 1))
-            ready.release()
-        wt.join()
-        wall = time.perf_counter() - t0
-        tot = srv.stats()
-    served = sum(pool[j][2] for _, j in arrivals)
-    lat = sorted(r["latency_ms"] for r in results)
-    pct = lambda q: lat[min(len(lat) - 1, int(q * (len(lat) - 1) + 0.5))]
+    load = serve(arrivals)
+    sat = None
+    if args.serve_burst > 0:
+        rnd = random.Random(11)
+        sat = serve([(0.0, rnd.randrange(len(pool))) for _ in range(args.serve_burst)])
+        sat["offered"] = "all jobs submitted at once (offered load far above capacity)"
+        sat["vs_plain_sequential"] = sat["sustained"]["value"] / capacity
     return {"workload": f"Poisson arrivals at 80% of the plain sequential capacity; {args.serve_jobs} jobs drawn "
-                        f"from {len(pool)} distinct jobs, k-mer counts log-uniform in [10k, 50M], k = 31 (p 0.7) "
-                        f"or 63, host memory to host memory", "jobs": args.serve_jobs,
-            "offered_jobs_per_s": rate, "sustained": {"value": served / wall, "unit": UNIT},
-            "plain_sequential": {"value": capacity, "unit": UNIT},
-            "latency_ms": {"p50": pct(0.5), "p99": pct(0.99), "max": lat[-1], "mean": sum(lat) / len(lat)},
-            "batches": int(tot["batches"]), "batched_jobs": int(tot["batched_jobs"]),
-            "pool_gb": tot["pool_bytes"] / 1e9, "pool_peak_gb": tot["pool_peak_bytes"] / 1e9}
+                        f"from {len(pool)} distinct jobs ({pool_bytes / 1e9:.1f} GB of text in pinned host "
+                        f"memory), k-mer counts log-uniform in [10k, 50M], k = 31 (p 0.7) or 63, host memory to "
+                        f"host memory", "jobs": args.serve_jobs, "distinct_jobs": len(pool),
+            "offered_jobs_per_s": rate, "offered": {"value": 0.8 * capacity, "unit": UNIT},
+            "sustained": load["sustained"], "plain_sequential": {"value": capacity, "unit": UNIT},
+            "latency_ms": load["latency_ms"], "wall_s": load["wall_s"], "n_kmers": load["n_kmers"],
+            "failed_jobs": load["failed_jobs"], "batches": load["batches"], "batched_jobs": load["batched_jobs"],
+            "pool_gb": load["pool_gb"], "pool_peak_gb": load["pool_peak_gb"], "saturation": sat,
+            "gen_seconds": gen_s}
 
 
 def main():
@@ -422,13 +537,17 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-sample", type=float, default=4e6, help="genome length of the CPU sample")
+    ap.add_argument("--cpu-sample-large", type=float, default=16e6,
+                    help="genome length of the larger CPU sample (0: skip)")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner (library defaults)")
     ap.add_argument("--tune-sample", type=float, default=2e8, help="genome length the autotuner times")
-    ap.add_argument("--batch-jobs", type=int, default=256, help="jobs of the batched-vs-plain comparison (0: skip)")
+    ap.add_argument("--batch-jobs", type=int, default=4096, help="jobs of the batched-vs-plain comparison (0: skip)")
     ap.add_argument("--batch-chunk", type=int, default=64, help="jobs per batched launch sequence")
+    ap.add_argument("--batch-gen-chunk", type=int, default=512, help="jobs generated on the GPU at a time")
     ap.add_argument("--no-configs", action="store_true", help="skip the small and wide-k single-job shapes")
-    ap.add_argument("--serve-jobs", type=int, default=400, help="arrivals of the serving measurement (0: skip)")
-    ap.add_argument("--serve-pool", type=int, default=24, help="distinct jobs the arrivals draw from")
+    ap.add_argument("--serve-jobs", type=int, default=20000, help="arrivals of the serving measurement (0: skip)")
+    ap.add_argument("--serve-pool", type=int, default=256, help="distinct jobs the arrivals draw from")
+    ap.add_argument("--serve-burst", type=int, default=2000, help="jobs of the saturation run (0: skip)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -555,9 +674,24 @@ def main():
     configs = measure_configs(args, local) if not args.no_configs else None
     serving = measure_serving(args, local) if args.serve_jobs > 0 else None
 
-    cpu = None
+    cpu = cpu_pairs = None
     if rank == 0 and not args.no_cpu:
         cpu = cpu_baseline(args)
+        # the same configs on both sides: the small plain job exactly (the one
+        # the reference runs on its CPU path), and a larger sample of the
+        # headline model to show how the CPU rate moves with size
+        c1 = cpu_baseline(args, text=_cpu_sample(args, synth.small_plain(), 31),
+                          sample="small plain job: 1 Mbp uniform genome, 200 SNP bubbles, {n} k-mers, k=31, l=8")
+        cpu_pairs = {"small_plain_1Mbp_k31": {"cpu_reference": c1,
+                                              "gpu": (configs or {}).get("small_plain_1Mbp_k31"),
+                                              "same_config": True}}
+        if args.cpu_sample_large > 0:
+            big = cpu_baseline(args, text=_cpu_sample(args, synth.scale_plain(length=int(args.cpu_sample_large),
+                                                                              seed=2), args.k),
+                               sample=f"{args.cpu_sample_large / 1e6:g} Mbp genome of the headline model (seed 2), "
+                                      f"{{n}} k-mers, k={args.k}, l={args.l}")
+            cpu_pairs["scale_plain_sample"] = {"cpu_reference": big, "gpu": None, "same_config": False,
+                                               "note": "CPU rate at a larger sample of the headline model"}
 
     if rank == 0:
         line = {
@@ -566,6 +700,7 @@ def main():
             "vs_baseline": None, "dtype": "u8/u64 (2-bit packed keys, 32-bit ids)", "data": "synthetic",
             "config": {"workload": f"plain single job: {args.genome / 1e9:g} Gbp genome, 41% GC, 5% repeat "
                                    f"families, 0.1% SNPs, k={args.k}", "k": args.k, "l": args.l,
+                       "l_used": int(st["l_used"]),
                        "n_kmers": n, "text_bytes": text_bytes, "l2_flush": "inputs larger than L2",
                        "parallelism": f"replicas x{world}", "genome_seed": 2},
             "roofline": {"bound": "hbm", "kernel": "k_tile_warp + k_tile", "achieved": achieved, "peak": peak,
@@ -577,7 +712,7 @@ def main():
             "stats": {k2: (float(v) if isinstance(v, float) else int(v)) for k2, v in st.items()},
             "tuning": tuning,
             "batched_vs_plain": batched, "serving": serving, "other_configs": configs,
-            "e2e": e2e, "cpu_baseline": cpu, "clocks": clk.summary(),
+            "e2e": e2e, "cpu_baseline": cpu, "cpu_vs_gpu": cpu_pairs, "clocks": clk.summary(),
             "gpu_launches": int(st["launches"]) * args.steps,
             "gen_seconds": gen_s,
         }

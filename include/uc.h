@@ -83,6 +83,24 @@ uc_status uc_ctx_sync(uc_ctx *ctx);
 uc_status uc_ctx_set_sorted_output(uc_ctx *ctx, int on);
 uc_status uc_ctx_set_tuning(uc_ctx *ctx, const uc_tuning *t);
 uc_status uc_ctx_get_tuning(const uc_ctx *ctx, uc_tuning *t);
+/* Failure injection for tests of the error paths; no counterpart in the
+ * reference, whose only error handling is exit(1) on a file it cannot open
+ * (driver.cpp:262-265, compact.h:12-15).  All zeros (the default) = off.
+ *  - fail_alloc_after: the n-th device allocation this context makes from
+ *    now on fails as out of memory (1 = the next one); the call returns
+ *    UC_ENOMEM and the context stays usable.
+ *  - hec_round_cap: at most this many HEC matching rounds (0 = enough for
+ *    any list).  The device reports rounds that ran out with lists still
+ *    open (the bounded wait of the contraction).
+ *  - hec_strict: when the HEC rounds run out, fail with UC_ETIMEOUT instead
+ *    of finishing the lists by pointer jumping. */
+typedef struct uc_faults {
+    uint32_t fail_alloc_after;
+    uint32_t hec_round_cap;
+    uint32_t hec_strict;
+    uint32_t reserved;
+} uc_faults;
+uc_status uc_ctx_set_faults(uc_ctx *ctx, const uc_faults *f);
 const char *uc_last_error(const uc_ctx *ctx);
 const char *uc_status_str(uc_status s);
 
@@ -140,10 +158,15 @@ uc_status uc_emit(uc_ctx *ctx, const uint64_t *d_keys, const uint32_t *d_succ,
  * work runs on cuda_stream (NULL = legacy default stream) of the current
  * device.  Calls no cudaMalloc or cudaFree; its scratch is one static device
  * array per device, so n is limited to UC_EMIT_NOALLOC_MAX_KMERS (larger n
- * fails with UC_EINPUT).  The first call on a device looks that array up
- * (make it before any stream capture).  All calls on a device share the
- * array: calls that overlap on the GPU race.  err (err_len bytes, may be
- * NULL) receives a one-line reason on failure. */
+ * fails with UC_EINPUT).  The first call in a CUDA context looks that
+ * array up and loads the emission kernels; CUDA loads modules lazily, so the
+ * array and the kernels take their device memory then.  Make that first
+ * call before the caller's own pool takes the rest of the device's memory
+ * (or run with CUDA_MODULE_LOADING=EAGER), and before any stream capture;
+ * later calls in the context allocate nothing.  A context destroyed and
+ * created again (cudaDeviceReset) is set up again at its first call.  All
+ * calls in a context share the array: calls that overlap on the GPU race.
+ * err (err_len bytes, may be NULL) receives a one-line reason on failure. */
 #define UC_EMIT_NOALLOC_MAX_KMERS (1u << 20)
 uc_status uc_emit_noalloc(void *cuda_stream, const uint64_t *d_keys,
                           const uint32_t *d_succ, const uint32_t *d_head,

@@ -50,6 +50,8 @@ def lib():
         L.orc_compact.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_int,
                                   ctypes.POINTER(ctypes.c_void_p), i64p, i64p, i64p]
         L.orc_compact.restype = ctypes.c_int
+        L.orc_sort_lines.argtypes = [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, i64p]
+        L.orc_sort_lines.restype = ctypes.c_int
         L.orc_free.argtypes = [ctypes.c_void_p]
         L.orc_free.restype = None
         _lib = L
@@ -149,3 +151,37 @@ def compact(text: bytes, k: int):
 
 def sorted_lines(data: bytes) -> list[bytes]:
     return sorted(data.split(b"\n")[:-1] if data.endswith(b"\n") else data.split(b"\n"))
+
+
+def compact_mapped(text_addr: int, size: int, k: int):
+    """Whole path over text at a raw address (e.g. a memory-mapped file).
+    Returns (ctypes address of the malloc'd output, its length, n, cycles);
+    release the output with ``free``."""
+    L = lib()
+    out = ctypes.c_void_p()
+    olen = ctypes.c_int64(0)
+    n = ctypes.c_int64(0)
+    cyc = ctypes.c_int64(0)
+    st = L.orc_compact(ctypes.cast(text_addr, ctypes.c_char_p), size, k, ctypes.byref(out), ctypes.byref(olen),
+                       ctypes.byref(n), ctypes.byref(cyc))
+    if st == 1:
+        raise OracleError("malformed k-mer text")
+    if st:
+        raise MemoryError("orc_compact")
+    return out.value, olen.value, n.value, cyc.value
+
+
+def free(addr: int) -> None:
+    lib().orc_free(addr)
+
+
+def sort_lines_into(src_addr: int, size: int, dst: np.ndarray) -> int:
+    """Copy the '\\n'-terminated lines at src_addr into dst (uint8, >= size
+    bytes) in byte order; returns the line count."""
+    n = ctypes.c_int64(0)
+    st = lib().orc_sort_lines(src_addr, size, dst.ctypes.data, ctypes.byref(n))
+    if st == 1:
+        raise OracleError("last line has no newline")
+    if st:
+        raise MemoryError("orc_sort_lines")
+    return n.value

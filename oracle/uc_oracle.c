@@ -364,4 +364,61 @@ done:
     return st;
 }
 
+/* ---------------------------------------------------------- sorted lines */
+
+/* Sort key of a line: its first 16 bytes big-endian (two words), then the
+ * rest by memcmp.  Unitig lines start with distinct k-mers, so the words
+ * nearly always decide. */
+typedef struct {
+    uint64_t w0, w1;
+    int64_t off, len;
+} orc_line;
+
+static const char *g_sort_base;
+
+static inline uint64_t be_word(const char *p, int64_t avail) {
+    uint64_t v = 0;
+    for (int i = 0; i < 8; i++) v = (v << 8) | (uint64_t)(unsigned char)(i < avail ? p[i] : 0);
+    return v;
+}
+
+static int cmp_line(const void *a, const void *b) {
+    const orc_line *x = (const orc_line *)a, *y = (const orc_line *)b;
+    if (x->w0 != y->w0) return x->w0 < y->w0 ? -1 : 1;
+    if (x->w1 != y->w1) return x->w1 < y->w1 ? -1 : 1;
+    int64_t m = x->len < y->len ? x->len : y->len;
+    int c = memcmp(g_sort_base + x->off, g_sort_base + y->off, (size_t)m);
+    if (c) return c;
+    return (x->len > y->len) - (x->len < y->len);
+}
+
+int orc_sort_lines(const char *in, int64_t len, char *out, int64_t *n_lines) {
+    int64_t n = 0;
+    for (int64_t i = 0; i < len; i++) n += in[i] == '\n';
+    if (len > 0 && in[len - 1] != '\n') return ORC_EINPUT;
+    orc_line *r = (orc_line *)malloc((size_t)(n > 0 ? n : 1) * sizeof(orc_line));
+    if (!r) return ORC_ENOMEM;
+    int64_t s = 0, j = 0;
+    for (int64_t i = 0; i < len; i++) {
+        if (in[i] != '\n') continue;
+        r[j].off = s;
+        r[j].len = i - s;
+        r[j].w0 = be_word(in + s, i - s);
+        r[j].w1 = be_word(in + s + 8, i - s - 8);
+        j++;
+        s = i + 1;
+    }
+    g_sort_base = in;
+    qsort(r, (size_t)n, sizeof(orc_line), cmp_line);
+    int64_t p = 0;
+    for (int64_t t = 0; t < n; t++) {
+        memcpy(out + p, in + r[t].off, (size_t)r[t].len);
+        p += r[t].len;
+        out[p++] = '\n';
+    }
+    free(r);
+    *n_lines = n;
+    return ORC_OK;
+}
+
 void orc_free(void *p) { free(p); }

@@ -65,6 +65,12 @@ int64_t orc_emit(const uint32_t *words, int64_t n, int k, const uint32_t *succ,
 int orc_compact(const char *text, size_t bytes, int k, char **out,
                 int64_t *out_len, int64_t *n_kmers, int64_t *n_cycles);
 
+/* Lines of in[0, len) (each '\n'-terminated) copied to out in byte order;
+ * *n_lines receives their count.  Used to digest outputs too large to sort
+ * as Python objects.  Returns ORC_OK / ORC_EINPUT (a line without its
+ * newline) / ORC_ENOMEM. */
+int orc_sort_lines(const char *in, int64_t len, char *out, int64_t *n_lines);
+
 void orc_free(void *p);
 
 #ifdef __cplusplus

@@ -8,6 +8,17 @@ needs inputs large enough that a 1/64 file chunk holds the header and a line,
 a header equal to the line count, no homopolymer k-mer, and k = 15 mod 16.
 
     python tests/golden/make_golden.py      (needs oracle/_ref/uc_ref_serial)
+
+Full-size checksums (checksums_fullsize.json) of the benchmark's own single-job
+inputs, which are far too large to commit or to sort as Python objects:
+
+    python tests/golden/make_golden.py --fullsize NAME --workdir DIR [--reference]
+
+writes the input text to DIR, runs the oracle (oracle/liboracle.so, itself
+pinned to the reference by the fixtures above) and, with --reference, the
+reference's OpenMP build (oracle/_ref/uc_ref_large) on it, sorts each output's
+lines with the oracle's C helper and records count, bytes and sha256 with the
+name of every program that printed them.  Both must agree when both run.
 """
 import gzip
 import os
@@ -41,6 +52,14 @@ CHECKSUMS = {
     "scale_like_k31": ("scale_plain", {"length": 2_000_000, "seed": 27}, 31, 8),
     "batched_job_k31": ("batched_job", {"job": 11, "scale": 0.3}, 31, 8),
 }
+
+
+# Full-size single-job shapes: name -> (synth factory, kwargs, k, l)
+FULLSIZE = {
+    "scale_plain_1Gbp_k31": ("scale_plain", {}, 31, 8),
+    "wide_k63_200Mbp": ("wide_k", {}, 63, 8),
+}
+REF_OMP = os.path.join(ROOT, "oracle", "_ref", "uc_ref_large")
 
 
 def spec_of(fn: str, kw: dict):
@@ -96,5 +115,98 @@ def main():
         json.dump(sums, f, indent=1, sort_keys=True)
 
 
+def write_text(fn: str, kw: dict, k: int, path: str, chunk: int = 1 << 24) -> int:
+    """The seeded input written to path in the reference format, streamed in
+    chunks of k-mers (the whole text is never held); returns n."""
+    from unitigcoarsening_b200 import synth
+    km = synth.kmer_set(spec_of(fn, kw), k)
+    n = km.shape[0]
+    with open(path, "wb") as f:
+        f.write(f"{n}\n".encode())
+        for c0 in range(0, n, chunk):
+            synth.kmers_to_lines(km[c0:c0 + chunk], k).numpy().tofile(f)
+    del km
+    return n
+
+
+def sorted_digest(addr: int, size: int):
+    """(lines, sha256 of the lines in byte order) of the output at addr."""
+    import hashlib
+
+    import numpy as np
+
+    from oracle import oracle as O
+    dst = np.empty(max(size, 1), dtype=np.uint8)
+    nl = O.sort_lines_into(addr, size, dst)
+    h = hashlib.sha256(memoryview(dst)[:size]).hexdigest()
+    del dst
+    return nl, h
+
+
+def fullsize(name: str, workdir: str, with_reference: bool) -> None:
+    import json
+    import time
+
+    import numpy as np
+
+    from oracle import oracle as O
+    fn, kw, k, l = FULLSIZE[name]
+    os.makedirs(workdir, exist_ok=True)
+    path = os.path.join(workdir, f"{name}.txt")
+    t0 = time.time()
+    if not os.path.exists(path):
+        write_text(fn, kw, k, path + ".part")
+        os.replace(path + ".part", path)
+    print(name, "text", os.path.getsize(path), "bytes", f"{time.time() - t0:.0f} s", flush=True)
+    results = {}
+    t0 = time.time()
+    text = np.memmap(path, dtype=np.uint8, mode="r")
+    out, size, n, cyc = O.compact_mapped(text.ctypes.data, text.size, k)
+    del text
+    try:
+        nl, h = sorted_digest(out, size)
+    finally:
+        O.free(out)
+    results["oracle"] = {"n_kmers": n, "n_lines": nl, "bytes": size, "sha256_sorted_lines": h, "cycles": cyc}
+    print(name, "oracle", results["oracle"], f"{time.time() - t0:.0f} s", flush=True)
+    if with_reference:
+        outp = os.path.join(workdir, f"{name}.ref.out")
+        if os.path.exists(outp):
+            os.remove(outp)  # the reference appends
+        t0 = time.time()
+        env = dict(os.environ, OMP_NUM_THREADS=str(os.cpu_count()), OMP_PROC_BIND="spread", KSHIM_SEED="7")
+        r = subprocess.run([REF_OMP, path, str(k), str(l), outp], check=True, capture_output=True, env=env)
+        ref = np.memmap(outp, dtype=np.uint8, mode="r")
+        nl, h = sorted_digest(ref.ctypes.data, ref.size)
+        results["reference"] = {"n_kmers": n, "n_lines": nl, "bytes": int(ref.size), "sha256_sorted_lines": h}
+        del ref
+        os.remove(outp)
+        tot = [x for x in r.stdout.decode().splitlines() if "Total time" in x]
+        print(name, "reference", results["reference"], f"{time.time() - t0:.0f} s", tot, flush=True)
+        a, b = results["oracle"], results["reference"]
+        if any(a[x] != b[x] for x in ("n_lines", "bytes", "sha256_sorted_lines")):
+            raise SystemExit(f"{name}: oracle and reference disagree: {a} vs {b}")
+    dst = os.path.join(HERE, "checksums_fullsize.json")
+    sums = {}
+    if os.path.exists(dst):
+        with open(dst) as f:
+            sums = json.load(f)
+    o = results["oracle"]
+    sums[name] = {"fn": fn, "kwargs": kw, "k": k, "l": l, "n_kmers": o["n_kmers"], "n_lines": o["n_lines"],
+                  "bytes": o["bytes"], "sha256_sorted_lines": o["sha256_sorted_lines"],
+                  "printed_by": sorted(results)}
+    with open(dst, "w") as f:
+        json.dump(sums, f, indent=1, sort_keys=True)
+
+
 if __name__ == "__main__":
-    main()
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--fullsize", choices=sorted(FULLSIZE))
+    ap.add_argument("--workdir", default=os.path.join(ROOT, "_data"))
+    ap.add_argument("--reference", action="store_true")
+    a = ap.parse_args()
+    if a.fullsize:
+        fullsize(a.fullsize, a.workdir, a.reference)
+    else:
+        main()

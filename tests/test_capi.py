@@ -5,6 +5,8 @@ import os
 import re
 import subprocess
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADERS = [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")]
 
@@ -49,3 +51,59 @@ def test_status_strings_without_gpu():
 def test_build_targets_sm100a_only():
     from unitigcoarsening_b200 import build as B
     assert B.ARCH == ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+# The three config files the reference ships (base, cond, fourpart), written
+# out in their form: six numeric lines, then one word (no final newline).
+# The reference's code never reads them; the CLI accepts this form and
+# rejects others without touching a GPU (--check).
+REFERENCE_CONFIGS = {
+    "base_config.txt": "4\n0\n0\n2\n10\n1e-10\nnone",
+    "cond_config.txt": "2\n0\n0\n2\n10\n1e-10\nnone",
+    "fourpart_config.txt": "4\n0\n0\n4\n10\n1e-10\nnone",
+}
+
+
+def _cli(tmp_path, *extra):
+    from unitigcoarsening_b200 import build as B
+    B.build()
+    inp = tmp_path / "in.txt"
+    inp.write_text("3\nACG\nCGT\nGTA\n")
+    return subprocess.run([B.CLI, str(inp), "3", "2", str(tmp_path / "out.txt"), "--check", *extra],
+                          capture_output=True, text=True)
+
+
+def test_cli_accepts_reference_config_files(tmp_path):
+    ref_dir = os.environ.get("UC_REFERENCE_DIR", "")
+    for name, body in REFERENCE_CONFIGS.items():
+        p = tmp_path / name
+        p.write_text(body)
+        r = _cli(tmp_path, "--config", str(p))
+        assert r.returncode == 0, r.stderr
+        assert "ok: 3 k-mers" in r.stdout
+        # the reference's own copy, where its tree is at hand
+        q = os.path.join(ref_dir, name)
+        if ref_dir and os.path.exists(q):
+            r = _cli(tmp_path, "--config", q)
+            assert r.returncode == 0, r.stderr
+
+
+@pytest.mark.parametrize("body", ["4\n0\nx\n2\n10\n1e-10\nnone", "4\n0\n0\n2\n10\n1e-10", "4\n0\n0\n2\n10\n1e-10\nno ne",
+                                  "4\n0\n0\n2\n10\n1e-10\nnone\n7\n", "4 5\n0\n0\n2\n10\n1e-10\nnone", ""])
+def test_cli_rejects_other_config_files(tmp_path, body):
+    p = tmp_path / "cfg.txt"
+    p.write_text(body)
+    r = _cli(tmp_path, "--config", str(p))
+    assert r.returncode != 0
+    assert "config" in r.stderr
+
+
+def test_cli_check_rejects_bad_arguments(tmp_path):
+    assert _cli(tmp_path).returncode == 0
+    from unitigcoarsening_b200 import build as B
+    r = subprocess.run([B.CLI, "in.txt", "3", "2"], capture_output=True, text=True)
+    assert r.returncode != 0 and "Usage" in r.stderr
+    inp = tmp_path / "in.txt"
+    inp.write_text("3\nACG\nCGT\nGTA\n")
+    r = subprocess.run([B.CLI, str(inp), "3", "3", str(tmp_path / "o.txt"), "--check"], capture_output=True, text=True)
+    assert r.returncode != 0  # l must be below k

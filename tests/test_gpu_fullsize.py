@@ -8,10 +8,25 @@ wide-k job (k=63).
 - Each line holds k + (its k-mers - 1) chars, so the output is k * lines + n
   bytes, and every line has at least k chars.
 - Sorted output is deterministic: two runs give equal bytes, in byte order.
-Bit-exactness against the reference itself is covered at smaller sizes by
-the golden fixtures and the oracle tests."""
+- The sorted lines equal, byte for byte, those that the oracle (and for the
+  200 Mbp job the reference itself) printed for the same seeded input: line
+  count, byte count and sha256 of the lines in byte order, committed in
+  tests/golden/checksums_fullsize.json by tests/golden/make_golden.py."""
+import hashlib
+import json
+import os
+
 import pytest
 import torch
+
+FULLSIZE = os.path.join(os.path.dirname(__file__), "golden", "checksums_fullsize.json")
+
+
+def _fullsize_cases():
+    if not os.path.exists(FULLSIZE):
+        return []
+    with open(FULLSIZE) as f:
+        return sorted(json.load(f).items())
 
 pytestmark = pytest.mark.gpu
 
@@ -122,3 +137,29 @@ def test_fullsize_sorted_output_deterministic(comp):
         gt |= eq & (v[1:] > v[:-1])
         eq &= v[1:] == v[:-1]
     assert bool(gt.all())
+
+
+@pytest.mark.parametrize("name,case", _fullsize_cases(), ids=[n for n, _ in _fullsize_cases()])
+def test_fullsize_sorted_lines_equal_pinned_checksum(comp, name, case):
+    from unitigcoarsening_b200 import synth
+    k, l = case["k"], case["l"]
+    spec = getattr(synth, case["fn"])(**case["kwargs"])
+    text = synth.make_text(spec, k, device="cuda")
+    torch.cuda.synchronize()
+    torch.cuda.empty_cache()
+    comp.set_sorted_output(True)
+    try:
+        out, st = comp.compact(text, k, l, stats=True)
+    finally:
+        comp.set_sorted_output(False)
+    del text
+    torch.cuda.synchronize()
+    assert st["n_kmers"] == case["n_kmers"]
+    assert out.numel() == case["bytes"]
+    n_lines = int((out == 10).sum().item())
+    assert n_lines == case["n_lines"]
+    host = out.cpu()
+    del out
+    torch.cuda.empty_cache()
+    digest = hashlib.sha256(memoryview(host.numpy())).hexdigest()
+    assert digest == case["sha256_sorted_lines"], f"{name}: sorted lines differ from {case['printed_by']}"

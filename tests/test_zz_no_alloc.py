@@ -69,6 +69,41 @@ def test_noalloc_emit_matches_emit_twice(comp, k, l, length, limit):
 
 
 @pytest.mark.gpu
+def test_noalloc_emit_takes_no_device_memory(comp):
+    """After the first call in this context, a call leaves the device's free
+    memory unchanged, and still works while the caller holds all but a
+    sliver of it (the position of a process whose own pool owns the GPU)."""
+    k = 31
+    text = synth.make_text(synth.small_plain(seed=9, length=200_000), k, device="cuda")
+    keys, succ, head, rank = _graph(comp, text, k, 8)
+    ref = comp.write_unitigs(keys, succ, head, rank, k)
+    out = torch.empty(ref.numel() + 64, dtype=torch.uint8, device="cuda")
+    torch.cuda.synchronize()
+    f = _noalloc()
+    st, nb, msg = _call(f, keys, succ, head, rank, k, out)  # warm-up: the set-up call
+    assert st == 0, msg
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    st, nb, msg = _call(f, keys, succ, head, rank, k, out)
+    assert st == 0, msg
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert torch.equal(out[:nb], ref)
+    # hold all but 256 MiB of the free memory, then call again
+    hold = torch.empty(max(free1 - (256 << 20), 0), dtype=torch.uint8, device="cuda")
+    try:
+        out.fill_(0)
+        st, nb, msg = _call(f, keys, succ, head, rank, k, out)
+        assert st == 0, msg
+        torch.cuda.synchronize()
+        assert torch.equal(out[:nb], ref)
+    finally:
+        del hold
+        torch.cuda.empty_cache()
+
+
+@pytest.mark.gpu
 def test_noalloc_emit_rejects_beyond_maximum(comp):
     # rejected on the host before any device access: the pointers are never read
     keys = torch.zeros((4, 1), dtype=torch.int64, device="cuda")

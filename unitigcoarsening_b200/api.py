@@ -67,6 +67,11 @@ class Tuning(ctypes.Structure):
                 ("bucket_fill", ctypes.c_uint32)]
 
 
+class Faults(ctypes.Structure):
+    _fields_ = [("fail_alloc_after", ctypes.c_uint32), ("hec_round_cap", ctypes.c_uint32),
+                ("hec_strict", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+
 class ServerConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("lanes", ctypes.c_int), ("max_batch", ctypes.c_int),
                 ("reserved", ctypes.c_int), ("hbm_budget", ctypes.c_size_t), ("batch_bytes", ctypes.c_size_t),
@@ -104,6 +109,7 @@ def lib():
             "uc_ctx_set_tuning": ([vp, ctypes.POINTER(Tuning)], i),
             "uc_ctx_set_sorted_output": ([vp, i], i),
             "uc_ctx_get_tuning": ([vp, ctypes.POINTER(Tuning)], i),
+            "uc_ctx_set_faults": ([vp, ctypes.POINTER(Faults)], i),
             "uc_last_error": ([vp], ctypes.c_char_p),
             "uc_status_str": ([i], ctypes.c_char_p),
             "uc_parse_header": ([vp, vp, sz, pu64, pu64], i),
@@ -208,6 +214,12 @@ class Compactor:
         """Whole-job calls leave the lines in byte order (deterministic
         output; uc_ctx_set_sorted_output)."""
         self._check(self._L.uc_ctx_set_sorted_output(self._h, 1 if on else 0))
+
+    def set_faults(self, fail_alloc_after: int = 0, hec_round_cap: int = 0, hec_strict: bool = False):
+        """Failure injection for error-path tests (uc_ctx_set_faults); the
+        defaults switch it off."""
+        f = Faults(int(fail_alloc_after), int(hec_round_cap), 1 if hec_strict else 0, 0)
+        self._check(self._L.uc_ctx_set_faults(self._h, ctypes.byref(f)))
 
     def get_tuning(self) -> dict:
         t = Tuning()

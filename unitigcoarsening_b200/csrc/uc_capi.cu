@@ -52,9 +52,14 @@ uc_status grow(uc_ctx* c, char** buf, size_t* cap, size_t want) {
   *buf = nullptr;
   *cap = 0;
   const size_t sz = want + (want >> 4) + 4096;
-  const cudaError_t e = cudaMalloc(buf, sz);
+  const cudaError_t e = c->env.dev_malloc(reinterpret_cast<void**>(buf), sz);
   if (e != cudaSuccess) {
     *buf = nullptr;
+    if (e == cudaErrorMemoryAllocation) {
+      cudaGetLastError();
+      c->env.err = "cudaMalloc of " + std::to_string(sz >> 20) + " MiB (job buffers) failed";
+      return UC_ENOMEM;
+    }
     return cuda_fail(c, e, "cudaMalloc (job buffers)");
   }
   *cap = sz;
@@ -235,6 +240,12 @@ uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
 uc_status uc_ctx_get_tuning(const uc_ctx* c, uc_tuning* t) {
   if (!c || !t) return UC_EINPUT;
   *t = c->env.tune;
+  return UC_OK;
+}
+
+uc_status uc_ctx_set_faults(uc_ctx* c, const uc_faults* f) {
+  if (!c || !f) return UC_EINPUT;
+  c->env.faults = *f;
   return UC_OK;
 }
 

@@ -1924,6 +1924,14 @@ int Env::fail(int code, const std::string& msg) {
   return code;
 }
 
+cudaError_t Env::dev_malloc(void** p, size_t bytes) {
+  if (faults.fail_alloc_after && --faults.fail_alloc_after == 0) {
+    *p = nullptr;
+    return cudaErrorMemoryAllocation;
+  }
+  return cudaMalloc(p, bytes);
+}
+
 void* Env::take(int w, size_t bytes) {
   Arena& a = ar[w];
   const size_t o = (a.used + 255) & ~size_t(255);
@@ -1950,7 +1958,7 @@ int Env::reserve(int w, size_t bytes) {
     a.base = nullptr;
     a.cap = 0;
   }
-  if (cudaMalloc(&a.base, bytes) != cudaSuccess) {
+  if (dev_malloc(reinterpret_cast<void**>(&a.base), bytes) != cudaSuccess) {
     cudaGetLastError();
     a.base = nullptr;
     return fail(UC_ENOMEM, "cudaMalloc of " + std::to_string(bytes >> 20) + " MiB failed");
@@ -2658,6 +2666,11 @@ static uint32_t hec_rounds(uint64_t nmax) {
   for (uint64_t t = 1; t < nmax; t <<= 1) r += 2;
   return r;
 }
+// The rounds a run enqueues: the bound above, or the injected cap.
+static uint32_t hec_rounds(const Env& e, uint64_t nmax) {
+  const uint32_t r = hec_rounds(nmax);
+  return (e.faults.hec_round_cap && e.faults.hec_round_cap < r) ? e.faults.hec_round_cap : r;
+}
 
 // HEC contraction of the lists (prev, next, w) into X (pointer | HEAD_BIT,
 // offset) and cycle flags, all rounds enqueued on the stream.
@@ -2687,7 +2700,7 @@ static int contract_hec(Env& e, const uint64_t* d_keys, const uint32_t* succ, co
                         int k, uint32_t* head, uint32_t* rank, uint64_t& ncyc, bool& fell_back) {
   fell_back = false;
   e.reset();
-  const uint32_t R = hec_rounds(n);
+  const uint32_t R = hec_rounds(e, n);
   int r = e.reserve(1, hec_bytes(n, R) + n * (8 + 4 + 1) + 8 + 4096);
   if (r) return r;
   HecPool h{};
@@ -2711,6 +2724,12 @@ static int contract_hec(Env& e, const uint64_t* d_keys, const uint32_t* succ, co
   r = e.read_ctr();
   if (r) return r;
   if (e.h_ctr->err) {
+    if (e.faults.hec_strict) {
+      r = e.check_err(e.h_ctr);
+      UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
+      e.reset();
+      return r;
+    }
     fell_back = true;
     UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
     e.reset();
@@ -2817,6 +2836,28 @@ int emit(Env& e, const uint64_t* d_keys, const uint32_t* succ, const uint32_t* h
 uint64_t emit_scratch_bytes(uint64_t n) {
   auto al = [](uint64_t b) { return (b + 255) & ~uint64_t(255); };
   return 2 * al(n * 4) + al((n + 1) * 8) + al(scan_tmp_elems(n) * 8);
+}
+
+int emit_preload(std::string& err) {
+  const void* fns[] = {
+      reinterpret_cast<const void*>(k_count_members),
+      reinterpret_cast<const void*>(k_line_len),
+      reinterpret_cast<const void*>(k_scan_reduce<uint32_t, unsigned long long>),
+      reinterpret_cast<const void*>(k_scan_down<uint32_t, unsigned long long>),
+      reinterpret_cast<const void*>(k_scan_reduce<unsigned long long, unsigned long long>),
+      reinterpret_cast<const void*>(k_scan_down<unsigned long long, unsigned long long>),
+      reinterpret_cast<const void*>(k_spell<1>),
+      reinterpret_cast<const void*>(k_spell<2>)};
+  for (const void* f : fns) {
+    cudaFuncAttributes a;
+    const cudaError_t c = cudaFuncGetAttributes(&a, f);
+    if (c != cudaSuccess) {
+      cudaGetLastError();
+      err = std::string("cudaFuncGetAttributes: ") + cudaGetErrorString(c);
+      return UC_ECUDA;
+    }
+  }
+  return UC_OK;
 }
 
 int emit_in(cudaStream_t s, int sm_count, const uint64_t* d_keys, const uint32_t* head, const uint32_t* rank,
@@ -3025,7 +3066,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   const uint64_t segchars = Sp * uint64_t(k) + copies + 64;
   const uint32_t R = 64;
   const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
-  const uint32_t RH = hec_rounds(Sp);
+  const uint32_t RH = hec_rounds(e, Sp);
   const size_t back = back_bytes(copies, X, Sp, nw, k, want_hec);
   r = e.reserve(1, back);
   if (r) return r;
@@ -3128,6 +3169,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     r = e.read_ctr();
     if (r) return r;
     if (e.h_ctr->err) {  // did not finish in its pool/rounds: pointer jumping
+      if (e.faults.hec_strict) return e.check_err(e.h_ctr);
       UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
       hec = false;
     }

@@ -57,9 +57,14 @@ struct Env {
   // recorded after them: from then on the job's text is no longer read, so
   // a host pipeline can upload the next job's text into the same buffer
   std::function<void()> after_pack;
+  // failure injection (uc_ctx_set_faults); zeros = off
+  uc_faults faults{};
   std::string err;
 
   int fail(int code, const std::string& msg);
+  // Every device allocation of a context goes through here, so that
+  // faults.fail_alloc_after can make one fail as out of memory.
+  cudaError_t dev_malloc(void** p, size_t bytes);
   void* take(int arena, size_t bytes);
   // Make an arena hold `bytes`; only while nothing is taken from it.
   int reserve(int arena, size_t bytes);
@@ -95,6 +100,10 @@ void batch_footprint(const Env& e, uint32_t njobs, const size_t* bytes, int k, i
 // (256-byte aligned) on stream s: the same kernels, no allocation.  Clears
 // the member counts it needs at zero itself.
 uint64_t emit_scratch_bytes(uint64_t n);
+// Loads every kernel emit_in launches.  Under lazy module loading (the CUDA
+// default) a kernel's module is loaded, and its device memory taken, at its
+// first use; after this call emit_in needs no device memory of its own.
+int emit_preload(std::string& err);
 int emit_in(cudaStream_t s, int sm_count, const uint64_t* d_keys, const uint32_t* head, const uint32_t* rank,
             uint64_t n, int k, char* out, uint64_t cap, uint64_t& out_bytes, void* scratch, std::string& err);
 

@@ -75,16 +75,24 @@ class _Stream:
         return min(hi, lo + int(self.unit() * (hi - lo + 1)))
 
 
+_CHUNK = 1 << 26  # elements per pass of the per-position draws (bounds peak memory)
+
+
 def random_bases(n: int, gc: float, seed: int, stream: int, device, offset: int = 0) -> torch.Tensor:
-    """i.i.d. bases (0..3 = A,C,G,T) with P(C)=P(G)=gc/2."""
-    idx = torch.arange(offset, offset + n, device=device, dtype=torch.int64)
-    u = rand_unit(seed, stream, idx)
-    gc_side = u < gc
-    v = torch.where(gc_side, u / max(gc, 1e-300), (u - gc) / max(1.0 - gc, 1e-300))
-    hi_half = v >= 0.5
-    # GC side: C (1) / G (2); AT side: A (0) / T (3)
-    b = torch.where(gc_side, torch.where(hi_half, 2, 1), torch.where(hi_half, 3, 0))
-    return b.to(torch.uint8)
+    """i.i.d. bases (0..3 = A,C,G,T) with P(C)=P(G)=gc/2.  Each base depends
+    only on its own counter, so the draws run in chunks of _CHUNK positions."""
+    out = torch.empty(n, dtype=torch.uint8, device=device)
+    for c0 in range(0, n, _CHUNK):
+        c1 = min(n, c0 + _CHUNK)
+        idx = torch.arange(offset + c0, offset + c1, device=device, dtype=torch.int64)
+        u = rand_unit(seed, stream, idx)
+        gc_side = u < gc
+        v = torch.where(gc_side, u / max(gc, 1e-300), (u - gc) / max(1.0 - gc, 1e-300))
+        hi_half = v >= 0.5
+        # GC side: C (1) / G (2); AT side: A (0) / T (3)
+        b = torch.where(gc_side, torch.where(hi_half, 2, 1), torch.where(hi_half, 3, 0))
+        out[c0:c1] = b.to(torch.uint8)
+    return out
 
 
 def _mutate(seq: torch.Tensor, rate: float, seed: int, stream: int, offset: int = 0) -> torch.Tensor:
@@ -159,8 +167,11 @@ def make_genome(spec: GenomeSpec, device="cpu"):
         idx = torch.arange(m, device=device, dtype=torch.int64)
         pos = rand_int(spec.seed, 3, idx, 0, L - 1)
     elif spec.snp_rate > 0:
-        idx = torch.arange(L, device=device, dtype=torch.int64)
-        pos = torch.nonzero(rand_unit(spec.seed, 3, idx) < spec.snp_rate).flatten()
+        hits = []
+        for c0 in range(0, L, _CHUNK):
+            idx = torch.arange(c0, min(L, c0 + _CHUNK), device=device, dtype=torch.int64)
+            hits.append(torch.nonzero(rand_unit(spec.seed, 3, idx) < spec.snp_rate).flatten() + c0)
+        pos = torch.cat(hits)
     else:
         pos = torch.zeros(0, dtype=torch.int64, device=device)
     pos = torch.unique(pos)
