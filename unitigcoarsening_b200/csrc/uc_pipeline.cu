@@ -2096,7 +2096,7 @@ static int job_buffers(Env& e, uint32_t njobs) {
   }
   e.jbuf = nullptr;
   e.jcap = 0;
-  if (cudaMalloc(&e.jbuf, want) != cudaSuccess) {
+  if (e.dev_malloc(reinterpret_cast<void**>(&e.jbuf), want) != cudaSuccess) {
     cudaGetLastError();
     e.jbuf = nullptr;
     return e.fail(UC_ENOMEM, "job table");
@@ -2484,7 +2484,7 @@ static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
       e.big_buf = nullptr;
       e.big_cap = 0;
       if (want > e.budget) return e.fail(UC_EBUDGET, "scratch for oversized buckets");
-      if (cudaMalloc(&e.big_buf, want) != cudaSuccess) {
+      if (e.dev_malloc(reinterpret_cast<void**>(&e.big_buf), want) != cudaSuccess) {
         cudaGetLastError();
         e.big_buf = nullptr;
         return e.fail(UC_ENOMEM, "scratch for oversized buckets");
