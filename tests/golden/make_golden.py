@@ -143,6 +143,50 @@ def sorted_digest(addr: int, size: int):
     return nl, h
 
 
+def _sorted_copy(addr: int, size: int) -> bytes:
+    import numpy as np
+
+    from oracle import oracle as O
+    dst = np.empty(max(size, 1), dtype=np.uint8)
+    O.sort_lines_into(addr, size, dst)
+    return dst[:size].tobytes()
+
+
+def _kmers_of(lines, k: int):
+    out = []
+    for x in lines:
+        out += [x[i:i + k] for i in range(len(x) - k + 1)]
+    return sorted(out)
+
+
+def cycle_only_difference(a: bytes, b: bytes, k: int, cycles: int):
+    """Compare two outputs line by line (both sorted).  The reference leaves
+    the member order of an isolated cycle unspecified (coarseners.h:191-230),
+    so outputs may differ in cycle lines only.  Returns the differing lines
+    of each side when they are at most `cycles` lines each and hold the same
+    k-mers as a set (each a rotation of the same cycle); None otherwise."""
+    la = a.split(b"\n")[:-1]
+    lb = b.split(b"\n")[:-1]
+    i = j = 0
+    da, db = [], []
+    while i < len(la) or j < len(lb):
+        if j >= len(lb) or (i < len(la) and la[i] < lb[j]):
+            da.append(la[i]); i += 1
+        elif i >= len(la) or lb[j] < la[i]:
+            db.append(lb[j]); j += 1
+        else:
+            i += 1; j += 1
+        if len(da) > cycles or len(db) > cycles:
+            return None
+    # a cycle of m k-mers spells k + m - 1 chars starting anywhere on it: its
+    # k-mer set (the windows of the circular string) is the same
+    if len(da) != len(db):
+        return None
+    if set(_kmers_of(da, k)) != set(_kmers_of(db, k)):
+        return None
+    return da, db
+
+
 def fullsize(name: str, workdir: str, with_reference: bool) -> None:
     import json
     import time
@@ -179,13 +223,30 @@ def fullsize(name: str, workdir: str, with_reference: bool) -> None:
         ref = np.memmap(outp, dtype=np.uint8, mode="r")
         nl, h = sorted_digest(ref.ctypes.data, ref.size)
         results["reference"] = {"n_kmers": n, "n_lines": nl, "bytes": int(ref.size), "sha256_sorted_lines": h}
-        del ref
-        os.remove(outp)
         tot = [x for x in r.stdout.decode().splitlines() if "Total time" in x]
         print(name, "reference", results["reference"], f"{time.time() - t0:.0f} s", tot, flush=True)
         a, b = results["oracle"], results["reference"]
         if any(a[x] != b[x] for x in ("n_lines", "bytes", "sha256_sorted_lines")):
-            raise SystemExit(f"{name}: oracle and reference disagree: {a} vs {b}")
+            # allowed only in the lines of isolated cycles, whose order the
+            # reference leaves unspecified
+            rb = _sorted_copy(ref.ctypes.data, ref.size)
+            del ref
+            text = np.memmap(path, dtype=np.uint8, mode="r")
+            out, size, _, _ = O.compact_mapped(text.ctypes.data, text.size, k)
+            del text
+            try:
+                ob = _sorted_copy(out, size)
+            finally:
+                O.free(out)
+            d = cycle_only_difference(ob, rb, k, results["oracle"]["cycles"])
+            if d is None:
+                raise SystemExit(f"{name}: oracle and reference disagree beyond cycle lines: {a} vs {b}")
+            results["reference"]["differs_only_in_cycle_lines"] = len(d[0])
+            print(name, "reference differs from the oracle only in", len(d[0]), "cycle line(s):",
+                  [x[:80] for x in d[0]], [x[:80] for x in d[1]], flush=True)
+        else:
+            del ref
+        os.remove(outp)
     dst = os.path.join(HERE, "checksums_fullsize.json")
     sums = {}
     if os.path.exists(dst):
@@ -193,8 +254,10 @@ def fullsize(name: str, workdir: str, with_reference: bool) -> None:
             sums = json.load(f)
     o = results["oracle"]
     sums[name] = {"fn": fn, "kwargs": kw, "k": k, "l": l, "n_kmers": o["n_kmers"], "n_lines": o["n_lines"],
-                  "bytes": o["bytes"], "sha256_sorted_lines": o["sha256_sorted_lines"],
+                  "bytes": o["bytes"], "sha256_sorted_lines": o["sha256_sorted_lines"], "cycles": o["cycles"],
                   "printed_by": sorted(results)}
+    if "reference" in results:
+        sums[name]["reference"] = results["reference"]
     with open(dst, "w") as f:
         json.dump(sums, f, indent=1, sort_keys=True)
 

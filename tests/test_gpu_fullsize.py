@@ -156,7 +156,7 @@ def test_fullsize_sorted_lines_equal_pinned_checksum(comp, name, case):
     torch.cuda.synchronize()
     assert st["n_kmers"] == case["n_kmers"]
     assert out.numel() == case["bytes"]
-    n_lines = int((out == 10).sum().item())
+    n_lines = sum(int((out[c0:c0 + (1 << 30)] == 10).sum().item()) for c0 in range(0, out.numel(), 1 << 30))
     assert n_lines == case["n_lines"]
     host = out.cpu()
     del out
