@@ -83,6 +83,24 @@ uc_status uc_ctx_sync(uc_ctx *ctx);
 uc_status uc_ctx_set_sorted_output(uc_ctx *ctx, int on);
 uc_status uc_ctx_set_tuning(uc_ctx *ctx, const uc_tuning *t);
 uc_status uc_ctx_get_tuning(const uc_ctx *ctx, uc_tuning *t);
+/* Host jobs larger than the device.  The reference runs jobs up to host
+ * memory by moving its 64 minimizer buckets to the device one at a time
+ * (driver.cpp:479-521, README.md:6-7).  uc_compact_host, uc_job_submit and
+ * uc_compact_file instead stream: the text goes to the device in chunks of
+ * chunk_lines lines, twice (bucket counts, then the bucketed copies), the
+ * tiles run in groups of about group_copies copies whose lines return to
+ * host memory group by group, and the cross-tile lines follow; the device
+ * holds one chunk, the copies of all k-mers and the segment arrays, so a
+ * job of several billion k-mers (64-bit k-mer indices) runs on one B200.
+ * mode UC_STREAM_AUTO (the default) streams a job whose resident run does
+ * not fit the budget; UC_STREAM_ALWAYS streams every host job;
+ * UC_STREAM_NEVER never does.  Streaming needs k chars + '\n' per line and
+ * unsorted output.  0 for chunk_lines / group_copies = defaults (2^26
+ * lines, 2^28 copies). */
+enum { UC_STREAM_AUTO = 0, UC_STREAM_ALWAYS = 1, UC_STREAM_NEVER = 2 };
+uc_status uc_ctx_set_streaming(uc_ctx *ctx, int mode, uint64_t chunk_lines,
+                               uint64_t group_copies);
+
 /* Failure injection for tests of the error paths; no counterpart in the
  * reference, whose only error handling is exit(1) on a file it cannot open
  * (driver.cpp:262-265, compact.h:12-15).  All zeros (the default) = off.

@@ -36,6 +36,7 @@ NONE = 0xFFFFFFFF
 
 CONTRACT_POINTER_JUMP = 0
 CONTRACT_HEC = 1
+STREAM_AUTO, STREAM_ALWAYS, STREAM_NEVER = 0, 1, 2
 
 STATUS = {0: "ok", 1: "invalid input", 2: "out of memory", 3: "HBM budget exceeded",
           4: "device wait timed out", 5: "internal error", 6: "CUDA error", 7: "job not finished"}
@@ -110,6 +111,7 @@ def lib():
             "uc_ctx_set_sorted_output": ([vp, i], i),
             "uc_ctx_get_tuning": ([vp, ctypes.POINTER(Tuning)], i),
             "uc_ctx_set_faults": ([vp, ctypes.POINTER(Faults)], i),
+            "uc_ctx_set_streaming": ([vp, i, u64, u64], i),
             "uc_last_error": ([vp], ctypes.c_char_p),
             "uc_status_str": ([i], ctypes.c_char_p),
             "uc_parse_header": ([vp, vp, sz, pu64, pu64], i),
@@ -220,6 +222,12 @@ class Compactor:
         defaults switch it off."""
         f = Faults(int(fail_alloc_after), int(hec_round_cap), 1 if hec_strict else 0, 0)
         self._check(self._L.uc_ctx_set_faults(self._h, ctypes.byref(f)))
+
+    def set_streaming(self, mode: int = STREAM_AUTO, chunk_lines: int = 0, group_copies: int = 0):
+        """Host jobs beyond the device budget run streamed
+        (uc_ctx_set_streaming): STREAM_AUTO, STREAM_ALWAYS or STREAM_NEVER,
+        with the chunk and tile-group sizes (0 = defaults)."""
+        self._check(self._L.uc_ctx_set_streaming(self._h, int(mode), int(chunk_lines), int(group_copies)))
 
     def get_tuning(self) -> dict:
         t = Tuning()

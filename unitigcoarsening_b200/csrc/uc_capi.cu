@@ -19,6 +19,9 @@ struct uc_ctx {
   // uc_compact_host_many: the upload stream and its completion event
   cudaStream_t up_stream = nullptr;
   cudaEvent_t up_done = nullptr;
+  // host jobs beyond the device budget (uc_ctx_set_streaming)
+  int stream_mode = UC_STREAM_AUTO;
+  uint64_t stream_chunk_lines = 0, stream_group_copies = 0;
 };
 
 struct uc_job {
@@ -67,11 +70,62 @@ uc_status grow(uc_ctx* c, char** buf, size_t* cap, size_t want) {
 }
 
 // Host text in, host lines out (synchronous).
+uc_status run_resident(uc_ctx* c, const char* text, size_t bytes, int k, int l, char** out_owned,
+                       char* out_user, size_t out_cap, size_t* out_len, uc_stats* st);
+
+// The streamed path (uc::compact_streamed) from host text into dst (out_user,
+// or a buffer of the output bound allocated here).
+uc_status run_streamed(uc_ctx* c, const char* text, size_t bytes, int k, int l, char** out_owned,
+                       char* out_user, size_t out_cap, size_t* out_len, uc_stats* st) {
+  // the device copies of the in-memory path are not used here
+  if (c->io_text) cudaFree(c->io_text);
+  if (c->io_out) cudaFree(c->io_out);
+  c->io_text = c->io_out = nullptr;
+  c->io_text_cap = c->io_out_cap = 0;
+  const uint64_t bound = uc::output_bound(bytes, k);
+  char* dst = out_user;
+  size_t cap = out_cap;
+  if (!dst) {
+    dst = static_cast<char*>(std::malloc(bound ? bound : 1));
+    if (!dst) {
+      c->env.err = "host malloc of the result failed";
+      return UC_ENOMEM;
+    }
+    cap = bound;
+  }
+  uint64_t ob = 0;
+  const int r = uc::compact_streamed(c->env, text, bytes, k, l, dst, cap, ob, st, c->stream_chunk_lines,
+                                     c->stream_group_copies);
+  if (r) {
+    if (!out_user) std::free(dst);
+    return as_status(r);
+  }
+  if (out_owned) *out_owned = dst;
+  *out_len = ob;
+  return UC_OK;
+}
+
 uc_status run_host(uc_ctx* c, const char* text, size_t bytes, int k, int l, char** out_owned,
                    char* out_user, size_t out_cap, size_t* out_len, uc_stats* st) {
   uc_status s = set_device(c);
   if (s) return s;
-  s = grow(c, &c->io_text, &c->io_text_cap, bytes + 64);
+  if (c->stream_mode == UC_STREAM_ALWAYS) return run_streamed(c, text, bytes, k, l, out_owned, out_user, out_cap,
+                                                               out_len, st);
+  s = run_resident(c, text, bytes, k, l, out_owned, out_user, out_cap, out_len, st);
+  // a job whose arrays do not fit the device (or its budget) beside its
+  // text and lines runs streamed, when the text has the fixed line layout
+  if ((s == UC_EBUDGET || s == UC_ENOMEM) && c->stream_mode == UC_STREAM_AUTO && !c->env.sorted) {
+    const std::string why = c->env.err;
+    c->env.reset();
+    s = run_streamed(c, text, bytes, k, l, out_owned, out_user, out_cap, out_len, st);
+    if (s) c->env.err = why + "; streamed: " + c->env.err;
+  }
+  return s;
+}
+
+uc_status run_resident(uc_ctx* c, const char* text, size_t bytes, int k, int l, char** out_owned,
+                       char* out_user, size_t out_cap, size_t* out_len, uc_stats* st) {
+  uc_status s = grow(c, &c->io_text, &c->io_text_cap, bytes + 64);
   if (s) return s;
   const uint64_t bound = uc::output_bound(bytes, k);
   s = grow(c, &c->io_out, &c->io_out_cap, bound);
@@ -240,6 +294,18 @@ uc_status uc_ctx_set_tuning(uc_ctx* c, const uc_tuning* t) {
 uc_status uc_ctx_get_tuning(const uc_ctx* c, uc_tuning* t) {
   if (!c || !t) return UC_EINPUT;
   *t = c->env.tune;
+  return UC_OK;
+}
+
+uc_status uc_ctx_set_streaming(uc_ctx* c, int mode, uint64_t chunk_lines, uint64_t group_copies) {
+  if (!c) return UC_EINPUT;
+  if (mode != UC_STREAM_AUTO && mode != UC_STREAM_ALWAYS && mode != UC_STREAM_NEVER) {
+    c->env.err = "mode must be UC_STREAM_AUTO, UC_STREAM_ALWAYS or UC_STREAM_NEVER";
+    return UC_EINPUT;
+  }
+  c->stream_mode = mode;
+  c->stream_chunk_lines = chunk_lines;
+  c->stream_group_copies = group_copies;
   return UC_OK;
 }
 

@@ -25,13 +25,28 @@ struct Counters {
   uint32_t work_next;                // level-2 scatter work counter
   uint32_t nwarp, nblock;            // tiles per tier
   uint32_t wtile_next;
-  uint32_t count_ovf;                // a 16-bit bucket count wrapped in k_pack
 };
+
+// One open segment of the fused path (written by the tile that finds it): the
+// offset of its chars in the segment-char area (low 40 bits) and its job
+// (high 24 bits), its copy count, and the cross index through which its line
+// continues (NONE where the line ends).  Segment ids: a segment that starts
+// at the S-only copy of cross k-mer x has id x; a segment that starts a line
+// (at a P-role copy) takes an id from its job's head pool, after all cross
+// indices.
+struct __align__(16) SegRec {
+  unsigned long long off_job;
+  uint32_t len;
+  uint32_t next;
+};
+constexpr int SEG_OFF_BITS = 40;
+constexpr unsigned long long SEG_OFF_MASK = (1ull << SEG_OFF_BITS) - 1ull;
 
 // One job of a batch (a single call is a batch of one).  Its k-mers occupy
 // keys[koff, koff + n); its buckets are (job << job_bits) | local; its lines
-// go to out[obase, obase + ocap); its open segments use ids
-// [seg_base, seg_base + seg_cap).
+// go to out[obase, obase + ocap); the segments that start its stitched
+// lines take head-pool ids [seg_base, seg_base + seg_cap) (after the cross
+// indices).
 struct JobTab {
   const uint8_t* text;
   unsigned long long tbytes, body, end, n, koff, lb0;  // lb0: first 256-line block
@@ -53,8 +68,7 @@ struct TileParams {
   const JobTab* jobs;
   const uint32_t* tile_job;     // job of each tile
   unsigned long long* jout;     // per-job closed-line cursor (bytes)
-  uint32_t* jseg;               // per-job segment cursor
-  uint32_t* seg_job;            // job of each segment
+  uint32_t* jseg;               // per-job head-pool cursor
   char* big_scratch;
   const unsigned long long* big_off;
   int k;
@@ -69,12 +83,9 @@ struct TileParams {
   char* segchars;
   unsigned long long segchars_cap;
   uint32_t seg_cap;
-  unsigned long long* seg_off;
-  uint32_t* seg_len;
-  uint32_t* seg_sx;
-  uint32_t* seg_ex;
-  uint32_t* start_seg;
-  uint32_t* end_seg;
+  SegRec* seg;                  // open segments by id
+  unsigned long long* Xr;       // list-ranking state by segment id
+  uint32_t xcount;              // cross k-mers (the head pool starts there)
 };
 
 // Shared memory of one tile: keys plus four 16-bit arrays per copy, and

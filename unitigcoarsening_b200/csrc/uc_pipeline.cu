@@ -7,13 +7,16 @@
 //   --scan/plan--> tiles of whole buckets --k_scatter_coarse/fine--> copies
 //   in bucket order --k_tile_warp / k_tile / k_tile_big (persistent; a warp,
 //   a CTA, or global scratch per tile)--> finished lines + open segments
-//   --stitch (k_seg_link, list ranking, k_seg_copy)--> cross-tile lines.
+//   (records, links and the first ranking state by segment id)
+//   --stitch (list ranking, k_chain_len, k_seg_copy)--> cross-tile lines.
 // The phase-by-phase entry points (pack, minimizers, find_edges, contract,
 // emit) run the same kernels separately.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/uc.h"
@@ -83,6 +86,18 @@ static void scan_excl(const Tin* in, uint64_t n, Tout* out, Tout* tmp, cudaStrea
   k_scan_down<Tin, Tout><<<unsigned(nb), 1024, 0, s>>>(in, n, out, boff, per_block, total_out);
 }
 
+// Kernels scan_excl launches for n elements.
+static uint32_t scan_launches(uint64_t n) {
+  uint32_t c = 0;
+  const uint64_t per_block = 1024 * 8;
+  for (;;) {
+    const uint64_t nb = std::max<uint64_t>(1, (n + per_block - 1) / per_block);
+    c += 2;
+    if (nb == 1) return c;
+    n = nb;
+  }
+}
+
 static uint64_t scan_tmp_elems(uint64_t n) {
   uint64_t t = 0;
   const uint64_t per_block = 1024 * 8;
@@ -149,12 +164,13 @@ __device__ __forceinline__ uint32_t job_of_block(const JobTab* __restrict__ jobs
 // 2^25 buckets take 64 MiB and the count atomics stay in L2; a half that
 // wraps raises *ovf, and the counts are then taken again at 32 bits
 // (k_count_buckets).  k_widen16 turns them into 32-bit counts.
-__device__ __forceinline__ void count16(uint32_t* c16, uint32_t b, uint32_t* ovf) {
-  const uint32_t sh = (b & 1u) * 16u;
-  const uint32_t old = atomicAdd(c16 + (b >> 1), 1u << sh);
-  if (((old >> sh) & 0xFFFFu) == 0xFFFFu) atomicOr(ovf, 1u);
+__device__ __forceinline__ void count16(uint32_t* c16, uint32_t b) {
+  // a reduction (no value returned, so no wait): a count that wraps its 16
+  // bits carries into its neighbour or out of the word, which shows up on
+  // the host as a total below the copies the pack counted (k-mers plus cross
+  // k-mers), and the counts are then taken again at 32 bits
+  atomicAdd(c16 + (b >> 1), 1u << ((b & 1u) * 16u));
 }
-
 __global__ void k_widen16(const uint32_t* __restrict__ c16, uint64_t M, uint32_t* __restrict__ counts) {
   for (uint64_t b = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; b < M; b += uint64_t(gridDim.x) * blockDim.x)
     counts[b] = (c16[b >> 1] >> ((b & 1u) * 16u)) & 0xFFFFu;
@@ -177,8 +193,7 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
                                               const unsigned long long* __restrict__ starts, int k,
                                               uint64_t* __restrict__ keys, uint32_t* err, int l, uint64_t seed,
                                               uint32_t jb, uint32_t* __restrict__ b1, uint32_t* __restrict__ b2,
-                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ jcross,
-                                              uint32_t* ovf) {
+                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ jcross) {
   __shared__ uint32_t buf[PACK_WORDS];
   __shared__ uint32_t s_cross;
   uint32_t bad = 0;
@@ -330,10 +345,12 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
         b = jp | bucket_of(b, jb);
         __stcs(b1 + koff + line, a);
         __stcs(b2 + koff + line, b);
-        count16(counts, a, ovf);
-        if (a != b) {
-          count16(counts, b, ovf);
-          mycross = 1;
+        if (counts) {  // (the streamed path's second pass only needs the buckets)
+          count16(counts, a);
+          if (a != b) {
+            count16(counts, b);
+            mycross = 1;
+          }
         }
       }
     }
@@ -342,7 +359,7 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
       if ((threadIdx.x & 31) == 0 && mycross) atomicAdd(&s_cross, mycross);
     }
     __syncthreads();
-    if (FUSE && threadIdx.x == 0 && s_cross) atomicAdd(jcross + j, s_cross);
+    if (FUSE && threadIdx.x == 0 && s_cross && jcross) atomicAdd(jcross + j, s_cross);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(err, starts ? ERR_LINE : ERR_LAYOUT);
 }
@@ -528,9 +545,9 @@ __global__ void k_tile_write(const uint32_t* __restrict__ flag, const uint32_t* 
 __global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Counters* ctr, uint32_t wcap,
                            uint32_t cap, uint32_t* __restrict__ wlist, uint32_t* __restrict__ blist,
                            uint32_t* __restrict__ big_list, unsigned long long* __restrict__ big_size, int nw,
-                           uint32_t lf) {
-  const uint32_t nt = ctr->ntiles;
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+                           uint32_t lf, uint32_t t0, uint32_t t1) {
+  const uint32_t nt = min(ctr->ntiles, t1);
+  for (uint32_t t = t0 + blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
     const uint64_t c = tile_begin[t + 1] - tile_begin[t];
     // (a tile's line bytes must fit 32-bit offsets: c * 64 < 2^32)
     if (tile_begin[t + 1] < tile_begin[t] || c > (1ull << 26)) {
@@ -559,16 +576,17 @@ __global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Co
 // copies of a cross k-mer share one cross index; in edges mode every copy
 // carries the k-mer's id instead.
 //
-// Two levels keep the write frontier inside L2.  Level 1 groups each block's
-// copies by coarse partition (high bucket bits, at most 256 partitions) in
-// shared memory and writes them out as contiguous runs, one reservation per
-// block and partition.  A coarse partition occupies exactly the final
-// positions of its buckets, so level 1 writes (key, link, bucket) records
-// into the same index range of a staging array; level 2 then walks the
-// staged records in index order - that is, partition by partition - with
-// every block taking the next chunk from a shared counter, and places each
-// record with its bucket's cursor.  All blocks therefore write into the same
-// one or two partitions at any time.
+// Three levels keep the write frontier inside L2 and the global atomics few.
+// Level 1 groups each block's copies by coarse partition (high bucket bits,
+// at most 256 partitions) in shared memory and writes them out as contiguous
+// runs, one reservation per block and partition.  A coarse partition
+// occupies exactly the final positions of its buckets, so level 1 writes
+// (key, link, bucket) records into the same index range of a staging
+// region.  Level 2 groups each partition's records the same way by
+// sub-partition (2^sb buckets), into the same index ranges of a second
+// region; all blocks take chunks in partition order.  Level 3 gives each
+// sub-partition to one block, which places the records inside its range with
+// shared-memory cursors per bucket.
 // k-mers per level-1 block pass (at most twice as many copies): large chunks
 // spread the per-chunk reservations and barriers over more copies; 3072
 // 64-bit keys (100 KB of staging, 2 CTAs per SM) beat 2048 (3 CTAs per SM)
@@ -578,7 +596,6 @@ __host__ __device__ constexpr int sc_chunk() {
   return NW == 1 ? 3072 : 2048;
 }
 static_assert(2 * sc_chunk<1>() < 65536 && 2 * sc_chunk<2>() < 65536, "chunk copy counts share a 32-bit scan");
-constexpr int SC_FINE = 4096;    // staged records per level-2 work item
 
 __global__ void k_coarse_init(const unsigned long long* __restrict__ boff, uint32_t fb, uint32_t mc,
                               unsigned long long* __restrict__ ccur) {
@@ -715,43 +732,239 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
   }
 }
 
-// Level 2: staged records in index order, a chunk per grab.
+// Level 2: within each coarse partition the staged records are grouped again
+// by sub-partition (2^sb consecutive buckets, a few thousand copies), the way
+// level 1 groups by partition: a block takes a chunk of one partition's
+// staged records, counts them per sub-partition in shared memory, reserves
+// one run per sub-partition (one global atomic per run, a few records each
+// instead of one per record) and writes its records out as contiguous runs.
+// Chunks never span partitions (their list comes from k_mid_items), so the
+// counts index one partition's sub-partitions.  All blocks take chunks in
+// partition order, which keeps the write frontier inside L2.
+constexpr int MID_CHUNK = 4096;    // staged records per level-2 chunk
+constexpr int MID_MAX_BINS = 1024; // sub-partitions per coarse partition
+constexpr int SUB_MAX_BITS = 8;    // buckets per sub-partition: at most 2^8
+
+// Chunk list of level 2: item_start[p] = first chunk of coarse partition p
+// (partition p holds the staged records [boff[p << fb], boff[(p+1) << fb])).
+__global__ void k_mid_items(const unsigned long long* __restrict__ boff, uint32_t fb, uint32_t mc,
+                            uint32_t* __restrict__ item_start) {
+  __shared__ uint32_t sc[33];
+  const uint32_t p = threadIdx.x;
+  uint32_t items = 0;
+  if (p < mc) {
+    const unsigned long long lo = boff[uint64_t(p) << fb], hi = boff[uint64_t(p + 1) << fb];
+    items = uint32_t((hi - lo + MID_CHUNK - 1) / MID_CHUNK);
+  }
+  uint32_t tot;
+  const uint32_t pre = block_excl_scan(items, sc, &tot);
+  if (p < mc) item_start[p] = pre;
+  if (p == 0) item_start[mc] = tot;
+}
+
 template <int NW>
-__global__ void __launch_bounds__(256) k_scatter_fine(const uint64_t* __restrict__ rkey,
-                                                      const uint32_t* __restrict__ rlink,
-                                                      const uint32_t* __restrict__ rbkt, uint64_t total,
-                                                      unsigned long long* __restrict__ fcur,
-                                                      uint64_t* __restrict__ pkeys, uint32_t* __restrict__ plink,
-                                                      Counters* ctr) {
-  __shared__ uint64_t s_c;
-  constexpr int PER = SC_FINE / 256;
+__global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict__ rkey,
+                                                     const uint32_t* __restrict__ rlink,
+                                                     const uint32_t* __restrict__ rbkt,
+                                                     const unsigned long long* __restrict__ boff,
+                                                     const uint32_t* __restrict__ item_start, uint32_t fb,
+                                                     uint32_t sb, uint32_t mc, unsigned long long* __restrict__ scur,
+                                                     uint64_t* __restrict__ okey, uint32_t* __restrict__ olink,
+                                                     uint32_t* __restrict__ obkt, Counters* ctr) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);                              // [MID_CHUNK*NW]
+  uint32_t* slink = reinterpret_cast<uint32_t*>(skey + MID_CHUNK * NW);              // [MID_CHUNK]
+  uint32_t* sbkt = slink + MID_CHUNK;                                                // [MID_CHUNK]
+  unsigned long long* gbase = reinterpret_cast<unsigned long long*>(sbkt + MID_CHUNK);  // [nb]
+  const uint32_t nb = 1u << (fb - sb);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(gbase + nb);                          // [nb]
+  uint32_t* lofs = hist + nb;                                                        // [nb + 1]
+  uint32_t* istart = lofs + nb + 1;                                                  // [mc + 1]
+  __shared__ uint32_t sc[33];
+  __shared__ uint32_t s_t, s_p;
+  for (uint32_t j = threadIdx.x; j <= mc; j += blockDim.x) istart[j] = item_start[j];
+  __syncthreads();
+  const uint32_t nitems = istart[mc];
+  constexpr int PT = MID_CHUNK / 256;
   for (;;) {
-    if (threadIdx.x == 0) s_c = uint64_t(atomicAdd(&ctr->work_next, 1u)) * SC_FINE;
-    __syncthreads();
-    const uint64_t c0 = s_c;
-    __syncthreads();
-    if (c0 >= total) break;
-    uint32_t bk[PER];
-    uint64_t pos[PER];
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      const uint64_t i = c0 + uint64_t(q) * blockDim.x + threadIdx.x;
-      bk[q] = (i < total) ? rbkt[i] : NONE;
-    }
-#pragma unroll
-    for (int q = 0; q < PER; ++q) pos[q] = (bk[q] != NONE) ? atomicAdd(fcur + bk[q], 1ull) : 0ull;
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      const uint64_t i = c0 + uint64_t(q) * blockDim.x + threadIdx.x;
-      if (bk[q] != NONE) {
-        st_key<NW>(pkeys, pos[q], ld_key<NW>(rkey, i));
-        plink[pos[q]] = rlink[i];
+    if (threadIdx.x == 0) {
+      const uint32_t t = atomicAdd(&ctr->work_next, 1u);
+      uint32_t lo = 0, hi = mc;  // the partition p with istart[p] <= t < istart[p + 1]
+      while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (istart[mid] <= t) lo = mid;
+        else hi = mid;
       }
+      s_t = t;
+      s_p = lo;
+    }
+    __syncthreads();
+    const uint32_t t = s_t, p = s_p;
+    __syncthreads();
+    if (t >= nitems) break;
+    const unsigned long long pend = boff[uint64_t(p + 1) << fb];
+    const unsigned long long c0 = boff[uint64_t(p) << fb] + uint64_t(t - istart[p]) * MID_CHUNK;
+    const uint32_t cn = uint32_t(min(pend - c0, (unsigned long long)MID_CHUNK));
+    const uint32_t sub0 = p << (fb - sb);  // first sub-partition of partition p
+    // bucket ids of the chunk (in registers) and the counts per sub-partition
+    uint32_t bb[PT];
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const uint32_t i = uint32_t(q) * 256u + threadIdx.x;
+      bb[q] = (i < cn) ? rbkt[c0 + i] : 0u;
+    }
+    for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) hist[j] = 0;
+    __syncthreads();
+    // a record outside partition p would be a broken staging order: flag it
+    // and leave it out rather than index past the counts
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const uint32_t i = uint32_t(q) * 256u + threadIdx.x;
+      if (i < cn) {
+        const uint32_t bin = (bb[q] >> sb) - sub0;
+        if (bin < nb) atomicAdd(hist + bin, 1u);
+        else atomicOr(&ctr->err, ERR_INTERNAL);
+      }
+    }
+    __syncthreads();
+    // local offsets and one reservation per non-empty sub-partition
+    {
+      const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+      const uint32_t j0 = min(nb, threadIdx.x * per), j1 = min(nb, j0 + per);
+      uint32_t acc = 0;
+      for (uint32_t j = j0; j < j1; ++j) acc += hist[j];
+      uint32_t tot;
+      uint32_t pre = block_excl_scan(acc, sc, &tot);
+      for (uint32_t j = j0; j < j1; ++j) {
+        const uint32_t h = hist[j];
+        lofs[j] = pre;
+        gbase[j] = h ? atomicAdd(scur + sub0 + j, (unsigned long long)h) : 0ull;
+        pre += h;
+        hist[j] = 0;
+      }
+      if (threadIdx.x == 0) lofs[nb] = tot;
+    }
+    __syncthreads();
+    // place every record in its sub-partition's run of the staging area
+#pragma unroll
+    for (int q = 0; q < PT; ++q) {
+      const uint32_t i = uint32_t(q) * 256u + threadIdx.x;
+      const uint32_t bin = (bb[q] >> sb) - sub0;
+      if (i < cn && bin < nb) {
+        const uint32_t sl = lofs[bin] + atomicAdd(hist + bin, 1u);
+        st_key<NW>(skey, sl, ld_key<NW>(rkey, c0 + i));
+        slink[sl] = rlink[c0 + i];
+        sbkt[sl] = bb[q];
+      }
+    }
+    __syncthreads();
+    const uint32_t placed = lofs[nb];
+    for (uint32_t sl = threadIdx.x; sl < placed; sl += blockDim.x) {
+      const uint32_t bk = sbkt[sl];
+      const uint32_t bin = (bk >> sb) - sub0;
+      const uint64_t pos = gbase[bin] + (sl - lofs[bin]);
+      st_key<NW>(okey, pos, ld_key<NW>(skey, sl));
+      olink[pos] = slink[sl];
+      obkt[pos] = bk;
+    }
+    __syncthreads();
+  }
+}
+
+// Level 3: one block owns a sub-partition (2^sb buckets) and places each of
+// its records at its bucket's offset plus a rank from a shared-memory
+// cursor: no global atomics.  A sub-partition of at most `cap` records is
+// assembled in shared memory and written out as one contiguous range; a
+// larger one (a large repeat bucket) is placed straight into global memory.
+// Blocks take sub-partitions from a counter.
+template <int NW>
+__global__ void __launch_bounds__(512) k_scatter_sub(const uint64_t* __restrict__ ikey,
+                                                     const uint32_t* __restrict__ ilink,
+                                                     const uint32_t* __restrict__ ibkt,
+                                                     const unsigned long long* __restrict__ boff, uint32_t sb,
+                                                     uint32_t nsub, uint32_t cap, uint64_t* __restrict__ pkeys,
+                                                     uint32_t* __restrict__ plink, Counters* ctr) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);        // [cap * NW]
+  uint32_t* slink = reinterpret_cast<uint32_t*>(skey + size_t(cap) * NW);  // [cap]
+  __shared__ unsigned long long s_off[1 << SUB_MAX_BITS];
+  __shared__ uint32_t s_cur[1 << SUB_MAX_BITS];
+  __shared__ uint32_t s_sp;
+  const uint32_t nbk = 1u << sb;
+  constexpr int PER = 4;  // records per thread and pass: their loads are in flight together
+  for (;;) {
+    if (threadIdx.x == 0) s_sp = atomicAdd(&ctr->work_next, 1u);
+    __syncthreads();
+    const uint32_t sp = s_sp;
+    if (sp >= nsub) break;
+    const uint64_t b0 = uint64_t(sp) << sb;
+    for (uint32_t j = threadIdx.x; j < nbk; j += blockDim.x) {
+      s_off[j] = boff[b0 + j];
+      s_cur[j] = 0;
+    }
+    __syncthreads();
+    const unsigned long long lo = boff[b0], hi = boff[b0 + nbk];
+    const bool staged = hi - lo <= cap;
+    for (unsigned long long i0 = lo; i0 < hi; i0 += uint64_t(blockDim.x) * PER) {
+      uint32_t bk[PER];
+      Key<NW> kk[PER];
+      uint32_t ln[PER];
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const unsigned long long i = i0 + uint64_t(q) * blockDim.x + threadIdx.x;
+        if (i < hi) {
+          bk[q] = ibkt[i];
+          kk[q] = ld_key<NW>(ikey, i);
+          ln[q] = ilink[i];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const unsigned long long i = i0 + uint64_t(q) * blockDim.x + threadIdx.x;
+        if (i < hi) {
+          const uint32_t lb = bk[q] - uint32_t(b0);
+          if (lb >= nbk) {  // not this sub-partition's: a broken order upstream
+            atomicOr(&ctr->err, ERR_INTERNAL);
+            continue;
+          }
+          const uint64_t pos = s_off[lb] + atomicAdd(s_cur + lb, 1u);
+          if (staged) {
+            st_key<NW>(skey, pos - lo, kk[q]);
+            slink[pos - lo] = ln[q];
+          } else {
+            st_key<NW>(pkeys, pos, kk[q]);
+            plink[pos] = ln[q];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (staged) {
+      const uint32_t cnt = uint32_t(hi - lo);
+      for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+        st_key<NW>(pkeys, lo + t, ld_key<NW>(skey, t));
+        plink[lo + t] = slink[t];
+      }
+      __syncthreads();  // the staging area, s_off / s_cur / s_sp are reused
     }
   }
 }
 
 // ==================================================================== tiles
+
+// List-ranking entries: (pointer, distance) in one 64-bit word.
+__device__ __forceinline__ unsigned long long pk(uint32_t p, uint32_t o) {
+  return (static_cast<unsigned long long>(o) << 32) | p;
+}
+__device__ __forceinline__ uint32_t pk_p(unsigned long long v) { return uint32_t(v); }
+__device__ __forceinline__ uint32_t pk_o(unsigned long long v) { return uint32_t(v >> 32); }
+// A head's own entry carries HEAD_BIT in its pointer, so "reached a head" is
+// a property of the target entry, not a self-pointer (which a pointer running
+// around a cycle can also produce).  Entry counts stay below 2^31.
+constexpr uint32_t HEAD_BIT = 0x80000000u;
+__device__ __forceinline__ uint32_t ptr_of(unsigned long long v) { return pk_p(v) & ~HEAD_BIT; }
+__device__ __forceinline__ bool is_head_entry(unsigned long long v) { return (pk_p(v) & HEAD_BIT) != 0; }
+
 
 // In-tile indices: 16-bit for shared-memory tiles (capacity <= 32766), 32-bit
 // for oversized tiles worked in global scratch.  The top bit of A marks a
@@ -966,6 +1179,7 @@ template <int NW, typename IT, typename G>
 __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint64_t beg, uint32_t c,
                              uint32_t job) {
   constexpr uint32_t NONE_I = Ix<IT>::NONE, DUP_I = Ix<IT>::DUP, CNONE_I = Ix<IT>::CNONE;
+  constexpr uint32_t OPEN_S = NONE_I - 1u;  // an open segment that starts at an S-only copy
   const PrefMask pm = pref_mask(p.k);
   // this tile's hash slots: the power of two above c * lf / 100, at most the
   // carved table (32-bit arithmetic for shared-memory tiles, c <= 8192)
@@ -974,6 +1188,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     const uint32_t want = (sizeof(IT) == 2) ? (c * p.lf) / 100u : uint32_t((uint64_t(c) * p.lf) / 100u);
     const uint32_t x = want > c ? want : c + 1u;
     ts = 1u << (32 - __clz(x - 1u));
+    ts = ts < 4u ? 4u : ts;  // whole slot groups (the carved table holds at least 64)
     ts = ts < m.ts ? ts : m.ts;
   }
   const uint32_t tmask = ts - 1;
@@ -1001,47 +1216,130 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   G::sync();
   // ---- prefix table of the P copies (generate_hashmap, assembler.h:120-150):
   // one slot per distinct (k-1)-prefix; a prefix held by two copies marks the
-  // slot's copy DUP ("nullified")
-  for (uint32_t i = G::rank(); i < c; i += G::size()) {
-    const Key<NW> x = skey(m, i);
-    if (!(roles(x) & ROLE_P)) continue;
-    const Key<NW> pf = prefix_of(x, pm);
-    uint32_t h = key_hash(pf) & tmask;
-    for (uint32_t probe = 0; probe <= tmask; ++probe) {
-      const uint32_t cur = at_cas(m.T + h, NONE_I, i);
-      if (cur == NONE_I) break;
-      if (key_eq(prefix_of(skey(m, cur), pm), pf)) {
-        at_or(m.A + cur, DUP_I);
-        break;
+  // slot's copy DUP ("nullified").  Then the suffix lookups of the S copies
+  // (find_vtx_from_edge, assembler.h:89-111) and the in-degree counts
+  // ("count edges", assembler.h:180-188).
+  //
+  // Warp tiles of at most 256 copies use groups of four 16-bit slots, each
+  // an 8-bit copy index under an 8-bit fingerprint of the prefix hash: one
+  // 8-byte load reads a group, a key is loaded only on a fingerprint match,
+  // and a lookup ends at the first group with a free slot (inserts fill the
+  // groups in probe order, and nothing is removed).  Most lookups end in the
+  // first group, so the lanes of a warp stay together.  Larger tiles probe
+  // single slots holding a copy index.
+  constexpr bool WARP = std::is_same<G, WarpGroup>::value;
+  if (WARP && c <= 256u) {
+    constexpr uint32_t EMPTY = 0xFFFFu;
+    const uint32_t gmask = (ts >> 2) - 1u;
+    uint64_t* grp = reinterpret_cast<uint64_t*>(m.T);
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
+      const Key<NW> x = skey(m, i);
+      if (!(roles(x) & ROLE_P)) continue;
+      const Key<NW> pf = prefix_of(x, pm);
+      const uint32_t h = key_hash(pf);
+      const uint32_t fp = min(h >> 24, 254u);
+      const uint32_t mine = (fp << 8) | i;
+      uint32_t gi = h & gmask;
+      for (uint32_t probe = 0; probe <= gmask;) {
+        const uint64_t g = grp[gi];
+        bool done = false, free_slot = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t sl = uint32_t(g >> (16 * q)) & 0xFFFFu;
+          if (sl == EMPTY) {
+            free_slot = true;
+          } else if (!done && (sl >> 8) == fp && key_eq(prefix_of(skey(m, sl & 0xFFu), pm), pf)) {
+            at_or(m.A + (sl & 0xFFu), DUP_I);
+            done = true;
+          }
+        }
+        if (done) break;
+        if (!free_slot) {  // a full group: the next one
+          gi = (gi + 1) & gmask;
+          ++probe;
+          continue;
+        }
+        // claim the group's first free slot; if another lane took it first,
+        // read the group again (that lane may hold the same prefix)
+        const int q = (uint32_t(g) & 0xFFFFu) == EMPTY ? 0
+                      : (uint32_t(g >> 16) & 0xFFFFu) == EMPTY ? 1
+                      : (uint32_t(g >> 32) & 0xFFFFu) == EMPTY ? 2 : 3;
+        if (at_cas(m.T + 4u * gi + uint32_t(q), EMPTY, mine) == EMPTY) break;
       }
-      h = (h + 1) & tmask;
     }
-  }
-  G::sync();
-  // ---- suffix lookups of the S copies (find_vtx_from_edge, assembler.h:89-111)
-  // and in-degree counts ("count edges", assembler.h:180-188)
-  for (uint32_t i = G::rank(); i < c; i += G::size()) {
-    const Key<NW> x = skey(m, i);
-    if (!(roles(x) & ROLE_S)) continue;
-    const Key<NW> sf = suffix_of(x, pm);
-    uint32_t h = key_hash(sf) & tmask;
-    uint32_t cand = CNONE_I;
-    for (uint32_t probe = 0; probe <= tmask; ++probe) {
-      const uint32_t cur = m.T[h];
-      if (cur == NONE_I) break;
-      if (key_eq(prefix_of(skey(m, cur), pm), sf)) {
-        if (!(uint32_t(m.A[cur]) & DUP_I)) cand = cur;
-        break;
+    G::sync();
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
+      const Key<NW> x = skey(m, i);
+      if (!(roles(x) & ROLE_S)) continue;
+      const Key<NW> sf = suffix_of(x, pm);
+      const uint32_t h = key_hash(sf);
+      const uint32_t fp = min(h >> 24, 254u);
+      uint32_t gi = h & gmask;
+      uint32_t cand = CNONE_I;
+      for (uint32_t probe = 0; probe <= gmask; ++probe) {
+        const uint64_t g = grp[gi];
+        bool done = false, free_slot = false;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const uint32_t sl = uint32_t(g >> (16 * q)) & 0xFFFFu;
+          if (sl == EMPTY) {
+            free_slot = true;
+          } else if (!done && (sl >> 8) == fp && key_eq(prefix_of(skey(m, sl & 0xFFu), pm), sf)) {
+            const uint32_t cur = sl & 0xFFu;
+            if (!(uint32_t(m.A[cur]) & DUP_I)) cand = cur;
+            done = true;
+          }
+        }
+        if (done || free_slot) break;
+        gi = (gi + 1) & gmask;
       }
-      h = (h + 1) & tmask;
+      if (cand != CNONE_I) {
+        at_inc(m.B + cand);
+        m.P[cand] = IT(i);
+      }
+      m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
     }
-    if (cand != CNONE_I) {
-      at_inc(m.B + cand);
-      m.P[cand] = IT(i);
+    G::sync();
+  } else {
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
+      const Key<NW> x = skey(m, i);
+      if (!(roles(x) & ROLE_P)) continue;
+      const Key<NW> pf = prefix_of(x, pm);
+      uint32_t h = key_hash(pf) & tmask;
+      for (uint32_t probe = 0; probe <= tmask; ++probe) {
+        const uint32_t cur = at_cas(m.T + h, NONE_I, i);
+        if (cur == NONE_I) break;
+        if (key_eq(prefix_of(skey(m, cur), pm), pf)) {
+          at_or(m.A + cur, DUP_I);
+          break;
+        }
+        h = (h + 1) & tmask;
+      }
     }
-    m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
+    G::sync();
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
+      const Key<NW> x = skey(m, i);
+      if (!(roles(x) & ROLE_S)) continue;
+      const Key<NW> sf = suffix_of(x, pm);
+      uint32_t h = key_hash(sf) & tmask;
+      uint32_t cand = CNONE_I;
+      for (uint32_t probe = 0; probe <= tmask; ++probe) {
+        const uint32_t cur = m.T[h];
+        if (cur == NONE_I) break;
+        if (key_eq(prefix_of(skey(m, cur), pm), sf)) {
+          if (!(uint32_t(m.A[cur]) & DUP_I)) cand = cur;
+          break;
+        }
+        h = (h + 1) & tmask;
+      }
+      if (cand != CNONE_I) {
+        at_inc(m.B + cand);
+        m.P[cand] = IT(i);
+      }
+      m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
+    }
+    G::sync();
   }
-  G::sync();
   // ---- kept edges: u->v iff v is u's unique successor and u is v's only
   // predecessor ("write edges", assembler.h:189-197); rank init alongside
   for (uint32_t i = G::rank(); i < c; i += G::size()) {
@@ -1125,29 +1423,56 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   IT* lo_a = (ptr == m.Q) ? m.B : m.Q;
   IT* hi_a = (rnk == m.T) ? m.T + c : m.T;
   // ---- emission: closed segments (start has role P, end has role S) are
-  // whole unitigs; the others are stitched across tiles
-  // each thread takes copies rank, rank + size, ...: its lines are
-  // contiguous in the tile's output, in that order (the order of lines is
-  // free), and neighbouring threads read neighbouring shared words
+  // whole unitigs; the others are stitched across tiles.  Open segments that
+  // start at a P-role copy start a stitched line: they take head-pool ids;
+  // the others start at an S-only copy and take its cross index.
+  // A warp tile first packs its segment ends into a list (in A, which only
+  // marked the ends from here on), so that the per-segment loops keep every
+  // lane busy; a block tile walks its copies and skips the others.  Each
+  // thread's lines are contiguous in the tile's output, in the order the
+  // thread visits them (the order of lines is free).
+  uint32_t nend = c;
+  if constexpr (WARP) {
+    const uint32_t lane = G::rank();
+    nend = 0;
+    for (uint32_t base = 0; base < c; base += 32) {
+      const uint32_t i = base + lane;
+      const bool e = i < c && m.A[i] == NONE_I;
+      const uint32_t mask = __ballot_sync(0xFFFFFFFFu, e);
+      __syncwarp();  // the reads of this chunk before any write into it
+      if (e) m.A[nend + __popc(mask & ((1u << lane) - 1u))] = IT(i);
+      nend += uint32_t(__popc(mask));
+    }
+    __syncwarp();
+  }
+  // the segment end visited at step j (NONE_I: not an end)
+  auto end_at = [&](uint32_t j) -> uint32_t {
+    if constexpr (WARP) return m.A[j];
+    else return m.A[j] == NONE_I ? j : NONE_I;
+  };
   U3 mine{0, 0, 0};
-  for (uint32_t i = G::rank(); i < c; i += G::size()) {
-    if (m.A[i] != NONE_I) continue;
+  for (uint32_t j = G::rank(); j < nend; j += G::size()) {
+    const uint32_t i = end_at(j);
+    if (i == NONE_I) continue;
     const uint32_t s = ptr[i];
     const uint32_t len = uint32_t(rnk[i]) + 1;
-    const bool closed = (roles(skey(m, s)) & ROLE_P) && (roles(skey(m, i)) & ROLE_S);
+    const bool starts_p = (roles(skey(m, s)) & ROLE_P) != 0;
+    const bool closed = starts_p && (roles(skey(m, i)) & ROLE_S);
     if (closed) mine.a += uint64_t(k) + len;
-    else { mine.b += uint64_t(k) - 1 + len; mine.c += 1; }
+    else { mine.b += uint64_t(k) - 1 + len; mine.c += starts_p ? 1 : 0; }
   }
   U3 tot;
   U3 pre = G::scan3(mine, &tot);
   unsigned long long s_base[3];
   if (!G::reserve(p, job, tot, s_base)) return;
   const unsigned long long cbase = s_base[0], obase = s_base[1], sbase = s_base[2];
-  for (uint32_t i = G::rank(); i < c; i += G::size()) {
-    if (m.A[i] != NONE_I) continue;
+  for (uint32_t j = G::rank(); j < nend; j += G::size()) {
+    const uint32_t i = end_at(j);
+    if (i == NONE_I) continue;
     const uint32_t s = ptr[i];
     const uint32_t len = uint32_t(rnk[i]) + 1;
-    const bool closed = (roles(skey(m, s)) & ROLE_P) && (roles(skey(m, i)) & ROLE_S);
+    const bool starts_p = (roles(skey(m, s)) & ROLE_P) != 0;
+    const bool closed = starts_p && (roles(skey(m, i)) & ROLE_S);
     uint64_t loc;
     if (closed) {
       loc = pre.a;
@@ -1155,9 +1480,9 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
       pre.a += uint64_t(k) + len;
     } else {
       loc = pre.b;
-      m.P[s] = IT(pre.c);
+      m.P[s] = IT(starts_p ? uint32_t(pre.c) : OPEN_S);
       pre.b += uint64_t(k) - 1 + len;
-      pre.c += 1;
+      if (starts_p) pre.c += 1;
     }
     if constexpr (sizeof(IT) == 2) {
       lo_a[s] = IT(loc & 0xFFFFu);
@@ -1167,37 +1492,49 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     }
   }
   G::sync();
-  for (uint32_t i = G::rank(); i < c; i += G::size()) {
+  // per segment: its first k-mer in full, then its line break or, for an
+  // open segment, its record and links
+  for (uint32_t j = G::rank(); j < nend; j += G::size()) {
+    const uint32_t i = end_at(j);
+    if (i == NONE_I) continue;
     const uint32_t s = ptr[i];
     const uint32_t r = rnk[i];
     uint64_t loc = lo_a[s];
     if constexpr (sizeof(IT) == 2) loc |= uint64_t(hi_a[s]) << 16;
     const uint32_t sid = m.P[s];
-    const Key<NW> x = skey(m, i);
     char* dst = (sid == NONE_I) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
-    if (r == 0) {
-      spell_key<NW>(dst, x, k);
+    spell_key<NW>(dst, skey(m, s), k);
+    if (sid == NONE_I) {
+      dst[k + r] = '\n';
     } else {
-      dst[k - 1 + r] = acgt(key_char(x, k - 1));
+      // the segment's record under its id; a segment that ends at the P-only
+      // copy of cross k-mer ex is the predecessor of segment ex, so it
+      // writes ex's first ranking entry (itself, and the chars it adds to the
+      // line: all k - 1 + len of a line's first segment, len - 1 of the
+      // others, whose first k-mer ends the segment before)
+      const bool head = sid != OPEN_S;
+      const bool p_only = (roles(skey(m, i)) & ROLE_S) == 0;
+      const uint32_t g = head ? p.xcount + uint32_t(sbase) + sid : p.plink[beg + s];
+      const uint32_t ex = p_only ? p.plink[beg + i] : NONE;
+      SegRec rec;
+      rec.off_job = (obase + loc) | (static_cast<unsigned long long>(job) << SEG_OFF_BITS);
+      rec.len = r + 1;
+      rec.next = ex;
+      p.seg[g] = rec;
+      if (head) p.Xr[g] = pk(g | HEAD_BIT, 0);
+      if (p_only) p.Xr[ex] = pk(g, head ? uint32_t(k) + r : r);
     }
-    if (m.A[i] == NONE_I) {
-      if (sid == NONE_I) {
-        dst[k + r] = '\n';
-      } else {
-        const uint32_t g = uint32_t(sbase) + sid;
-        const bool s_only = (roles(skey(m, s)) & ROLE_P) == 0;
-        const bool p_only = (roles(x) & ROLE_S) == 0;
-        p.seg_off[g] = obase + loc;
-        p.seg_len[g] = r + 1;
-        p.seg_job[g] = job;
-        const uint32_t sx = s_only ? p.plink[beg + s] : NONE;
-        const uint32_t ex = p_only ? p.plink[beg + i] : NONE;
-        p.seg_sx[g] = sx;
-        p.seg_ex[g] = ex;
-        if (s_only) p.start_seg[sx] = g;
-        if (p_only) p.end_seg[ex] = g;
-      }
-    }
+  }
+  // every later copy of a segment adds its last char
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
+    const uint32_t r = rnk[i];
+    if (r == 0) continue;
+    const uint32_t s = ptr[i];
+    uint64_t loc = lo_a[s];
+    if constexpr (sizeof(IT) == 2) loc |= uint64_t(hi_a[s]) << 16;
+    const uint32_t sid = m.P[s];
+    char* dst = (sid == NONE_I) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
+    dst[k - 1 + r] = acgt(key_char(skey(m, i), k - 1));
   }
 }
 
@@ -1259,23 +1596,22 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
 }
 
 // ================================================================= stitch
+//
+// Open segments continue through cross k-mers: the segment that ends at the
+// P-only copy of cross k-mer x is followed by segment x (the one that starts
+// at x's S-only copy); both hold x, so every later segment of a line drops
+// its first k chars (write_unitigs4, compact.h:59-112).  The tiles write each
+// segment's record and the ranking's first state (every segment x has a
+// predecessor, written by the segment before it; a line's first segment is
+// a head), so ranking starts at once over the ids [0, X).  Line lengths are
+// written at the heads, scanned over the head pools (per job, in job order)
+// and each segment copies its chars to its line's base plus its offset.
 
-// next/prev/weight of each open segment.  A segment ending in a P-only copy
-// of cross k-mer x continues with the segment starting at x's S-only copy;
-// both hold x, so every later segment drops its first k chars
-// (write_unitigs4, compact.h:59-112).
-// Segment ids come from per-job pools; an unused id has length 0.
-__device__ __forceinline__ unsigned long long pk(uint32_t p, uint32_t o) {
-  return (static_cast<unsigned long long>(o) << 32) | p;
+// The chars a segment adds to its line: all k - 1 + len for a line's first
+// segment (a head-pool id), len - 1 for the others.
+__device__ __forceinline__ uint32_t seg_w(uint32_t s, uint32_t len, uint32_t nx, int k) {
+  return s < nx ? len - 1u : uint32_t(k) - 1u + len;
 }
-__device__ __forceinline__ uint32_t pk_p(unsigned long long v) { return uint32_t(v); }
-__device__ __forceinline__ uint32_t pk_o(unsigned long long v) { return uint32_t(v >> 32); }
-// A head's own entry carries HEAD_BIT in its pointer, so "reached a head" is
-// a property of the target entry, not a self-pointer (which a pointer running
-// around a cycle can also produce).  Entry counts stay below 2^31.
-constexpr uint32_t HEAD_BIT = 0x80000000u;
-__device__ __forceinline__ uint32_t ptr_of(unsigned long long v) { return pk_p(v) & ~HEAD_BIT; }
-__device__ __forceinline__ bool is_head_entry(unsigned long long v) { return (pk_p(v) & HEAD_BIT) != 0; }
 
 // First of c consecutive slots for each thread of a block that appends to a
 // shared list: one atomic per block.  A list counter that every block of the
@@ -1290,75 +1626,6 @@ __device__ __forceinline__ uint32_t block_append(uint32_t* count, uint32_t c, ui
   const uint32_t b = sc[32] + pre;
   __syncthreads();  // sc is reused by the next call
   return b;
-}
-
-// Segment links: next/prev through the cross k-mer at each open end, and
-// each segment's weight (the chars it adds to the line).  With X, the list
-// ranking's first state is written too, from the predecessor's side: a
-// segment without a predecessor is a head, and every segment s with a
-// successor t sets X[t] = (s, w[s]) - every cross k-mer joins exactly one
-// segment ending there to one starting there, so each entry is written once.
-// Segments with a predecessor go to the active list.
-__global__ void __launch_bounds__(256) k_seg_link(uint32_t S, const uint32_t* __restrict__ seg_sx,
-                           const uint32_t* __restrict__ seg_ex, const uint32_t* __restrict__ seg_len,
-                           const uint32_t* __restrict__ start_seg, const uint32_t* __restrict__ end_seg,
-                           uint32_t* __restrict__ next, uint32_t* __restrict__ prev,
-                           uint32_t* __restrict__ w, int k, unsigned long long* __restrict__ X,
-                           uint32_t* __restrict__ act, uint32_t* act_count) {
-  constexpr int PER = 4;  // segments per thread and pass: their gathers are in flight together
-  __shared__ uint32_t sc[33];
-  const uint64_t B = blockDim.x;
-  // whole blocks iterate together (block_append needs every thread)
-  for (uint64_t b0 = uint64_t(blockIdx.x) * B * PER; b0 < S; b0 += uint64_t(gridDim.x) * B * PER) {
-    uint32_t sid[PER], len[PER], ex[PER], sx[PER], nx[PER], pv[PER];
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      const uint64_t i = b0 + uint64_t(q) * B + threadIdx.x;
-      const bool in = i < S;
-      sid[q] = in ? uint32_t(i) : NONE;
-      // the three slot loads are issued together; an unused slot's ends are
-      // not used
-      len[q] = in ? seg_len[i] : 0u;
-      ex[q] = in ? seg_ex[i] : NONE;
-      sx[q] = in ? seg_sx[i] : NONE;
-    }
-#pragma unroll
-    for (int q = 0; q < PER; ++q)
-      if (!len[q]) ex[q] = sx[q] = NONE;
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      nx[q] = (ex[q] == NONE) ? NONE : start_seg[ex[q]];
-      pv[q] = (sx[q] == NONE) ? NONE : end_seg[sx[q]];
-    }
-    uint32_t tails = 0;  // bit q: segment q has a predecessor
-#pragma unroll
-    for (int q = 0; q < PER; ++q) {
-      const uint32_t s = sid[q];
-      if (s == NONE) continue;
-      if (len[q] == 0) {  // an unused slot of the segment pool
-        next[s] = NONE;
-        prev[s] = NONE;
-        w[s] = 0;
-        if (X) X[s] = pk(s | HEAD_BIT, 0);
-      } else {
-        const uint32_t ws = (pv[q] == NONE) ? uint32_t(k) - 1u + len[q] : len[q] - 1u;
-        next[s] = nx[q];
-        prev[s] = pv[q];
-        w[s] = ws;
-        if (X) {
-          if (pv[q] == NONE) X[s] = pk(s | HEAD_BIT, 0);
-          if (nx[q] != NONE) X[nx[q]] = pk(s, ws);
-          if (pv[q] != NONE) tails |= 1u << q;
-        }
-      }
-    }
-    if (X) {
-      uint32_t slot = block_append(act_count, uint32_t(__popc(tails)), sc);
-#pragma unroll
-      for (int q = 0; q < PER; ++q)
-        if ((tails >> q) & 1u) act[slot++] = sid[q];
-    }
-  }
 }
 
 // X[v] = (start pointer, weight distance); heads point at themselves.
@@ -1386,15 +1653,16 @@ __global__ void __launch_bounds__(256) k_rank_init(const uint32_t* __restrict__ 
   }
 }
 
-// One round of asynchronous pointer jumping over the active list.  Entries
-// are (pointer, distance) pairs in one 64-bit word, so a concurrent reader
-// always sees a consistent pair; the list keeps the entries whose pointer
-// does not yet reach a head.
+// One round of asynchronous pointer jumping over the active list (act ==
+// nullptr: the first round, over the ids [0, n0)).  Entries are (pointer,
+// distance) pairs in one 64-bit word, so a concurrent reader always sees a
+// consistent pair; the list keeps the entries whose pointer does not yet
+// reach a head.
 __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restrict__ X, const uint32_t* __restrict__ act,
-                             const uint32_t* act_count, uint32_t* __restrict__ act_out,
+                             const uint32_t* act_count, uint32_t n0, uint32_t* __restrict__ act_out,
                              uint32_t* act_out_count) {
   __shared__ uint32_t sc[33];
-  const uint32_t na = *act_count;
+  const uint32_t na = act ? *act_count : n0;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   // whole blocks iterate together (block_append needs every thread)
   for (uint64_t j0 = uint64_t(blockIdx.x) * blockDim.x; j0 < na; j0 += stride) {
@@ -1402,7 +1670,7 @@ __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restri
     bool keep = false;
     uint32_t s = 0;
     if (j < na) {
-      s = act[j];
+      s = act ? act[j] : uint32_t(j);
       const unsigned long long v = reinterpret_cast<volatile unsigned long long*>(X)[s];
       const unsigned long long u = reinterpret_cast<volatile unsigned long long*>(X)[ptr_of(v)];
       if (!is_head_entry(u)) {  // not yet pointing at a head
@@ -1418,42 +1686,61 @@ __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restri
 }
 
 // Line length of each chain, stored at its head (every live chain has one
-// tail, which writes it; the array is zeroed before).
-__global__ void k_chain_len(uint32_t S, const uint32_t* __restrict__ seg_len, const unsigned long long* __restrict__ X,
-                            const uint32_t* __restrict__ next, const uint32_t* __restrict__ w,
-                            const uint8_t* __restrict__ oncycle, uint32_t* __restrict__ linelen) {
+// tail, which writes it; the array is zeroed before).  A line's tail starts
+// at an S-only copy (a line's first segment always continues).
+__global__ void k_chain_len(uint32_t S, const SegRec* __restrict__ seg, const unsigned long long* __restrict__ X,
+                            const uint8_t* __restrict__ oncycle, uint32_t nx, int k, uint32_t* __restrict__ linelen,
+                            Counters* ctr) {
   constexpr int PER = 4;  // slots per thread and pass: their loads are in flight together
   const uint64_t span = uint64_t(gridDim.x) * blockDim.x;
   for (uint64_t s0 = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s0 < S; s0 += span * PER) {
-    uint32_t len[PER], nx[PER], ws[PER];
+    SegRec r[PER];
     uint8_t cyc[PER];
     unsigned long long v[PER];
 #pragma unroll
     for (int q = 0; q < PER; ++q) {
       const uint64_t s = s0 + uint64_t(q) * span;
       const bool in = s < S;
-      len[q] = in ? seg_len[s] : 0u;
-      nx[q] = in ? next[s] : NONE;
-      ws[q] = in ? w[s] : 0u;
+      r[q] = in ? seg[s] : SegRec{0ull, 0u, 0u};
       cyc[q] = in ? oncycle[s] : uint8_t(1);
       v[q] = in ? X[s] : 0ull;
     }
 #pragma unroll
-    for (int q = 0; q < PER; ++q)
-      if (len[q] && nx[q] == NONE && !cyc[q]) linelen[ptr_of(v[q])] = pk_o(v[q]) + ws[q] + 1u;
+    for (int q = 0; q < PER; ++q) {
+      if (!r[q].len || r[q].next != NONE || cyc[q]) continue;
+      const uint32_t h = ptr_of(v[q]);
+      const uint32_t s = uint32_t(s0 + uint64_t(q) * span);
+      if (h < nx || h >= S) {
+        atomicOr(&ctr->err, ERR_INTERNAL);
+        continue;
+      }
+      linelen[h - nx] = pk_o(v[q]) + seg_w(s, r[q].len, nx, k) + 1u;
+    }
+  }
+}
+
+// Each head's line base in the output: its job's region, after the job's
+// closed lines, at the job's running offset (the scan of line lengths over
+// the head pools, which lie in job order).
+__global__ void k_line_base(uint32_t H, const SegRec* __restrict__ heads, const JobTab* __restrict__ jobs,
+                            const unsigned long long* __restrict__ jclosed, const unsigned long long* __restrict__ loff,
+                            unsigned long long* __restrict__ lbase) {
+  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
+    const SegRec r = heads[h];
+    if (!r.len) continue;
+    const uint32_t job = uint32_t(r.off_job >> SEG_OFF_BITS);
+    const JobTab& J = jobs[job];
+    lbase[h] = J.obase + jclosed[job] + (loff[h] - loff[J.seg_base]);
   }
 }
 
 // Copy each segment's chars into its line.  A warp takes 32 consecutive
 // segments: each lane resolves one segment's source, destination and length
-// (independent loads, issued together), then groups of 8 lanes copy the
-// segments word by word.
+// (its record and ranking entry, then its head's line base), then groups of
+// 8 lanes copy the segments word by word.
 __global__ void __launch_bounds__(256) k_seg_copy(
-    uint32_t S, const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
-    const JobTab* __restrict__ jobs, const unsigned long long* __restrict__ jclosed,
-    const unsigned long long* __restrict__ X, const uint32_t* __restrict__ next,
-    const uint32_t* __restrict__ prev, const uint32_t* __restrict__ w, const uint8_t* __restrict__ oncycle,
-    const unsigned long long* __restrict__ seg_off, const unsigned long long* __restrict__ loff,
+    uint32_t S, const SegRec* __restrict__ seg, const unsigned long long* __restrict__ X,
+    const uint8_t* __restrict__ oncycle, uint32_t nx, const unsigned long long* __restrict__ lbase,
     const char* __restrict__ segchars, char* __restrict__ out, int k) {
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -1464,20 +1751,17 @@ __global__ void __launch_bounds__(256) k_seg_copy(
     uint64_t dst = 0, src = 0;
     uint32_t nb = 0, last = 0;
     if (live) {
-      // every per-slot load is issued before the test; the gathers that
-      // depend on them only for live segments
-      const uint32_t len = seg_len[s], job = seg_job[s], pv = prev[s], ws = w[s], nx = next[s];
+      // the per-slot loads are issued before the test; the line-base
+      // gather only for live segments
+      const SegRec r = seg[s];
       const uint8_t cyc = oncycle[s];
       const unsigned long long v = X[s];
-      const unsigned long long so = seg_off[s];
-      live = len != 0 && !cyc;
+      live = r.len != 0 && !cyc;
       if (live) {
-        const uint64_t obase = jobs[job].obase;
-        const uint32_t sb = jobs[job].seg_base;
-        dst = obase + jclosed[job] + (loff[ptr_of(v)] - loff[sb]) + pk_o(v);
-        src = so + ((pv == NONE) ? 0u : uint32_t(k));
-        nb = ws;
-        last = nx == NONE;
+        dst = lbase[ptr_of(v) - nx] + pk_o(v);
+        src = (r.off_job & SEG_OFF_MASK) + (s < nx ? uint32_t(k) : 0u);
+        nb = seg_w(s, r.len, nx, k);
+        last = r.next == NONE;
       }
     }
     // groups of 8 lanes: group g copies, one after another, the segments
@@ -1522,15 +1806,14 @@ __global__ void k_mark_cycle(const uint32_t* __restrict__ act, const uint32_t* a
     oncycle[act[j]] = 1;
 }
 
-// Cycles of segments (rare): one thread spells each cycle starting at its
-// smallest k-mer.  The cycle's distinct k-mers are the last chars of each
-// segment after its first k-mer, read circularly.
+// Cycles of segments (rare; they hold only segments that start at S-only
+// copies): one thread spells each cycle starting at its smallest k-mer.  The
+// cycle's distinct k-mers are the last chars of each segment after its first
+// k-mer, read circularly.
 template <int NW>
 __global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restrict__ act, uint32_t na,
-                             uint8_t* __restrict__ oncycle, const uint32_t* __restrict__ next,
-                             const uint32_t* __restrict__ seg_len, const uint32_t* __restrict__ seg_job,
+                             uint8_t* __restrict__ oncycle, const SegRec* __restrict__ seg,
                              const JobTab* __restrict__ jobs, unsigned long long* __restrict__ jout,
-                             const unsigned long long* __restrict__ seg_off,
                              const char* __restrict__ segchars, char* __restrict__ out, int k) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
   for (uint32_t j = 0; j < na; ++j) {
@@ -1540,10 +1823,10 @@ __global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restri
     uint64_t N = 0;
     uint32_t s = s0, steps = 0;
     do {
-      N += seg_len[s] - 1u;
+      N += seg[s].len - 1u;
       oncycle[s] = 2;
-      s = next[s];
-    } while (s != s0 && s != NONE && ++steps <= S);
+      s = seg[s].next;
+    } while (s != s0 && s < S && ++steps <= S);
     if (s != s0 || N == 0) {
       atomicOr(&ctr->err, ERR_INTERNAL);
       continue;
@@ -1553,10 +1836,11 @@ __global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restri
     auto at = [&](uint64_t q) -> char {
       uint32_t t = s0;
       for (uint32_t guard = 0; guard <= S; ++guard) {
-        const uint64_t m = seg_len[t] - 1u;
-        if (q < m) return segchars[seg_off[t] + k + q];
+        const SegRec r = seg[t];
+        const uint64_t m = r.len - 1u;
+        if (q < m) return segchars[(r.off_job & SEG_OFF_MASK) + k + q];
         q -= m;
-        t = next[t];
+        t = r.next;
       }
       return 'A';
     };
@@ -1580,7 +1864,7 @@ __global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restri
       if (key_lt(x, bk)) { bk = x; best = q; }
     }
     const uint64_t len = uint64_t(k) + N;  // k + (N - 1) chars + '\n'
-    const uint32_t job = seg_job[s0];
+    const uint32_t job = uint32_t(seg[s0].off_job >> SEG_OFF_BITS);
     const unsigned long long o = atomicAdd(jout + job, len);
     if (o + len > jobs[job].ocap) {
       atomicOr(&ctr->err, ERR_CAPACITY);
@@ -1594,7 +1878,7 @@ __global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restri
 }
 
 // After the copy: each job's byte count = closed lines + stitched lines
-// (the scan total over its segment pool range).
+// (the scan total over its head pool).
 __global__ void k_job_finish(const JobTab* __restrict__ jobs, uint32_t njobs,
                              const unsigned long long* __restrict__ jclosed,
                              const unsigned long long* __restrict__ loff, unsigned long long* __restrict__ jout) {
@@ -1643,6 +1927,31 @@ __global__ void k_hec_level0(HecPool h, const uint32_t* __restrict__ prev, const
     h.prv[u] = prev[u];
     h.nxt[u] = next[u];
     h.wt[u] = w ? w[u] : 1u;
+    h.first0[u] = uint32_t(u);
+  }
+}
+
+// Level 0 from the fused path's segments: next from the records, prev from
+// the first ranking state the tiles wrote (ids [0, nx) only: a line's first
+// segment has none), weights from the lengths.  Unused head-pool ids have
+// length 0 and stay isolated.
+__global__ void k_hec_level0_seg(HecPool h, const SegRec* __restrict__ seg, const unsigned long long* __restrict__ X0,
+                                 uint64_t S, uint32_t nx, int k) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    h.lb[0] = 0;
+    h.ln[0] = uint32_t(S);
+  }
+  for (uint64_t u = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; u < S; u += uint64_t(gridDim.x) * blockDim.x) {
+    const SegRec r = seg[u];
+    uint32_t pv = NONE, nx_ = NONE, w = 0;
+    if (r.len) {
+      pv = (u < nx) ? ptr_of(X0[u]) : NONE;
+      nx_ = r.next;
+      w = seg_w(uint32_t(u), r.len, nx, k);
+    }
+    h.prv[u] = pv;
+    h.nxt[u] = nx_;
+    h.wt[u] = w;
     h.first0[u] = uint32_t(u);
   }
 }
@@ -2073,17 +2382,17 @@ static void launch_pack(Env& e, const JobTab* jobs, const JobTab* one, uint32_t 
   if (fz && one)
     k_pack<NW, true, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
                                                         fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
-                                                        fz->jcross, &e.ctr->count_ovf);
+                                                        fz->jcross);
   else if (fz)
     k_pack<NW, true, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
                                                        fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
-                                                       fz->jcross, &e.ctr->count_ovf);
+                                                       fz->jcross);
   else if (one)
     k_pack<NW, false, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
-                                                         0, 0, nullptr, nullptr, nullptr, nullptr, nullptr);
+                                                         0, 0, nullptr, nullptr, nullptr, nullptr);
   else
     k_pack<NW, false, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
-                                                        0, 0, nullptr, nullptr, nullptr, nullptr, nullptr);
+                                                        0, 0, nullptr, nullptr, nullptr, nullptr);
 }
 
 // Grow-only device buffers for the job table and the per-job counters.
@@ -2370,8 +2679,8 @@ static size_t scatter_stage_bytes(uint64_t copies, int nw) { return copies * (8u
 
 // tile plan + scatter of every k-mer into its bucket(s).  stage: staging
 // records for level 1 (scatter_stage_bytes).
-static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, int nw, int ids_mode,
-                            uint64_t* pkeys, uint32_t* plink, char* stage, uint64_t copies) {
+// Tiles from the bucket counts: next-fit runs of whole buckets.
+static int plan_tiles(Env& e, const Front& f, const Plan& P) {
   const uint64_t M = P.M;
   const int gm = grid_for(e, M, 256);
   e.launches += 2 + 6;
@@ -2385,46 +2694,161 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
   }
   scan_excl<uint32_t, uint32_t>(f.flag, M, f.fidx, reinterpret_cast<uint32_t*>(f.scan_tmp), e.stream);
   k_tile_write<<<gm, 256, 0, e.stream>>>(f.flag, f.fidx, f.boff, uint32_t(M), P.jb, f.tile_begin, f.tile_job, e.ctr);
-  UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
-  if (n > 0) {
-    uint32_t mcb, fb;
-    scatter_split(P.bits, mcb, fb);
-    const uint32_t mc = 1u << mcb;
-    uint64_t* rkey = reinterpret_cast<uint64_t*>(stage);
-    uint32_t* rlink = reinterpret_cast<uint32_t*>(stage + copies * 8ull * nw);
-    uint32_t* rbkt = rlink + copies;
-    e.launches += 1;
-    k_coarse_init<<<grid_for(e, mc, 256), 256, 0, e.stream>>>(f.boff, fb, mc, f.cursor);
-    const uint64_t chunk = (nw == 1) ? sc_chunk<1>() : sc_chunk<2>();
-    const size_t sm1 = size_t(2 * chunk) * (8 * nw + 8) + size_t(mc) * 16 + 16;
-    int r0 = allow_max_smem(e, k_scatter_coarse<1>);
-    if (!r0) r0 = allow_max_smem(e, k_scatter_coarse<2>);
-    if (r0) return r0;
-    // one wave of resident CTAs (the chunks are strided statically)
-    int o1 = 0;
-    if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<1>, 256, sm1));
-    else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<2>, 256, sm1));
-    if (o1 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
-    const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + chunk - 1) / chunk,
-                                                                uint64_t(e.sm_count) * uint64_t(o1))));
-    UC_CK(cudaMemcpyAsync(f.fcur, f.boff, M * 8, cudaMemcpyDeviceToDevice, e.stream));
-    UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
-    const int g2 = e.sm_count * 8;
-    e.launches += 2;
-    if (nw == 1) {
-      k_scatter_coarse<1><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
-      k_scatter_fine<1><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, f.fcur, pkeys, plink, e.ctr);
-    } else {
-      k_scatter_coarse<2><<<g1, 256, sm1, e.stream>>>(f.keys, f.b1, f.b2, n, fb, mc, f.cursor, rkey, rlink, rbkt, ids_mode, e.ctr);
-      k_scatter_fine<2><<<g2, 256, 0, e.stream>>>(rkey, rlink, rbkt, copies, f.fcur, pkeys, plink, e.ctr);
-    }
-    UC_CK(cudaGetLastError());
-  }
-  ++e.launches;
-  k_classify<<<grid_for(e, M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, P.wcap, P.cap, f.wlist, f.blist,
-                                                         f.big_list, f.big_size, nw, P.lf);
   UC_CK(cudaGetLastError());
   return UC_OK;
+}
+
+// The three placement levels of the bucketed copies.  Level 1
+// (k_scatter_coarse) writes region r1; then either level 2 (k_scatter_mid)
+// writes r2 and level 3 (k_scatter_sub) writes back into r1, or, where a
+// coarse partition is already small, level 3 writes r2 straight away.  Both
+// regions hold scatter_stage_bytes(copies, nw); the final copies (pkeys,
+// plink) are the key and link arrays of the region level 3 wrote.  Level 1
+// may run over the k-mers in several launches (the streamed path's chunks):
+// its cursors and the cross-index counter carry over.
+struct Scatter {
+  uint32_t mcb = 0, fb = 0, mc = 0, sb = 0, nsub = 0, cap3 = 0;
+  bool mid = false;
+  int nw = 1;
+  uint64_t copies = 0;
+  uint64_t *k1 = nullptr, *k2 = nullptr;
+  uint32_t *l1 = nullptr, *l2 = nullptr, *b1 = nullptr, *b2 = nullptr;
+};
+
+static int scatter_begin(Env& e, const Front& f, const Plan& P, int nw, char* r1, char* r2, uint64_t copies,
+                         Scatter& sc) {
+  const uint64_t M = P.M;
+  sc.nw = nw;
+  sc.copies = copies;
+  auto region = [&](char* base, uint64_t*& key, uint32_t*& link, uint32_t*& bkt) {
+    key = reinterpret_cast<uint64_t*>(base);
+    link = reinterpret_cast<uint32_t*>(base + copies * 8ull * nw);
+    bkt = link + copies;
+  };
+  region(r1, sc.k1, sc.l1, sc.b1);
+  region(r2, sc.k2, sc.l2, sc.b2);
+  scatter_split(P.bits, sc.mcb, sc.fb);
+  sc.mc = 1u << sc.mcb;
+  // level-3 staging holds cap3 records (two CTAs per SM); sub-partitions of
+  // about half that many copies, at most 2^SUB_MAX_BITS buckets and at most
+  // MID_MAX_BINS of them per coarse partition
+  sc.cap3 = (nw == 1) ? 8192u : 4096u;
+  const double avg = double(copies) / double(M);
+  int sbi = avg > 0 ? int(std::lround(std::log2(0.5 * sc.cap3 / avg))) : SUB_MAX_BITS;
+  sbi = std::min(sbi, SUB_MAX_BITS);
+  sbi = std::min(sbi, int(sc.fb));
+  sbi = std::max(sbi, int(sc.fb) - int(std::log2(double(MID_MAX_BINS))));
+  sbi = std::max(sbi, 0);
+  if (sbi > SUB_MAX_BITS) return e.fail(UC_EINTERNAL, "bucket count beyond the three scatter levels");
+  sc.sb = uint32_t(sbi);
+  sc.mid = sc.sb < sc.fb;
+  sc.nsub = uint32_t(M >> sc.sb);
+  int r0 = allow_max_smem(e, k_scatter_coarse<1>);
+  if (!r0) r0 = allow_max_smem(e, k_scatter_coarse<2>);
+  if (!r0) r0 = allow_max_smem(e, k_scatter_mid<1>);
+  if (!r0) r0 = allow_max_smem(e, k_scatter_mid<2>);
+  if (!r0) r0 = allow_max_smem(e, k_scatter_sub<1>);
+  if (!r0) r0 = allow_max_smem(e, k_scatter_sub<2>);
+  if (r0) return r0;
+  UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
+  e.launches += 1;
+  k_coarse_init<<<grid_for(e, sc.mc, 256), 256, 0, e.stream>>>(f.boff, sc.fb, sc.mc, f.cursor);
+  UC_CK(cudaGetLastError());
+  return UC_OK;
+}
+
+static int scatter_l1(Env& e, const Front& f, const Scatter& sc, const uint64_t* keys, const uint32_t* b1,
+                      const uint32_t* b2, uint64_t n, int ids_mode) {
+  if (n == 0) return UC_OK;
+  const int nw = sc.nw;
+  const uint64_t chunk = (nw == 1) ? sc_chunk<1>() : sc_chunk<2>();
+  const size_t sm1 = size_t(2 * chunk) * (8 * nw + 8) + size_t(sc.mc) * 16 + 16;
+  // one wave of resident CTAs (the chunks are strided statically)
+  int o1 = 0;
+  if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<1>, 256, sm1));
+  else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<2>, 256, sm1));
+  if (o1 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
+  const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + chunk - 1) / chunk,
+                                                              uint64_t(e.sm_count) * uint64_t(o1))));
+  e.launches += 1;
+  if (nw == 1)
+    k_scatter_coarse<1><<<g1, 256, sm1, e.stream>>>(keys, b1, b2, n, sc.fb, sc.mc, f.cursor, sc.k1, sc.l1, sc.b1,
+                                                    ids_mode, e.ctr);
+  else
+    k_scatter_coarse<2><<<g1, 256, sm1, e.stream>>>(keys, b1, b2, n, sc.fb, sc.mc, f.cursor, sc.k1, sc.l1, sc.b1,
+                                                    ids_mode, e.ctr);
+  UC_CK(cudaGetLastError());
+  return UC_OK;
+}
+
+static int scatter_finish(Env& e, const Front& f, const Scatter& sc, uint64_t*& pkeys, uint32_t*& plink) {
+  const int nw = sc.nw;
+  pkeys = sc.k2;
+  plink = sc.l2;
+  if (sc.copies == 0) return UC_OK;
+  if (sc.mid) {
+    const uint32_t nb = 1u << (sc.fb - sc.sb);
+    uint32_t* item_start = reinterpret_cast<uint32_t*>(f.cursor + sc.mc);
+    const size_t sm2 = size_t(MID_CHUNK) * (8 * nw + 8) + size_t(nb) * 16 + 4 + size_t(sc.mc + 1) * 4;
+    int o2 = 0;
+    if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_scatter_mid<1>, 256, sm2));
+    else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_scatter_mid<2>, 256, sm2));
+    if (o2 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
+    e.launches += 3;
+    k_mid_items<<<1, 256, 0, e.stream>>>(f.boff, sc.fb, sc.mc, item_start);
+    k_coarse_init<<<grid_for(e, sc.nsub, 256), 256, 0, e.stream>>>(f.boff, sc.sb, sc.nsub, f.fcur);
+    UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
+    if (nw == 1)
+      k_scatter_mid<1><<<e.sm_count * o2, 256, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start, sc.fb, sc.sb,
+                                                                sc.mc, f.fcur, sc.k2, sc.l2, sc.b2, e.ctr);
+    else
+      k_scatter_mid<2><<<e.sm_count * o2, 256, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start, sc.fb, sc.sb,
+                                                                sc.mc, f.fcur, sc.k2, sc.l2, sc.b2, e.ctr);
+    pkeys = sc.k1;
+    plink = sc.l1;
+  }
+  const uint64_t* ik = sc.mid ? sc.k2 : sc.k1;
+  const uint32_t* il = sc.mid ? sc.l2 : sc.l1;
+  const uint32_t* ib = sc.mid ? sc.b2 : sc.b1;
+  UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
+  e.launches += 1;
+  const size_t sm3 = size_t(sc.cap3) * (8 * nw + 4);
+  int o3 = 0;
+  if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_scatter_sub<1>, 512, sm3));
+  else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o3, k_scatter_sub<2>, 512, sm3));
+  if (o3 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
+  const int g3 = int(std::min<uint64_t>(sc.nsub, uint64_t(e.sm_count) * uint64_t(o3)));
+  if (nw == 1)
+    k_scatter_sub<1><<<g3, 512, sm3, e.stream>>>(ik, il, ib, f.boff, sc.sb, sc.nsub, sc.cap3, pkeys, plink, e.ctr);
+  else
+    k_scatter_sub<2><<<g3, 512, sm3, e.stream>>>(ik, il, ib, f.boff, sc.sb, sc.nsub, sc.cap3, pkeys, plink, e.ctr);
+  UC_CK(cudaGetLastError());
+  return UC_OK;
+}
+
+// Sort the tiles [t0, t1) (clipped to the tile count) into their tiers.
+static int classify_tiles(Env& e, const Front& f, const Plan& P, int nw, uint32_t t0 = 0,
+                          uint32_t t1 = 0xFFFFFFFFu) {
+  ++e.launches;
+  k_classify<<<grid_for(e, P.M, 256), 256, 0, e.stream>>>(f.tile_begin, e.ctr, P.wcap, P.cap, f.wlist, f.blist,
+                                                           f.big_list, f.big_size, nw, P.lf, t0, t1);
+  UC_CK(cudaGetLastError());
+  return UC_OK;
+}
+
+// Tiles, then the bucketed copies of all k-mers in one pass.
+static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, int nw, int ids_mode,
+                            char* r1, char* r2, uint64_t copies, uint64_t*& pkeys, uint32_t*& plink) {
+  int r = plan_tiles(e, f, P);
+  if (r) return r;
+  Scatter sc;
+  r = scatter_begin(e, f, P, nw, r1, r2, copies, sc);
+  if (r) return r;
+  r = scatter_l1(e, f, sc, f.keys, f.b1, f.b2, n, ids_mode);
+  if (r) return r;
+  r = scatter_finish(e, f, sc, pkeys, plink);
+  if (r) return r;
+  return classify_tiles(e, f, P, nw);
 }
 
 template <int NW>
@@ -2529,13 +2953,14 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   uint64_t copies = 0;
   r = bucket_offsets(e, f, P.M, copies);
   if (r) return r;
-  r = e.reserve(1, copies * (8 * nw + 4) + scatter_stage_bytes(copies, nw) + 4096);
+  r = e.reserve(1, 2 * scatter_stage_bytes(copies, nw) + 4096);
   if (r) return r;
-  uint64_t* pkeys = static_cast<uint64_t*>(e.take(1, copies * 8 * nw));
-  uint32_t* plink = static_cast<uint32_t*>(e.take(1, copies * 4));
-  char* stage = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
-  if (!stage) return e.fail(UC_EBUDGET, "back arena overflow");
-  r = plan_and_scatter(e, f, P, n, nw, 1, pkeys, plink, stage, copies);
+  char* region1 = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  char* region2 = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  if (!region2) return e.fail(UC_EBUDGET, "back arena overflow");
+  uint64_t* pkeys = nullptr;
+  uint32_t* plink = nullptr;
+  r = plan_and_scatter(e, f, P, n, nw, 1, region1, region2, copies, pkeys, plink);
   if (r) return r;
   TileParams tp{};
   tp.pkeys = pkeys;
@@ -2619,13 +3044,15 @@ static int run_graph(Env& e, int slot, uint64_t key, F&& body) {
   return UC_OK;
 }
 
-// prefilled: X, act0 and cnt[0] were written by k_seg_link.
+// first_n >= 0: X already holds the first state (written by the tiles) and
+// the first round runs over the ids [0, first_n).
 static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t nmax, bool count_on_device,
                       unsigned long long* X, uint32_t* act0, uint32_t* act1, uint32_t* cnt, uint32_t& rounds,
-                      uint32_t*& act_final, uint32_t*& cnt_final, bool prefilled = false) {
+                      uint32_t*& act_final, uint32_t*& cnt_final, int64_t first_n = -1) {
   rounds = 2;
   for (uint64_t t = 1; t < nmax; t <<= 1) ++rounds;
   const int grid = grid_for(e, nmax ? nmax : 1, 256);
+  const bool prefilled = first_n >= 0;
   if (prefilled) {
     UC_CK(cudaMemsetAsync(cnt + 1, 0, rounds * 4, e.stream));
   } else {
@@ -2636,7 +3063,9 @@ static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t 
   uint32_t* lists[2] = {act0, act1};
   for (uint32_t r = 0; r < rounds; ++r) {
     ++e.launches;
-    k_rank_round<<<grid, 256, 0, e.stream>>>(X, lists[r & 1], cnt + r, lists[(r + 1) & 1], cnt + r + 1);
+    const uint32_t* in = (r == 0 && prefilled) ? nullptr : lists[r & 1];
+    k_rank_round<<<grid, 256, 0, e.stream>>>(X, in, cnt + r, prefilled ? uint32_t(first_n) : 0u,
+                                             lists[(r + 1) & 1], cnt + r + 1);
   }
   UC_CK(cudaGetLastError());
   act_final = lists[rounds & 1];
@@ -2674,13 +3103,16 @@ static uint32_t hec_rounds(const Env& e, uint64_t nmax) {
 
 // HEC contraction of the lists (prev, next, w) into X (pointer | HEAD_BIT,
 // offset) and cycle flags, all rounds enqueued on the stream.
+// With seg, level 0 comes from the fused path's segment records and the
+// first ranking state in X (nx cross indices) instead of (prev, next, w).
 static void hec_contract(Env& e, HecPool& h, uint32_t R, const uint32_t* prev, const uint32_t* next,
                          const uint32_t* w, uint64_t nmax, bool count_on_device, unsigned long long* X,
-                         uint8_t* oncycle) {
+                         uint8_t* oncycle, const SegRec* seg = nullptr, uint32_t nx = 0, int k = 0) {
   const int grid = grid_for(e, nmax ? nmax : 1, 256);
   cudaMemsetAsync(h.ln, 0, (R + 1) * 4, e.stream);
   ++e.launches;
-  k_hec_level0<<<grid, 256, 0, e.stream>>>(h, prev, next, w, nmax, count_on_device ? e.ctr : nullptr);
+  if (seg) k_hec_level0_seg<<<grid, 256, 0, e.stream>>>(h, seg, X, nmax, nx, k);
+  else k_hec_level0<<<grid, 256, 0, e.stream>>>(h, prev, next, w, nmax, count_on_device ? e.ctr : nullptr);
   for (uint32_t r = 0; r < R; ++r) {
     e.launches += 6;
     k_hec_prep<<<grid, 256, 0, e.stream>>>(h, int(r));
@@ -2909,6 +3341,102 @@ uint64_t output_bound(size_t text_bytes, int k) {
   return uint64_t(text_bytes) + 64;
 }
 
+// Segment arrays of the fused path's stitch (in the back arena).
+struct StitchBufs {
+  SegRec* seg;
+  unsigned long long* Xr;
+  char* segc;
+  uint32_t *act0, *act1;
+  uint8_t* oncyc;
+  uint32_t* hlen;
+  unsigned long long *loff, *lbase, *stmp;
+  uint32_t* rcnt;
+  HecPool hp;
+};
+
+// The cross-tile stitch over X cross-indexed segments and Hp head-pool ids:
+// ranking (pointer jumping, or HEC with pointer jumping when its rounds run
+// out), line lengths at the heads, line bases per job, the segment copies
+// into out, each job's byte count in jd.jout (after jd.jclosed), and the
+// rare segment cycles.
+static int run_stitch(Env& e, const StitchBufs& b, uint64_t X, uint64_t Hp, int k, int nw, bool want_hec,
+                      uint32_t RH, const JobDev& jd, uint32_t njobs, char* out, uint32_t& rounds) {
+  rounds = 0;
+  const uint32_t S = uint32_t(X + Hp), nx = uint32_t(X), H = uint32_t(Hp);
+  SegRec* seg = b.seg;
+  unsigned long long* Xr = b.Xr;
+  char* segc = b.segc;
+  uint32_t *act0 = b.act0, *act1 = b.act1, *hlen = b.hlen, *rcnt = b.rcnt;
+  uint8_t* oncyc = b.oncyc;
+  unsigned long long *loff = b.loff, *lbase = b.lbase, *stmp = b.stmp;
+  HecPool hp = b.hp;
+  int r = UC_OK;
+  const int gs = grid_for(e, S, 256);
+  uint32_t *act = nullptr, *left = nullptr;
+  bool hec = want_hec;
+  if (hec) {
+    // HEC matching rounds, captured as one graph
+    r = run_graph(e, 1, (uint64_t(RH) << 32) | uint32_t(gs), [&] {
+      cudaMemsetAsync(oncyc, 0, S, e.stream);
+      hec_contract(e, hp, RH, nullptr, nullptr, nullptr, S, false, Xr, oncyc, seg, nx, k);
+      cudaMemsetAsync(rcnt, 0, 4, e.stream);
+      ++e.launches;
+      k_cycle_list<<<gs, 256, 0, e.stream>>>(oncyc, S, nullptr, act0, rcnt);
+    });
+    if (r) return r;
+    act = act0;
+    left = rcnt;
+    rounds = RH;
+    r = e.read_ctr();
+    if (r) return r;
+    if (e.h_ctr->err) {  // did not finish in its pool/rounds: pointer jumping
+      if (e.faults.hec_strict) return e.check_err(e.h_ctr);
+      UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
+      hec = false;
+    }
+  }
+  if (!hec) {
+    // pointer-jumping rounds, captured as one graph.  Without HEC the tiles
+    // wrote the first state; after a HEC attempt it is rebuilt from the
+    // level-0 links the HEC pool kept
+    uint32_t rr = 2;
+    for (uint64_t t = 1; t < S; t <<= 1) ++rr;
+    int rl = UC_OK;
+    const bool first_from_tiles = !want_hec;
+    r = run_graph(e, 0, (uint64_t(rr) << 33) | (uint64_t(first_from_tiles) << 32) | uint32_t(gs), [&] {
+      rl = first_from_tiles ? rank_lists(e, nullptr, nullptr, S, false, Xr, act0, act1, rcnt, rounds, act, left, nx)
+                            : rank_lists(e, hp.prv, hp.wt, S, false, Xr, act0, act1, rcnt, rounds, act, left);
+      cudaMemsetAsync(oncyc, 0, S, e.stream);
+      ++e.launches;
+      k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
+    });
+    if (r) return r;
+    if (rl) return rl;
+  }
+  // line length at each head, the heads' running offsets per job, their line
+  // bases, then every segment's chars
+  UC_CK(cudaMemsetAsync(hlen, 0, size_t(H) * 4, e.stream));
+  e.launches += 4;
+  k_chain_len<<<gs, 256, 0, e.stream>>>(S, seg, Xr, oncyc, nx, k, hlen, e.ctr);
+  e.launches += scan_launches(H);
+  scan_excl<uint32_t, unsigned long long>(hlen, H, loff, stmp, e.stream);
+  k_line_base<<<grid_for(e, H, 256), 256, 0, e.stream>>>(H, seg + nx, jd.tab, jd.jclosed, loff, lbase);
+  k_seg_copy<<<grid_for(e, S, 256), 256, 0, e.stream>>>(S, seg, Xr, oncyc, nx, lbase, segc, out, k);
+  k_job_finish<<<(njobs + 255) / 256, 256, 0, e.stream>>>(jd.tab, njobs, jd.jclosed, loff, jd.jout);
+  uint32_t hleft = 0;
+  UC_CK(cudaMemcpyAsync(&hleft, left, 4, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  if (hleft) {
+    ++e.launches;
+    if (nw == 1)
+      k_seg_cycles<1><<<1, 1, 0, e.stream>>>(e.ctr, S, act, hleft, oncyc, seg, jd.tab, jd.jout, segc, out, k);
+    else
+      k_seg_cycles<2><<<1, 1, 0, e.stream>>>(e.ctr, S, act, hleft, oncyc, seg, jd.tab, jd.jout, segc, out, k);
+  }
+  UC_CK(cudaGetLastError());
+  return UC_OK;
+}
+
 // Back arena bytes of the fused path: the bucketed copies and their staging,
 // the segment pool (Sp segments for X cross k-mers) and the stitch arrays.
 static size_t back_bytes(uint64_t copies, uint64_t X, uint64_t Sp, int nw, int k, bool want_hec) {
@@ -2916,14 +3444,13 @@ static size_t back_bytes(uint64_t copies, uint64_t X, uint64_t Sp, int nw, int k
   const uint32_t R = 64;
   size_t back = 0;
   auto add = [&](size_t b) { back += (b + 255) & ~size_t(255); };
-  add(copies * 8 * nw); add(copies * 4);                                  // copies
-  add(scatter_stage_bytes(copies, nw));                                   // level-1 staging
-  add(Sp * 8); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // seg_off, len, sx, ex, job
-  add((X + 1) * 4); add((X + 1) * 4);                                     // start_seg, end_seg
+  const uint64_t Hp = Sp - X;                                             // head pools
+  add(scatter_stage_bytes(copies, nw)); add(scatter_stage_bytes(copies, nw));  // the scatter's two regions
+  add(Sp * sizeof(SegRec)); add(Sp * 8);                                  // segment records, ranking
   add(segchars);
-  add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4); add(Sp * 4);       // next, prev, w, act0, act1
-  add(Sp * 4); add(Sp * 8); add((Sp + 1) * 8); add(Sp);                  // hlen, X, loff, oncyc
-  add(scan_tmp_elems(Sp) * 8); add(R * 4);
+  add(Sp * 4); add(Sp * 4); add(Sp);                                      // act0, act1, oncyc
+  add(Hp * 4); add((Hp + 1) * 8); add(Hp * 8);                            // line lengths, offsets, bases
+  add(scan_tmp_elems(Hp) * 8); add(R * 4);
   if (want_hec) add(hec_bytes(Sp, hec_rounds(Sp)));
   return back;
 }
@@ -3042,8 +3569,11 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   UC_CK(cudaMemcpyAsync(xc.data(), jd.jcross, njobs * 4, cudaMemcpyDeviceToHost, e.stream));
   r = e.read_ctr();
   if (r) return r;
-  if (e.h_ctr->count_ovf && !e.h_ctr->err) {
-    // a bucket holds 65536 copies or more: count again at 32 bits
+  uint64_t xsum = 0;
+  for (uint32_t j = 0; j < njobs; ++j) xsum += xc[j];
+  if (copies != N + xsum && !e.h_ctr->err) {
+    // a bucket holds 65536 copies or more (its 16-bit count wrapped): count
+    // again at 32 bits
     UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
     e.launches += 1;
     k_count_buckets<<<grid_for(e, N, 256), 256, 0, e.stream>>>(f.b1, f.b2, N, f.counts);
@@ -3055,15 +3585,21 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     return e.check_err(e.h_ctr);
   }
   const uint64_t X = copies - N;
-  uint64_t Sp = 0;
+  // segment ids: [0, X) the segments that start at a cross k-mer's S-only
+  // copy; then each job's head pool (a line's first open segment ends at a
+  // P-only copy, so a job has at most one per cross k-mer)
+  uint64_t Hp = 0;
   for (uint32_t j = 0; j < njobs; ++j) {
-    J[j].seg_base = uint32_t(Sp);
-    J[j].seg_cap = 2 * xc[j] + 1;
-    Sp += J[j].seg_cap;
+    J[j].seg_base = uint32_t(Hp);
+    J[j].seg_cap = xc[j] + 1;
+    Hp += J[j].seg_cap;
   }
+  const uint64_t Sp = X + Hp;
   if (Sp >= 0x7FFFFFF0ull) return e.fail(UC_EINPUT, "too many cross-tile segments");
+  if (njobs >= (1u << (64 - SEG_OFF_BITS))) return e.fail(UC_EINPUT, "too many jobs in one batch");
   UC_CK(cudaMemcpyAsync(jd.tab, J.data(), njobs * sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
   const uint64_t segchars = Sp * uint64_t(k) + copies + 64;
+  if (segchars > SEG_OFF_MASK) return e.fail(UC_EINPUT, "segment chars beyond the 40-bit offsets");
   const uint32_t R = 64;
   const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
   const uint32_t RH = hec_rounds(e, Sp);
@@ -3072,27 +3608,18 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   if (r) return r;
   auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
   auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(1, c * 4)); };
-  uint64_t* pkeys = reinterpret_cast<uint64_t*>(T64(copies * nw));
-  uint32_t* plink = T32(copies);
-  char* stage = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
-  unsigned long long* seg_off = T64(Sp);
-  uint32_t* seg_len = T32(Sp);
-  uint32_t* seg_sx = T32(Sp);
-  uint32_t* seg_ex = T32(Sp);
-  uint32_t* seg_job = T32(Sp);
-  uint32_t* start_seg = T32(X + 1);
-  uint32_t* end_seg = T32(X + 1);
+  char* region1 = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  char* region2 = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  SegRec* seg = static_cast<SegRec*>(e.take(1, Sp * sizeof(SegRec)));
+  unsigned long long* Xr = T64(Sp);
   char* segc = static_cast<char*>(e.take(1, segchars));
-  uint32_t* next = T32(Sp);
-  uint32_t* prev = T32(Sp);
-  uint32_t* wgt = T32(Sp);
   uint32_t* act0 = T32(Sp);
   uint32_t* act1 = T32(Sp);
-  uint32_t* hlen = T32(Sp);
-  unsigned long long* Xr = T64(Sp);
-  unsigned long long* loff = T64(Sp + 1);
   uint8_t* oncyc = static_cast<uint8_t*>(e.take(1, Sp));
-  unsigned long long* stmp = T64(scan_tmp_elems(Sp));
+  uint32_t* hlen = T32(Hp);
+  unsigned long long* loff = T64(Hp + 1);
+  unsigned long long* lbase = T64(Hp);
+  unsigned long long* stmp = T64(scan_tmp_elems(Hp));
   uint32_t* rcnt = T32(R);
   if (!rcnt) return e.fail(UC_EBUDGET, "back arena overflow");
   HecPool hp{};
@@ -3100,10 +3627,13 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
     r = hec_take(e, Sp, RH, hp);
     if (r) return r;
   }
-  UC_CK(cudaMemsetAsync(seg_len, 0, Sp * 4, e.stream));
+  // unused head-pool ids keep length 0 (every id below X gets a record)
+  UC_CK(cudaMemsetAsync(seg + X, 0, Hp * sizeof(SegRec), e.stream));
   UC_CK(cudaMemsetAsync(jd.jout, 0, njobs * 8, e.stream));
   UC_CK(cudaMemsetAsync(jd.jseg, 0, njobs * 4, e.stream));
-  r = plan_and_scatter(e, f, P, N, nw, 0, pkeys, plink, stage, copies);
+  uint64_t* pkeys = nullptr;
+  uint32_t* plink = nullptr;
+  r = plan_and_scatter(e, f, P, N, nw, 0, region1, region2, copies, pkeys, plink);
   if (r) return r;
   cudaEventRecord(e.ev[2], e.stream);
 
@@ -3124,13 +3654,9 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   tp.out = out;
   tp.segchars = segc;
   tp.segchars_cap = segchars;
-  tp.seg_off = seg_off;
-  tp.seg_len = seg_len;
-  tp.seg_sx = seg_sx;
-  tp.seg_ex = seg_ex;
-  tp.seg_job = seg_job;
-  tp.start_seg = start_seg;
-  tp.end_seg = end_seg;
+  tp.seg = seg;
+  tp.Xr = Xr;
+  tp.xcount = uint32_t(X);
   tp.jobs = jd.tab;
   tp.jout = jd.jout;
   tp.jseg = jd.jseg;
@@ -3143,72 +3669,9 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   if (e.h_ctr->err) return e.check_err(e.h_ctr);
   UC_CK(cudaMemcpyAsync(jd.jclosed, jd.jout, njobs * 8, cudaMemcpyDeviceToDevice, e.stream));
   uint32_t rounds = 0;
-  const uint32_t S = uint32_t(Sp);
-  const int gs = grid_for(e, S, 256);
-  ++e.launches;
-  // pointer jumping takes its first state from the link pass
-  const bool link_ranks = !want_hec;
-  if (link_ranks) UC_CK(cudaMemsetAsync(rcnt, 0, 4, e.stream));
-  k_seg_link<<<gs, 256, 0, e.stream>>>(S, seg_sx, seg_ex, seg_len, start_seg, end_seg, next, prev, wgt, k,
-                                       link_ranks ? Xr : nullptr, act0, rcnt);
-  uint32_t *act = nullptr, *left = nullptr;
-  bool hec = want_hec;
-  if (hec) {
-    // HEC matching rounds, captured as one graph
-    r = run_graph(e, 1, (uint64_t(RH) << 32) | uint32_t(gs), [&] {
-      cudaMemsetAsync(oncyc, 0, S, e.stream);
-      hec_contract(e, hp, RH, prev, next, wgt, S, false, Xr, oncyc);
-      cudaMemsetAsync(rcnt, 0, 4, e.stream);
-      ++e.launches;
-      k_cycle_list<<<gs, 256, 0, e.stream>>>(oncyc, S, nullptr, act0, rcnt);
-    });
-    if (r) return r;
-    act = act0;
-    left = rcnt;
-    rounds = RH;
-    r = e.read_ctr();
-    if (r) return r;
-    if (e.h_ctr->err) {  // did not finish in its pool/rounds: pointer jumping
-      if (e.faults.hec_strict) return e.check_err(e.h_ctr);
-      UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
-      hec = false;
-    }
-  }
-  if (!hec) {
-    // pointer-jumping rounds, captured as one graph
-    uint32_t rr = 2;
-    for (uint64_t t = 1; t < S; t <<= 1) ++rr;
-    int rl = UC_OK;
-    r = run_graph(e, 0, (uint64_t(rr) << 33) | (uint64_t(link_ranks) << 32) | uint32_t(gs), [&] {
-      rl = rank_lists(e, prev, wgt, S, false, Xr, act0, act1, rcnt, rounds, act, left, link_ranks);
-      cudaMemsetAsync(oncyc, 0, S, e.stream);
-      ++e.launches;
-      k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
-    });
-    if (r) return r;
-    if (rl) return rl;
-  }
-  e.launches += 1 + 6 + 2;
-  // line length at each head, 0 at every other slot
-  UC_CK(cudaMemsetAsync(hlen, 0, size_t(S) * 4, e.stream));
-  k_chain_len<<<gs, 256, 0, e.stream>>>(S, seg_len, Xr, next, wgt, oncyc, hlen);
-  scan_excl<uint32_t, unsigned long long>(hlen, S, loff, stmp, e.stream);
-  k_seg_copy<<<grid_for(e, S, 256), 256, 0, e.stream>>>(S, seg_len, seg_job, jd.tab, jd.jclosed, Xr,
-                                                                        next, prev, wgt, oncyc, seg_off, loff, segc,
-                                                                        out, k);
-  k_job_finish<<<(njobs + 255) / 256, 256, 0, e.stream>>>(jd.tab, njobs, jd.jclosed, loff, jd.jout);
-  uint32_t hleft = 0;
-  UC_CK(cudaMemcpyAsync(&hleft, left, 4, cudaMemcpyDeviceToHost, e.stream));
-  UC_CK(cudaStreamSynchronize(e.stream));
-  if (hleft) {
-    ++e.launches;
-    if (nw == 1)
-      k_seg_cycles<1><<<1, 1, 0, e.stream>>>(e.ctr, S, act, hleft, oncyc, next, seg_len, seg_job, jd.tab, jd.jout,
-                                            seg_off, segc, out, k);
-    else
-      k_seg_cycles<2><<<1, 1, 0, e.stream>>>(e.ctr, S, act, hleft, oncyc, next, seg_len, seg_job, jd.tab, jd.jout,
-                                            seg_off, segc, out, k);
-  }
+  StitchBufs sbuf{seg, Xr, segc, act0, act1, oncyc, hlen, loff, lbase, stmp, rcnt, hp};
+  r = run_stitch(e, sbuf, X, Hp, k, nw, want_hec, RH, jd, njobs, out, rounds);
+  if (r) return r;
   UC_CK(cudaGetLastError());
   cudaEventRecord(e.ev[4], e.stream);
   std::vector<unsigned long long> jo(njobs), jc(st ? njobs : 0);
@@ -3256,6 +3719,309 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
       cudaEventElapsedTime(&st->ms_tile_warp, e.ev[8], e.ev[9]);
       cudaEventElapsedTime(&st->ms_tile_block, e.ev[9], e.ev[5]);
     }
+  }
+  e.reset();
+  return UC_OK;
+}
+
+// The streamed form of the fused path, for a job from host memory whose text
+// and lines do not fit in device memory beside the working arrays.  The text
+// goes to the device in chunks of whole lines, twice: the first pass counts
+// the buckets (the 16-bit counts, taken again at 32 bits in a third pass if
+// one wrapped), the second builds the bucketed copies (level 1 of the
+// scatter per chunk, its cursors carried over; levels 2 and 3 once).  The
+// tiles then run in groups of whole tiles; each group's closed lines go back
+// to host memory before the next group, while the open segments stay on the
+// device for the stitch, whose lines follow.  The device holds one chunk's
+// text, keys and buckets, the copies' two scatter regions, the segment
+// arrays and the output of one tile group; k-mer indices are 64-bit
+// throughout (the reference's LARGE/HUGE widths, defs.h:30-42), cross
+// indices and segment ids 31-bit.  Lines must be k chars + '\n' (the layout
+// the chunks are cut on).  Unsorted output only.
+int compact_streamed(Env& e, const char* h_text, size_t bytes, int k, int l, char* h_out, uint64_t cap,
+                     uint64_t& out_bytes, uc_stats* st, uint64_t chunk_lines, uint64_t group_copies) {
+  out_bytes = 0;
+  if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
+  if (l < 1 || l > 16 || l > k - 1) return e.fail(UC_EINPUT, "l must be in [1, min(16, k-1)]");
+  if (e.sorted) return e.fail(UC_EINPUT, "the streamed path writes unsorted output");
+  const int nw = (k <= 31) ? 1 : 2;
+  const uint64_t stride = uint64_t(k) + 1;
+  // count line (driver.cpp:296-304) and the fixed line layout
+  size_t p = 0;
+  while (p < bytes && (h_text[p] == ' ' || h_text[p] == '\t' || h_text[p] == '\r')) ++p;
+  if (p >= bytes || h_text[p] < '0' || h_text[p] > '9') return e.fail(UC_EINPUT, "missing k-mer count header");
+  uint64_t n = 0;
+  while (p < bytes && h_text[p] >= '0' && h_text[p] <= '9') {
+    n = n * 10 + uint64_t(h_text[p] - '0');
+    if (n > (1ull << 40)) return e.fail(UC_EINPUT, "k-mer count too large");
+    ++p;
+  }
+  while (p < bytes && h_text[p] != '\n') ++p;
+  const uint64_t body = (p < bytes) ? p + 1 : bytes;
+  uint64_t end = bytes;
+  while (end > body && (h_text[end - 1] == '\n' || h_text[end - 1] == '\r')) --end;
+  if (!((n == 0 && end == body) || (n > 0 && end - body == n * stride - 1)))
+    return e.fail(UC_EINPUT, "the streamed path needs k chars + '\\n' per line and a matching count");
+  e.reset();
+  e.launches = 0;
+  e.graph_nodes = 0;
+  if (n == 0) return UC_OK;
+  if (!chunk_lines) chunk_lines = 64ull << 20;
+  if (!group_copies) group_copies = 256ull << 20;
+  chunk_lines = std::min(chunk_lines, n);
+  const Plan P = plan_buckets(e, n, 1, k, l);
+  const size_t chunk_text = size_t(chunk_lines * stride + 64);
+  int r = e.reserve(0, front_bytes(chunk_lines, nw, P.M, true) + chunk_text + 4096);
+  if (r) return r;
+  Front f{};
+  r = take_front(e, chunk_lines, nw, P.M, true, f);
+  if (r) return r;
+  char* d_chunk = static_cast<char*>(e.take(0, chunk_text));
+  if (!d_chunk) return e.fail(UC_EBUDGET, "front arena overflow");
+  r = job_buffers(e, 1);
+  if (r) return r;
+  JobDev jd = job_dev(e, 1);
+  UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
+  UC_CK(cudaMemsetAsync(f.c16, 0, (P.M + 1) / 2 * 4, e.stream));
+  UC_CK(cudaMemsetAsync(jd.jcross, 0, 4, e.stream));
+  FuseArgs fz;
+  fz.l = P.l_used;
+  fz.seed = e.seed;
+  fz.jb = P.jb;
+  fz.b1 = f.b1;
+  fz.b2 = f.b2;
+  fz.M = P.M;
+  // one chunk of lines to the device and packed (fz.counts / fz.jcross null:
+  // buckets only)
+  auto pack_chunk = [&](uint64_t c0, uint64_t cl, uint32_t* counts, uint32_t* jcross) -> int {
+    const uint64_t src = body + c0 * stride;
+    const uint64_t len = std::min<uint64_t>(cl * stride, uint64_t(bytes) - src);
+    UC_CK(cudaMemcpyAsync(d_chunk, h_text + src, len, cudaMemcpyHostToDevice, e.stream));
+    JobTab J{};
+    J.text = reinterpret_cast<const uint8_t*>(d_chunk);
+    J.tbytes = len;
+    J.body = 0;
+    J.end = cl * stride - 1;
+    J.n = cl;
+    J.fixed = 1;
+    FuseArgs z = fz;
+    z.counts = counts;
+    z.jcross = jcross;
+    const uint64_t nblocks = (cl + PACK_LINES - 1) / PACK_LINES;
+    if (nw == 1) launch_pack<1>(e, jd.tab, &J, 1, nblocks, nullptr, k, f.keys, &z);
+    else launch_pack<2>(e, jd.tab, &J, 1, nblocks, nullptr, k, f.keys, &z);
+    UC_CK(cudaGetLastError());
+    return UC_OK;
+  };
+  cudaEventRecord(e.ev[0], e.stream);
+  for (uint64_t c0 = 0; c0 < n; c0 += chunk_lines) {
+    r = pack_chunk(c0, std::min(chunk_lines, n - c0), f.c16, jd.jcross);
+    if (r) return r;
+  }
+  r = e.read_ctr();
+  if (r) return r;
+  if (e.h_ctr->err) {
+    if (e.h_ctr->err & ERR_LAYOUT) return e.fail(UC_EINPUT, "a k-mer line is shorter than k");
+    return e.check_err(e.h_ctr);
+  }
+  cudaEventRecord(e.ev[1], e.stream);
+  ++e.launches;
+  k_widen16<<<grid_for(e, P.M, 256), 256, 0, e.stream>>>(f.c16, P.M, f.counts);
+  uint64_t copies = 0;
+  r = bucket_offsets(e, f, P.M, copies);
+  if (r) return r;
+  uint32_t xc = 0;
+  UC_CK(cudaMemcpyAsync(&xc, jd.jcross, 4, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  if (copies != n + xc) {
+    // a bucket holds 65536 copies or more: count again at 32 bits
+    UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
+    for (uint64_t c0 = 0; c0 < n; c0 += chunk_lines) {
+      const uint64_t cl = std::min(chunk_lines, n - c0);
+      r = pack_chunk(c0, cl, nullptr, nullptr);
+      if (r) return r;
+      ++e.launches;
+      k_count_buckets<<<grid_for(e, cl, 256), 256, 0, e.stream>>>(f.b1, f.b2, cl, f.counts);
+    }
+    r = bucket_offsets(e, f, P.M, copies);
+    if (r) return r;
+  }
+  const uint64_t X = copies - n;
+  const uint64_t Hp = X + 1;
+  const uint64_t Sp = X + Hp;
+  if (Sp >= 0x7FFFFFF0ull) return e.fail(UC_EINPUT, "too many cross-tile segments");
+  const uint64_t segchars = Sp * uint64_t(k) + copies + 64;
+  if (segchars > SEG_OFF_MASK) return e.fail(UC_EINPUT, "segment chars beyond the 40-bit offsets");
+  // the tiles, grouped: whole tiles up to group_copies copies (a larger tile
+  // alone); a group's closed lines fit its copies' lines
+  r = plan_tiles(e, f, P);
+  if (r) return r;
+  r = e.read_ctr();
+  if (r) return r;
+  const uint32_t ntiles = e.h_ctr->ntiles;
+  std::vector<unsigned long long> tb(size_t(ntiles) + 1);
+  UC_CK(cudaMemcpyAsync(tb.data(), f.tile_begin, (size_t(ntiles) + 1) * 8, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  std::vector<uint32_t> groups{0};
+  uint64_t gmax = 0;
+  for (uint32_t t = 0; t < ntiles;) {
+    const uint32_t g0 = t;
+    do {
+      ++t;
+    } while (t < ntiles && tb[t + 1] - tb[g0] <= group_copies);
+    groups.push_back(t);
+    gmax = std::max<uint64_t>(gmax, tb[t] - tb[g0]);
+  }
+  const uint64_t gout = gmax * stride + 64;
+  const uint64_t sout = segchars + Sp + 64;  // stitched lines: segment chars and a break each at most
+  const uint32_t R = 64;
+  const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
+  const uint32_t RH = hec_rounds(e, Sp);
+  r = e.reserve(1, back_bytes(copies, X, Sp, nw, k, want_hec) + gout + sout + 4096);
+  if (r) return r;
+  auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
+  auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(1, c * 4)); };
+  char* region1 = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  char* region2 = static_cast<char*>(e.take(1, scatter_stage_bytes(copies, nw)));
+  SegRec* seg = static_cast<SegRec*>(e.take(1, Sp * sizeof(SegRec)));
+  unsigned long long* Xr = T64(Sp);
+  char* segc = static_cast<char*>(e.take(1, segchars));
+  uint32_t* act0 = T32(Sp);
+  uint32_t* act1 = T32(Sp);
+  uint8_t* oncyc = static_cast<uint8_t*>(e.take(1, Sp));
+  uint32_t* hlen = T32(Hp);
+  unsigned long long* loff = T64(Hp + 1);
+  unsigned long long* lbase = T64(Hp);
+  unsigned long long* stmp = T64(scan_tmp_elems(Hp));
+  uint32_t* rcnt = T32(R);
+  char* d_gout = static_cast<char*>(e.take(1, gout));
+  char* d_sout = static_cast<char*>(e.take(1, sout));
+  if (!d_sout) return e.fail(UC_EBUDGET, "back arena overflow");
+  HecPool hp{};
+  if (want_hec) {
+    r = hec_take(e, Sp, RH, hp);
+    if (r) return r;
+  }
+  UC_CK(cudaMemsetAsync(seg + X, 0, Hp * sizeof(SegRec), e.stream));
+  UC_CK(cudaMemsetAsync(jd.jseg, 0, 4, e.stream));
+  // the bucketed copies: level 1 chunk by chunk, then levels 2 and 3
+  Scatter sc;
+  r = scatter_begin(e, f, P, nw, region1, region2, copies, sc);
+  if (r) return r;
+  for (uint64_t c0 = 0; c0 < n; c0 += chunk_lines) {
+    const uint64_t cl = std::min(chunk_lines, n - c0);
+    r = pack_chunk(c0, cl, nullptr, nullptr);
+    if (r) return r;
+    r = scatter_l1(e, f, sc, f.keys, f.b1, f.b2, cl, 0);
+    if (r) return r;
+  }
+  uint64_t* pkeys = nullptr;
+  uint32_t* plink = nullptr;
+  r = scatter_finish(e, f, sc, pkeys, plink);
+  if (r) return r;
+  cudaEventRecord(e.ev[2], e.stream);
+  // one job whose region is a tile group's output buffer
+  JobTab J{};
+  J.n = n;
+  J.obase = 0;
+  J.ocap = gout;
+  J.seg_base = 0;
+  J.seg_cap = uint32_t(Hp);
+  UC_CK(cudaMemcpyAsync(jd.tab, &J, sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
+  TileParams tp{};
+  tp.pkeys = pkeys;
+  tp.plink = plink;
+  tp.tile_begin = f.tile_begin;
+  tp.tile_job = f.tile_job;
+  tp.ctr = e.ctr;
+  tp.k = k;
+  tp.cap = P.cap;
+  tp.tslots = P.tslots;
+  tp.lf = P.lf;
+  tp.wcap = P.wcap;
+  tp.wts = P.wts;
+  tp.wbytes = P.wbytes;
+  tp.mode = 1;
+  tp.out = d_gout;
+  tp.segchars = segc;
+  tp.segchars_cap = segchars;
+  tp.seg = seg;
+  tp.Xr = Xr;
+  tp.xcount = uint32_t(X);
+  tp.jobs = jd.tab;
+  tp.jout = jd.jout;
+  tp.jseg = jd.jseg;
+  const uint32_t threads = e.tune.tile_threads ? e.tune.tile_threads : 512;
+  uint64_t closed = 0;
+  float ms_tiles = 0;
+  for (size_t g = 0; g + 1 < groups.size(); ++g) {
+    // per group: the tier lists and their counters, the group's line cursor
+    UC_CK(cudaMemsetAsync(&e.ctr->tile_next, 0, 4, e.stream));
+    UC_CK(cudaMemsetAsync(&e.ctr->nbig, 0, 4, e.stream));
+    UC_CK(cudaMemsetAsync(&e.ctr->nwarp, 0, 12, e.stream));  // nwarp, nblock, wtile_next
+    UC_CK(cudaMemsetAsync(jd.jout, 0, 8, e.stream));
+    r = classify_tiles(e, f, P, nw, groups[g], groups[g + 1]);
+    if (r) return r;
+    r = (nw == 1) ? run_tiles<1>(e, tp, f, threads) : run_tiles<2>(e, tp, f, threads);
+    if (r) return r;
+    float a = 0;
+    cudaEventElapsedTime(&a, e.ev[8], e.ev[5]);
+    ms_tiles += a;
+    unsigned long long gb = 0;
+    UC_CK(cudaMemcpyAsync(&gb, jd.jout, 8, cudaMemcpyDeviceToHost, e.stream));
+    r = e.read_ctr();
+    if (r) return r;
+    if (e.h_ctr->err) return e.check_err(e.h_ctr);
+    if (closed + gb > cap) return e.fail(UC_EINPUT, "output buffer smaller than uc_output_bound");
+    UC_CK(cudaMemcpyAsync(h_out + closed, d_gout, gb, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    closed += gb;
+  }
+  cudaEventRecord(e.ev[3], e.stream);
+  // the stitch into its own buffer (no closed lines before it there)
+  J.ocap = sout;
+  UC_CK(cudaMemcpyAsync(jd.tab, &J, sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
+  UC_CK(cudaMemsetAsync(jd.jclosed, 0, 8, e.stream));
+  uint32_t rounds = 0;
+  StitchBufs sbuf{seg, Xr, segc, act0, act1, oncyc, hlen, loff, lbase, stmp, rcnt, hp};
+  r = run_stitch(e, sbuf, X, Hp, k, nw, want_hec, RH, jd, 1, d_sout, rounds);
+  if (r) return r;
+  cudaEventRecord(e.ev[4], e.stream);
+  unsigned long long sb = 0;
+  UC_CK(cudaMemcpyAsync(&sb, jd.jout, 8, cudaMemcpyDeviceToHost, e.stream));
+  r = e.read_ctr();
+  if (r) return r;
+  if (e.h_ctr->err) return e.check_err(e.h_ctr);
+  if (sb > sout) return e.fail(UC_EINTERNAL, "output bound exceeded");
+  if (closed + sb > cap) return e.fail(UC_EINPUT, "output buffer smaller than uc_output_bound");
+  UC_CK(cudaMemcpyAsync(h_out + closed, d_sout, sb, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaStreamSynchronize(e.stream));
+  out_bytes = closed + sb;
+  if (st) {
+    st->n_kmers = n;
+    st->n_copies = copies;
+    st->n_cross = X;
+    st->n_tiles = ntiles;
+    st->n_segments = Sp;
+    st->n_cycles = e.h_ctr->cycles;
+    st->closed_bytes = closed;
+    st->seg_chars = e.h_ctr->seg_char_cursor;
+    st->out_bytes = out_bytes;
+    st->stitch_rounds = rounds;
+    st->l_used = uint32_t(P.l_used);
+    st->bucket_bits = P.bits;
+    st->tile_capacity = P.cap;
+    st->launches = e.launches;
+    st->graph_nodes = e.graph_nodes;
+    float a = 0, b = 0, d = 0;
+    cudaEventElapsedTime(&a, e.ev[0], e.ev[1]);
+    cudaEventElapsedTime(&b, e.ev[1], e.ev[2]);
+    cudaEventElapsedTime(&d, e.ev[3], e.ev[4]);
+    st->ms_pack = a;
+    st->ms_bucket = b;
+    st->ms_tiles = ms_tiles;
+    st->ms_stitch = d;
+    st->ms_total = a + b + ms_tiles + d;
   }
   e.reset();
   return UC_OK;

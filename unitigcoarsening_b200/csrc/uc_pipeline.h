@@ -88,6 +88,11 @@ int compact_device(Env& e, const char* d_text, size_t bytes, int k, int l, char*
 int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t* bytes, int k, int l, char* out,
                   uint64_t out_cap, uint64_t* out_off, uint64_t* out_len, uc_stats* st);
 uint64_t output_bound(size_t text_bytes, int k);
+// The fused path for one job from host memory in chunks of chunk_lines lines
+// (two passes over the text) and tile groups of about group_copies copies,
+// for jobs whose text and lines exceed the device budget (0 = defaults).
+int compact_streamed(Env& e, const char* h_text, size_t bytes, int k, int l, char* h_out, uint64_t cap,
+                     uint64_t& out_bytes, uc_stats* st, uint64_t chunk_lines, uint64_t group_copies);
 // Reorder the lines of out[0, bytes) into byte order in place (scratch from
 // the back arena).
 int sort_lines(Env& e, char* out, uint64_t bytes, int k);
