@@ -55,6 +55,9 @@ def test_failed_allocation_is_enomem_and_context_recovers(job, nth):
 def test_failed_allocation_on_host_path(job):
     text, want, _ = job
     with Compactor(0) as c:
+        # resident only: by default a host job that cannot allocate runs
+        # streamed instead (tests/test_gpu_streamed.py)
+        c.set_streaming(api.STREAM_NEVER)
         c.set_faults(fail_alloc_after=1)  # the device text buffer of the host path
         with pytest.raises(api.UCError) as ei:
             c.compact_host(text, 31, 8)

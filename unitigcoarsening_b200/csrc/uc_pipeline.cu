@@ -806,12 +806,20 @@ __global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict_
     const unsigned long long c0 = boff[uint64_t(p) << fb] + uint64_t(t - istart[p]) * MID_CHUNK;
     const uint32_t cn = uint32_t(min(pend - c0, (unsigned long long)MID_CHUNK));
     const uint32_t sub0 = p << (fb - sb);  // first sub-partition of partition p
-    // bucket ids of the chunk (in registers) and the counts per sub-partition
-    uint32_t bb[PT];
+    // the chunk's records, all loads issued at once (in registers), and the
+    // counts per sub-partition
+    uint32_t bb[PT], ll[PT];
+    Key<NW> kk[PT];
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
       const uint32_t i = uint32_t(q) * 256u + threadIdx.x;
-      bb[q] = (i < cn) ? rbkt[c0 + i] : 0u;
+      if (i < cn) {
+        bb[q] = rbkt[c0 + i];
+        kk[q] = ld_key<NW>(rkey, c0 + i);
+        ll[q] = rlink[c0 + i];
+      } else {
+        bb[q] = 0u;
+      }
     }
     for (uint32_t j = threadIdx.x; j < nb; j += blockDim.x) hist[j] = 0;
     __syncthreads();
@@ -852,8 +860,8 @@ __global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict_
       const uint32_t bin = (bb[q] >> sb) - sub0;
       if (i < cn && bin < nb) {
         const uint32_t sl = lofs[bin] + atomicAdd(hist + bin, 1u);
-        st_key<NW>(skey, sl, ld_key<NW>(rkey, c0 + i));
-        slink[sl] = rlink[c0 + i];
+        st_key<NW>(skey, sl, kk[q]);
+        slink[sl] = ll[q];
         sbkt[sl] = bb[q];
       }
     }
@@ -1188,7 +1196,6 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     const uint32_t want = (sizeof(IT) == 2) ? (c * p.lf) / 100u : uint32_t((uint64_t(c) * p.lf) / 100u);
     const uint32_t x = want > c ? want : c + 1u;
     ts = 1u << (32 - __clz(x - 1u));
-    ts = ts < 4u ? 4u : ts;  // whole slot groups (the carved table holds at least 64)
     ts = ts < m.ts ? ts : m.ts;
   }
   const uint32_t tmask = ts - 1;
@@ -1216,130 +1223,47 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   G::sync();
   // ---- prefix table of the P copies (generate_hashmap, assembler.h:120-150):
   // one slot per distinct (k-1)-prefix; a prefix held by two copies marks the
-  // slot's copy DUP ("nullified").  Then the suffix lookups of the S copies
-  // (find_vtx_from_edge, assembler.h:89-111) and the in-degree counts
-  // ("count edges", assembler.h:180-188).
-  //
-  // Warp tiles of at most 256 copies use groups of four 16-bit slots, each
-  // an 8-bit copy index under an 8-bit fingerprint of the prefix hash: one
-  // 8-byte load reads a group, a key is loaded only on a fingerprint match,
-  // and a lookup ends at the first group with a free slot (inserts fill the
-  // groups in probe order, and nothing is removed).  Most lookups end in the
-  // first group, so the lanes of a warp stay together.  Larger tiles probe
-  // single slots holding a copy index.
-  constexpr bool WARP = std::is_same<G, WarpGroup>::value;
-  if (WARP && c <= 256u) {
-    constexpr uint32_t EMPTY = 0xFFFFu;
-    const uint32_t gmask = (ts >> 2) - 1u;
-    uint64_t* grp = reinterpret_cast<uint64_t*>(m.T);
-    for (uint32_t i = G::rank(); i < c; i += G::size()) {
-      const Key<NW> x = skey(m, i);
-      if (!(roles(x) & ROLE_P)) continue;
-      const Key<NW> pf = prefix_of(x, pm);
-      const uint32_t h = key_hash(pf);
-      const uint32_t fp = min(h >> 24, 254u);
-      const uint32_t mine = (fp << 8) | i;
-      uint32_t gi = h & gmask;
-      for (uint32_t probe = 0; probe <= gmask;) {
-        const uint64_t g = grp[gi];
-        bool done = false, free_slot = false;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const uint32_t sl = uint32_t(g >> (16 * q)) & 0xFFFFu;
-          if (sl == EMPTY) {
-            free_slot = true;
-          } else if (!done && (sl >> 8) == fp && key_eq(prefix_of(skey(m, sl & 0xFFu), pm), pf)) {
-            at_or(m.A + (sl & 0xFFu), DUP_I);
-            done = true;
-          }
-        }
-        if (done) break;
-        if (!free_slot) {  // a full group: the next one
-          gi = (gi + 1) & gmask;
-          ++probe;
-          continue;
-        }
-        // claim the group's first free slot; if another lane took it first,
-        // read the group again (that lane may hold the same prefix)
-        const int q = (uint32_t(g) & 0xFFFFu) == EMPTY ? 0
-                      : (uint32_t(g >> 16) & 0xFFFFu) == EMPTY ? 1
-                      : (uint32_t(g >> 32) & 0xFFFFu) == EMPTY ? 2 : 3;
-        if (at_cas(m.T + 4u * gi + uint32_t(q), EMPTY, mine) == EMPTY) break;
+  // slot's copy DUP ("nullified")
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
+    const Key<NW> x = skey(m, i);
+    if (!(roles(x) & ROLE_P)) continue;
+    const Key<NW> pf = prefix_of(x, pm);
+    uint32_t h = key_hash(pf) & tmask;
+    for (uint32_t probe = 0; probe <= tmask; ++probe) {
+      const uint32_t cur = at_cas(m.T + h, NONE_I, i);
+      if (cur == NONE_I) break;
+      if (key_eq(prefix_of(skey(m, cur), pm), pf)) {
+        at_or(m.A + cur, DUP_I);
+        break;
       }
+      h = (h + 1) & tmask;
     }
-    G::sync();
-    for (uint32_t i = G::rank(); i < c; i += G::size()) {
-      const Key<NW> x = skey(m, i);
-      if (!(roles(x) & ROLE_S)) continue;
-      const Key<NW> sf = suffix_of(x, pm);
-      const uint32_t h = key_hash(sf);
-      const uint32_t fp = min(h >> 24, 254u);
-      uint32_t gi = h & gmask;
-      uint32_t cand = CNONE_I;
-      for (uint32_t probe = 0; probe <= gmask; ++probe) {
-        const uint64_t g = grp[gi];
-        bool done = false, free_slot = false;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const uint32_t sl = uint32_t(g >> (16 * q)) & 0xFFFFu;
-          if (sl == EMPTY) {
-            free_slot = true;
-          } else if (!done && (sl >> 8) == fp && key_eq(prefix_of(skey(m, sl & 0xFFu), pm), sf)) {
-            const uint32_t cur = sl & 0xFFu;
-            if (!(uint32_t(m.A[cur]) & DUP_I)) cand = cur;
-            done = true;
-          }
-        }
-        if (done || free_slot) break;
-        gi = (gi + 1) & gmask;
-      }
-      if (cand != CNONE_I) {
-        at_inc(m.B + cand);
-        m.P[cand] = IT(i);
-      }
-      m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
-    }
-    G::sync();
-  } else {
-    for (uint32_t i = G::rank(); i < c; i += G::size()) {
-      const Key<NW> x = skey(m, i);
-      if (!(roles(x) & ROLE_P)) continue;
-      const Key<NW> pf = prefix_of(x, pm);
-      uint32_t h = key_hash(pf) & tmask;
-      for (uint32_t probe = 0; probe <= tmask; ++probe) {
-        const uint32_t cur = at_cas(m.T + h, NONE_I, i);
-        if (cur == NONE_I) break;
-        if (key_eq(prefix_of(skey(m, cur), pm), pf)) {
-          at_or(m.A + cur, DUP_I);
-          break;
-        }
-        h = (h + 1) & tmask;
-      }
-    }
-    G::sync();
-    for (uint32_t i = G::rank(); i < c; i += G::size()) {
-      const Key<NW> x = skey(m, i);
-      if (!(roles(x) & ROLE_S)) continue;
-      const Key<NW> sf = suffix_of(x, pm);
-      uint32_t h = key_hash(sf) & tmask;
-      uint32_t cand = CNONE_I;
-      for (uint32_t probe = 0; probe <= tmask; ++probe) {
-        const uint32_t cur = m.T[h];
-        if (cur == NONE_I) break;
-        if (key_eq(prefix_of(skey(m, cur), pm), sf)) {
-          if (!(uint32_t(m.A[cur]) & DUP_I)) cand = cur;
-          break;
-        }
-        h = (h + 1) & tmask;
-      }
-      if (cand != CNONE_I) {
-        at_inc(m.B + cand);
-        m.P[cand] = IT(i);
-      }
-      m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
-    }
-    G::sync();
   }
+  G::sync();
+  // ---- suffix lookups of the S copies (find_vtx_from_edge, assembler.h:89-111)
+  // and in-degree counts ("count edges", assembler.h:180-188)
+  for (uint32_t i = G::rank(); i < c; i += G::size()) {
+    const Key<NW> x = skey(m, i);
+    if (!(roles(x) & ROLE_S)) continue;
+    const Key<NW> sf = suffix_of(x, pm);
+    uint32_t h = key_hash(sf) & tmask;
+    uint32_t cand = CNONE_I;
+    for (uint32_t probe = 0; probe <= tmask; ++probe) {
+      const uint32_t cur = m.T[h];
+      if (cur == NONE_I) break;
+      if (key_eq(prefix_of(skey(m, cur), pm), sf)) {
+        if (!(uint32_t(m.A[cur]) & DUP_I)) cand = cur;
+        break;
+      }
+      h = (h + 1) & tmask;
+    }
+    if (cand != CNONE_I) {
+      at_inc(m.B + cand);
+      m.P[cand] = IT(i);
+    }
+    m.A[i] = IT((uint32_t(m.A[i]) & DUP_I) | cand);
+  }
+  G::sync();
   // ---- kept edges: u->v iff v is u's unique successor and u is v's only
   // predecessor ("write edges", assembler.h:189-197); rank init alongside
   for (uint32_t i = G::rank(); i < c; i += G::size()) {
@@ -1431,6 +1355,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   // lane busy; a block tile walks its copies and skips the others.  Each
   // thread's lines are contiguous in the tile's output, in the order the
   // thread visits them (the order of lines is free).
+  constexpr bool WARP = std::is_same<G, WarpGroup>::value;
   uint32_t nend = c;
   if constexpr (WARP) {
     const uint32_t lane = G::rank();
@@ -1734,36 +1659,50 @@ __global__ void k_line_base(uint32_t H, const SegRec* __restrict__ heads, const 
   }
 }
 
-// Copy each segment's chars into its line.  A warp takes 32 consecutive
-// segments: each lane resolves one segment's source, destination and length
-// (its record and ranking entry, then its head's line base), then groups of
-// 8 lanes copy the segments word by word.
+// Copy each segment's chars into its line.  A warp takes 4 x 32 consecutive
+// segments: each lane resolves four segments' source, destination and
+// length (their records and ranking entries, then their heads' line bases;
+// all four gathers in flight together), then groups of 8 lanes copy the
+// segments word by word.
 __global__ void __launch_bounds__(256) k_seg_copy(
     uint32_t S, const SegRec* __restrict__ seg, const unsigned long long* __restrict__ X,
     const uint8_t* __restrict__ oncycle, uint32_t nx, const unsigned long long* __restrict__ lbase,
     const char* __restrict__ segchars, char* __restrict__ out, int k) {
+  constexpr int PER = 4;
   const int lane = threadIdx.x & 31;
   const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (uint32_t base = warp * 32u; base < S; base += nwarps * 32u) {
-    const uint32_t s = base + uint32_t(lane);
-    bool live = s < S;
-    uint64_t dst = 0, src = 0;
-    uint32_t nb = 0, last = 0;
-    if (live) {
-      // the per-slot loads are issued before the test; the line-base
-      // gather only for live segments
-      const SegRec r = seg[s];
-      const uint8_t cyc = oncycle[s];
-      const unsigned long long v = X[s];
-      live = r.len != 0 && !cyc;
-      if (live) {
-        dst = lbase[ptr_of(v) - nx] + pk_o(v);
-        src = (r.off_job & SEG_OFF_MASK) + (s < nx ? uint32_t(k) : 0u);
-        nb = seg_w(s, r.len, nx, k);
-        last = r.next == NONE;
+  for (uint64_t base = uint64_t(warp) * 32u * PER; base < S; base += uint64_t(nwarps) * 32u * PER) {
+    uint64_t dst[PER], src[PER];
+    uint32_t nb[PER], last[PER], hd[PER];
+    unsigned long long off[PER];
+    bool live[PER];
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const uint64_t s = base + uint64_t(q) * 32u + uint32_t(lane);
+      live[q] = s < S;
+      dst[q] = src[q] = 0;
+      nb[q] = last[q] = 0;
+      hd[q] = 0;
+      off[q] = 0;
+      if (live[q]) {
+        const SegRec r = seg[s];
+        const uint8_t cyc = oncycle[s];
+        const unsigned long long v = X[s];
+        // (a pointer short of a head is flagged by k_chain_len)
+        live[q] = r.len != 0 && !cyc && ptr_of(v) >= nx && ptr_of(v) < S;
+        if (live[q]) {
+          hd[q] = ptr_of(v) - nx;
+          off[q] = pk_o(v);
+          src[q] = (r.off_job & SEG_OFF_MASK) + (s < nx ? uint32_t(k) : 0u);
+          nb[q] = seg_w(uint32_t(s), r.len, nx, k);
+          last[q] = r.next == NONE;
+        }
       }
     }
+#pragma unroll
+    for (int q = 0; q < PER; ++q)
+      if (live[q]) dst[q] = lbase[hd[q]] + off[q];
     // groups of 8 lanes: group g copies, one after another, the segments
     // resolved by its own 8 lanes.  Each lane of the group stores aligned
     // 4-byte words of the destination, funnel-shifted from the two aligned
@@ -1772,29 +1711,32 @@ __global__ void __launch_bounds__(256) k_seg_copy(
     // are read only where they hold a byte of the segment, so they stay in
     // the segment chars' allocation.
     const uint32_t gl = uint32_t(lane) & 7u;
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
 #pragma unroll 1
-    for (int i = 0; i < 8; ++i) {
-      const uint64_t d = __shfl_sync(0xFFFFFFFFu, dst, i, 8);
-      const uint64_t c = __shfl_sync(0xFFFFFFFFu, src, i, 8);
-      const uint32_t m = __shfl_sync(0xFFFFFFFFu, nb, i, 8);
-      const uint32_t e = __shfl_sync(0xFFFFFFFFu, last, i, 8);
-      // bytes before the first aligned word of the destination (the output
-      // buffer itself may start at any byte)
-      const uint32_t hb = min((4u - uint32_t(reinterpret_cast<uintptr_t>(out + d) & 3u)) & 3u, m);
-      const uint32_t nbody = (m - hb) >> 2;
-      const uint32_t tb = (m - hb) & 3u;
-      const char* sp = segchars + c + hb;
-      char* dp = out + d + hb;
-      const uint32_t sh = 8u * uint32_t(reinterpret_cast<uintptr_t>(sp) & 3u);
-      const uint32_t* sw = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(sp) & ~uintptr_t(3));
-      for (uint32_t wi = gl; wi < nbody; wi += 8) {
-        const uint32_t w0 = sw[wi];
-        const uint32_t v = sh ? __funnelshift_r(w0, sw[wi + 1], sh) : w0;
-        reinterpret_cast<uint32_t*>(dp)[wi] = v;
+      for (int i = 0; i < 8; ++i) {
+        const uint64_t d = __shfl_sync(0xFFFFFFFFu, dst[q], i, 8);
+        const uint64_t c = __shfl_sync(0xFFFFFFFFu, src[q], i, 8);
+        const uint32_t m = __shfl_sync(0xFFFFFFFFu, nb[q], i, 8);
+        const uint32_t e = __shfl_sync(0xFFFFFFFFu, last[q], i, 8);
+        // bytes before the first aligned word of the destination (the output
+        // buffer itself may start at any byte)
+        const uint32_t hb = min((4u - uint32_t(reinterpret_cast<uintptr_t>(out + d) & 3u)) & 3u, m);
+        const uint32_t nbody = (m - hb) >> 2;
+        const uint32_t tb = (m - hb) & 3u;
+        const char* sp = segchars + c + hb;
+        char* dp = out + d + hb;
+        const uint32_t sh = 8u * uint32_t(reinterpret_cast<uintptr_t>(sp) & 3u);
+        const uint32_t* sw = reinterpret_cast<const uint32_t*>(reinterpret_cast<uintptr_t>(sp) & ~uintptr_t(3));
+        for (uint32_t wi = gl; wi < nbody; wi += 8) {
+          const uint32_t w0 = sw[wi];
+          const uint32_t v = sh ? __funnelshift_r(w0, sw[wi + 1], sh) : w0;
+          reinterpret_cast<uint32_t*>(dp)[wi] = v;
+        }
+        if (gl < hb) out[d + gl] = segchars[c + gl];
+        if (gl >= 4 && gl - 4 < tb) dp[4 * nbody + (gl - 4)] = sp[4 * nbody + (gl - 4)];
+        if (gl == 7 && e) out[d + m] = '\n';
       }
-      if (gl < hb) out[d + gl] = segchars[c + gl];
-      if (gl >= 4 && gl - 4 < tb) dp[4 * nbody + (gl - 4)] = sp[4 * nbody + (gl - 4)];
-      if (gl == 7 && e) out[d + m] = '\n';
     }
   }
 }
