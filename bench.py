@@ -531,6 +531,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--genome", type=float, default=1e9, help="genome length (bp)")
+    ap.add_argument("--model", default="scale_plain", choices=["scale_plain", "wide_k", "small_plain"],
+                    help="genome model of the timed job (the headline is scale_plain)")
     ap.add_argument("--k", type=int, default=31)
     ap.add_argument("--l", type=int, default=8)
     ap.add_argument("--e2e-steps", type=int, default=4)
@@ -582,7 +584,8 @@ def main():
         torch.cuda.empty_cache()
 
     t0 = time.time()
-    spec = synth.scale_plain(length=int(args.genome), seed=2 + rank)
+    seed = {"scale_plain": 2, "wide_k": 3, "small_plain": 1}[args.model] + rank
+    spec = getattr(synth, args.model)(length=int(args.genome), seed=seed)
     with torch.no_grad():
         text = synth.make_text(spec, args.k, device="cuda")
     torch.cuda.synchronize()
@@ -698,11 +701,13 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u8/u64 (2-bit packed keys, 32-bit ids)", "data": "synthetic",
-            "config": {"workload": f"plain single job: {args.genome / 1e9:g} Gbp genome, 41% GC, 5% repeat "
-                                   f"families, 0.1% SNPs, k={args.k}", "k": args.k, "l": args.l,
+            "config": {"workload": (f"plain single job: {args.genome / 1e9:g} Gbp genome, 41% GC, 5% repeat "
+                                    f"families, 0.1% SNPs, k={args.k}") if args.model == "scale_plain" else
+                                   f"{args.model} job: {args.genome / 1e9:g} Gbp genome, k={args.k}",
+                       "model": args.model, "k": args.k, "l": args.l,
                        "l_used": int(st["l_used"]),
                        "n_kmers": n, "text_bytes": text_bytes, "l2_flush": "inputs larger than L2",
-                       "parallelism": f"replicas x{world}", "genome_seed": 2},
+                       "parallelism": f"replicas x{world}", "genome_seed": seed},
             "roofline": {"bound": "hbm", "kernel": "k_tile_warp + k_tile", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (tpc * st["n_copies"]) if tpc else None,

@@ -242,6 +242,7 @@ __device__ __forceinline__ void lmins(const Key<NW>& key, int k, int l, uint64_t
       // l-mer p sits in bits [64 - 2p - 2l, 64 - 2p) of hi
       int s = 64 - 2 * l;
       first = static_cast<uint32_t>(hi >> s) * m + a;
+#pragma unroll
       for (int p = 1; p < w - 1; ++p) {
         s -= 2;
         mid = min(mid, static_cast<uint32_t>(hi >> s) * m + a);
@@ -250,6 +251,7 @@ __device__ __forceinline__ void lmins(const Key<NW>& key, int k, int l, uint64_t
     } else {
       const int s = 64 - 2 * l;
       first = static_cast<uint32_t>(hi >> s) * m + a;
+#pragma unroll
       for (int p = 1; p < w - 1; ++p) {
         hi = (hi << 2) | (lo >> 62);
         lo <<= 2;

@@ -187,19 +187,25 @@ __global__ void k_count_buckets(const uint32_t* __restrict__ b1, const uint32_t*
 
 // MULTI: the block's job comes from the job table (batches); otherwise the
 // one job is a kernel parameter, read from the constant bank.
-template <int NW, bool FUSE, bool MULTI>
+// KC, LC: k and l fixed at compile time (0: taken from the arguments), so
+// that the per-word and per-l-mer loops of the common shapes unroll with
+// constant shifts.
+template <int NW, bool FUSE, bool MULTI, int KC = 0, int LC = 0>
 __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, const JobTab one, uint32_t njobs,
                                               uint64_t nblocks,
-                                              const unsigned long long* __restrict__ starts, int k,
-                                              uint64_t* __restrict__ keys, uint32_t* err, int l, uint64_t seed,
+                                              const unsigned long long* __restrict__ starts, int k_arg,
+                                              uint64_t* __restrict__ keys, uint32_t* err, int l_arg, uint64_t seed,
                                               uint32_t jb, uint32_t* __restrict__ b1, uint32_t* __restrict__ b2,
                                               uint32_t* __restrict__ counts, uint32_t* __restrict__ jcross) {
   __shared__ uint32_t buf[PACK_WORDS];
   __shared__ uint32_t s_cross;
+  const int k = KC ? KC : k_arg;
+  const int l = LC ? LC : l_arg;
   uint32_t bad = 0;
   const uint32_t stride = uint32_t(k) + 1;
-  const uint64_t kmask_hi = (NW == 1) ? ((k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull))
-                                      : ((2 * k - 64 >= 64) ? ~0ull : ((1ull << (2 * k - 64)) - 1ull));
+  uint64_t kmask_hi;
+  if constexpr (NW == 1) kmask_hi = (k >= 32) ? ~0ull : ((1ull << (2 * k)) - 1ull);
+  else kmask_hi = (2 * k - 64 >= 64) ? ~0ull : ((1ull << ((2 * k - 64) & 63)) - 1ull);
   for (uint64_t g = blockIdx.x; g < nblocks; g += gridDim.x) {
     const uint32_t j = MULTI ? job_of_block(jobs, njobs, g) : 0u;
     const uint8_t* text = MULTI ? jobs[j].text : one.text;
@@ -2299,14 +2305,46 @@ struct FuseArgs {
   uint64_t M = 0;
 };
 
-template <int NW, bool FUSE, bool MULTI>
+template <int NW, bool FUSE, bool MULTI, int KC = 0, int LC = 0>
 static int pack_occupancy() {
   static int o = 0;  // resident CTAs per SM (per template instance)
   if (!o) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_pack<NW, FUSE, MULTI>, 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k_pack<NW, FUSE, MULTI, KC, LC>, 256, 0);
     if (o < 1) o = 1;
   }
   return o;
+}
+
+// The single-job fused pack with k and l fixed at compile time: k = 31 or
+// 63 with l in [8, 16] (the bucket count raises l to at least 13 for large
+// jobs).  Returns false for other shapes.
+template <int NW, int KC, int LC>
+static bool launch_pack_fixed_l(Env& e, const JobTab* jobs, const JobTab& J, uint64_t nblocks, uint64_t* keys,
+                                const FuseArgs* fz) {
+  const int o = pack_occupancy<NW, true, false, KC, LC>();
+  const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(nblocks, uint64_t(e.sm_count) * o)));
+  ++e.launches;
+  k_pack<NW, true, false, KC, LC><<<grid, 256, 0, e.stream>>>(jobs, J, 1, nblocks, nullptr, KC, keys, &e.ctr->err,
+                                                               LC, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
+                                                               fz->jcross);
+  return true;
+}
+
+template <int NW, int KC>
+static bool launch_pack_fixed(Env& e, const JobTab* jobs, const JobTab& J, uint64_t nblocks, uint64_t* keys,
+                              const FuseArgs* fz) {
+  switch (fz->l) {
+    case 8: return launch_pack_fixed_l<NW, KC, 8>(e, jobs, J, nblocks, keys, fz);
+    case 9: return launch_pack_fixed_l<NW, KC, 9>(e, jobs, J, nblocks, keys, fz);
+    case 10: return launch_pack_fixed_l<NW, KC, 10>(e, jobs, J, nblocks, keys, fz);
+    case 11: return launch_pack_fixed_l<NW, KC, 11>(e, jobs, J, nblocks, keys, fz);
+    case 12: return launch_pack_fixed_l<NW, KC, 12>(e, jobs, J, nblocks, keys, fz);
+    case 13: return launch_pack_fixed_l<NW, KC, 13>(e, jobs, J, nblocks, keys, fz);
+    case 14: return launch_pack_fixed_l<NW, KC, 14>(e, jobs, J, nblocks, keys, fz);
+    case 15: return launch_pack_fixed_l<NW, KC, 15>(e, jobs, J, nblocks, keys, fz);
+    case 16: return launch_pack_fixed_l<NW, KC, 16>(e, jobs, J, nblocks, keys, fz);
+    default: return false;
+  }
 }
 
 // one: the job of a single-job launch (host copy), or NULL for a batch
@@ -2320,6 +2358,10 @@ static void launch_pack(Env& e, const JobTab* jobs, const JobTab* one, uint32_t 
                    : (one ? pack_occupancy<NW, false, false>() : pack_occupancy<NW, false, true>());
   const int grid = int(std::max<uint64_t>(1, std::min<uint64_t>(nblocks, uint64_t(e.sm_count) * o)));
   const JobTab J = one ? *one : JobTab{};
+  if (fz && one && !starts) {
+    if (NW == 1 && k == 31 && launch_pack_fixed<NW, 31>(e, jobs, J, nblocks, keys, fz)) return;
+    if (NW == 2 && k == 63 && launch_pack_fixed<NW, 63>(e, jobs, J, nblocks, keys, fz)) return;
+  }
   ++e.launches;
   if (fz && one)
     k_pack<NW, true, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
