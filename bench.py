@@ -428,7 +428,7 @@ def measure_serving(args, device: int):
     import torch
     from unitigcoarsening_b200 import Compactor, Server, UCError, synth
     pool, pool_bytes = [], 0
-    host_cap = psutil.virtual_memory().available // 3  # the pool, its outputs, and headroom
+    host_cap = psutil.virtual_memory().available // 2  # the pool (results are dropped), and headroom
     t0 = time.perf_counter()
     with torch.no_grad():
         for j in range(args.serve_pool):

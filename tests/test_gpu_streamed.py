@@ -88,26 +88,35 @@ def test_streamed_beyond_31_bit_kmer_counts():
 
     from tests.test_gpu_fullsize import C0, _output_hash
     k = 31
-    spec = synth.scale_plain(length=int(float(HUGE) * 1e9), seed=31)
-    with torch.no_grad():
-        km = synth.kmer_set(spec, k, device="cuda")
-    n = km.shape[0]
+    # two genomes of half the length each (one k-mer set of more than 2^31
+    # elements is beyond the GPU sort that deduplicates it); a k-mer in both
+    # is a repeated input line, which the properties below still hold for
+    half = int(float(HUGE) * 1e9) // 2
+    parts = []
+    for seed in (31, 32):
+        with torch.no_grad():
+            parts.append(synth.kmer_set(synth.scale_plain(length=half, seed=seed), k, device="cuda").cpu())
+        torch.cuda.empty_cache()
+    n = sum(p.shape[0] for p in parts)
     # the input's hash in the library's key layout (char x at bits 2x)
     want = 0
-    for c0 in range(0, n, 1 << 26):
-        v = km[c0:c0 + (1 << 26)]
-        lib = torch.zeros_like(v)
-        for x in range(k):
-            lib |= ((v >> (2 * (k - 1 - x))) & 3) << (2 * x)
-        want += int((lib * C0).sum().item())
-    want &= (1 << 64) - 1
     header = f"{n}\n".encode()
     text = torch.empty(len(header) + n * (k + 1), dtype=torch.uint8)
     text[: len(header)] = torch.tensor(list(header), dtype=torch.uint8)
-    for c0 in range(0, n, 1 << 26):
-        lines = synth.kmers_to_lines(km[c0:c0 + (1 << 26)], k).flatten().cpu()
-        text[len(header) + c0 * (k + 1): len(header) + c0 * (k + 1) + lines.numel()] = lines
-    del km, lines
+    pos = len(header)
+    for km in parts:
+        for c0 in range(0, km.shape[0], 1 << 26):
+            v = km[c0:c0 + (1 << 26)].cuda()
+            lib = torch.zeros_like(v)
+            for x in range(k):
+                lib |= ((v >> (2 * (k - 1 - x))) & 3) << (2 * x)
+            want += int((lib * C0).sum().item())
+            lines = synth.kmers_to_lines(v, k).flatten().cpu()
+            text[pos: pos + lines.numel()] = lines
+            pos += lines.numel()
+            del v, lib, lines
+    want &= (1 << 64) - 1
+    del parts
     torch.cuda.empty_cache()
     with Compactor(0) as c:
         c.set_streaming(api.STREAM_ALWAYS)
