@@ -111,12 +111,15 @@ uc_status uc_ctx_set_streaming(uc_ctx *ctx, int mode, uint64_t chunk_lines,
  *    any list).  The device reports rounds that ran out with lists still
  *    open (the bounded wait of the contraction).
  *  - hec_strict: when the HEC rounds run out, fail with UC_ETIMEOUT instead
- *    of finishing the lists by pointer jumping. */
+ *    of finishing the lists by pointer jumping.
+ *  - walk_cap: the line walk of the stitch follows at most this many
+ *    segments after a line's head (0 = 1024); longer lines go through list
+ *    ranking, so a small cap sends small jobs down that path. */
 typedef struct uc_faults {
     uint32_t fail_alloc_after;
     uint32_t hec_round_cap;
     uint32_t hec_strict;
-    uint32_t reserved;
+    uint32_t walk_cap;
 } uc_faults;
 uc_status uc_ctx_set_faults(uc_ctx *ctx, const uc_faults *f);
 const char *uc_last_error(const uc_ctx *ctx);

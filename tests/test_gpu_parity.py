@@ -393,3 +393,42 @@ def test_batch_with_tiers_and_hec(comp, oracle):
         for t, o in zip(jobs, outs):
             want, _, _ = oracle.compact(t, 31)
             assert sorted_lines(o.cpu().numpy().tobytes()) == sorted_lines(want)
+
+
+@pytest.mark.parametrize("cap", [1, 3])
+@pytest.mark.parametrize("cfg", ["small_plain", "wide_k63", "scale_sample"])
+def test_walk_cap_sends_long_lines_to_ranking(comp, oracle, texts, cfg, cap):
+    """Lines longer than the stitch's line walk take the ranking path
+    (pointer jumping from the segment records, one reservation per line, a
+    copy per segment) while the walk writes the others: a cap of 1 or 3
+    segments splits a small job's lines between the two, and the lines
+    equal the oracle's."""
+    text, k = texts[cfg]
+    want, _, _ = oracle.compact(text, k)
+    comp.set_faults(walk_cap=cap)
+    try:
+        assert fused_lines(comp, text, k, 8) == sorted_lines(want)
+    finally:
+        comp.set_faults()
+
+
+def test_walk_cap_with_cycles_and_batches(comp, oracle, texts):
+    """The ranking path after a capped walk with cycles in the job, and in a
+    batch, where the lines it reserves come in any job order."""
+    from unitigcoarsening_b200 import synth
+    km = cyclic_kmers(500, 31, seed=2) + walk_kmers(distinct_path(3000, 31, seed=7), 31)
+    cyc = text_of(shuffled(km, 5))
+    jobs = [synth.make_text(synth.batched_job(j, scale=0.02), 31).numpy().tobytes() for j in range(8)]
+    jobs += [cyc, texts["small_plain"][0]]
+    comp.set_faults(walk_cap=2)
+    try:
+        want, _, ocyc = oracle.compact(cyc, 31)
+        assert ocyc == 1
+        assert fused_lines(comp, cyc, 31, 6) == sorted_lines(want)
+        outs = comp.compact_batch([dev(t) for t in jobs], 31, 8)
+        torch.cuda.synchronize()
+    finally:
+        comp.set_faults()
+    for t, o in zip(jobs, outs):
+        want, _, _ = oracle.compact(t, 31)
+        assert sorted_lines(o.cpu().numpy().tobytes()) == sorted_lines(want)

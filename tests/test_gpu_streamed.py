@@ -121,6 +121,8 @@ def test_streamed_beyond_31_bit_kmer_counts():
     with Compactor(0) as c:
         c.set_streaming(api.STREAM_ALWAYS)
         out, st = c.compact_host(text, k, 8, stats=True)
+    print(f"streamed job: {n} k-mers, {out.numel()} output bytes, {st['n_cross']} cross k-mers, "
+          f"{st['n_tiles']} tiles, device ms {st['ms_total']:.1f}")
     assert st["n_kmers"] == n > (1 << 31)
     del text
     got, windows, lines = 0, 0, 0

@@ -70,7 +70,7 @@ class Tuning(ctypes.Structure):
 
 class Faults(ctypes.Structure):
     _fields_ = [("fail_alloc_after", ctypes.c_uint32), ("hec_round_cap", ctypes.c_uint32),
-                ("hec_strict", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("hec_strict", ctypes.c_uint32), ("walk_cap", ctypes.c_uint32)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -217,10 +217,12 @@ class Compactor:
         output; uc_ctx_set_sorted_output)."""
         self._check(self._L.uc_ctx_set_sorted_output(self._h, 1 if on else 0))
 
-    def set_faults(self, fail_alloc_after: int = 0, hec_round_cap: int = 0, hec_strict: bool = False):
+    def set_faults(self, fail_alloc_after: int = 0, hec_round_cap: int = 0, hec_strict: bool = False,
+                   walk_cap: int = 0):
         """Failure injection for error-path tests (uc_ctx_set_faults); the
-        defaults switch it off."""
-        f = Faults(int(fail_alloc_after), int(hec_round_cap), 1 if hec_strict else 0, 0)
+        defaults switch it off.  walk_cap > 0 caps the stitch's line walk, so
+        that longer lines take the list-ranking path."""
+        f = Faults(int(fail_alloc_after), int(hec_round_cap), 1 if hec_strict else 0, int(walk_cap))
         self._check(self._L.uc_ctx_set_faults(self._h, ctypes.byref(f)))
 
     def set_streaming(self, mode: int = STREAM_AUTO, chunk_lines: int = 0, group_copies: int = 0):

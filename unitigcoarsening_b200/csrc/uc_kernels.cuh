@@ -30,7 +30,9 @@ struct Counters {
 // One open segment of the fused path (written by the tile that finds it): the
 // offset of its chars in the segment-char area (low 40 bits) and its job
 // (high 24 bits), its copy count, and the cross index through which its line
-// continues (NONE where the line ends).  Segment ids: a segment that starts
+// continues (NONE where the line ends).  A segment that starts a line keeps
+// k - 1 + len chars there; the others keep the len - 1 chars they add (their
+// first k-mer ends the segment before).  Segment ids: a segment that starts
 // at the S-only copy of cross k-mer x has id x; a segment that starts a line
 // (at a P-role copy) takes an id from its job's head pool, after all cross
 // indices.
@@ -84,7 +86,6 @@ struct TileParams {
   unsigned long long segchars_cap;
   uint32_t seg_cap;
   SegRec* seg;                  // open segments by id
-  unsigned long long* Xr;       // list-ranking state by segment id
   uint32_t xcount;              // cross k-mers (the head pool starts there)
 };
 

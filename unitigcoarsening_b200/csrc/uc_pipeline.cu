@@ -7,8 +7,9 @@
 //   --scan/plan--> tiles of whole buckets --k_scatter_coarse/fine--> copies
 //   in bucket order --k_tile_warp / k_tile / k_tile_big (persistent; a warp,
 //   a CTA, or global scratch per tile)--> finished lines + open segments
-//   (records, links and the first ranking state by segment id)
-//   --stitch (list ranking, k_chain_len, k_seg_copy)--> cross-tile lines.
+//   (one record per segment id: its chars, length and continuation)
+//   --stitch (k_walk_emit: each line from its head; list ranking,
+//   k_chain_len, k_seg_copy for what the walk leaves)--> cross-tile lines.
 // The phase-by-phase entry points (pack, minimizers, find_edges, contract,
 // emit) run the same kernels separately.
 #include <algorithm>
@@ -86,17 +87,6 @@ static void scan_excl(const Tin* in, uint64_t n, Tout* out, Tout* tmp, cudaStrea
   k_scan_down<Tin, Tout><<<unsigned(nb), 1024, 0, s>>>(in, n, out, boff, per_block, total_out);
 }
 
-// Kernels scan_excl launches for n elements.
-static uint32_t scan_launches(uint64_t n) {
-  uint32_t c = 0;
-  const uint64_t per_block = 1024 * 8;
-  for (;;) {
-    const uint64_t nb = std::max<uint64_t>(1, (n + per_block - 1) / per_block);
-    c += 2;
-    if (nb == 1) return c;
-    n = nb;
-  }
-}
 
 static uint64_t scan_tmp_elems(uint64_t n) {
   uint64_t t = 0;
@@ -746,10 +736,15 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
 // instead of one per record) and writes its records out as contiguous runs.
 // Chunks never span partitions (their list comes from k_mid_items), so the
 // counts index one partition's sub-partitions.  All blocks take chunks in
-// partition order, which keeps the write frontier inside L2.
+// partition order and reserve at the same cursors, so the runs of the
+// chunks in flight stay next to each other: the write frontier is one
+// partition's cursors and stays inside L2.  (Reserving for ranges of
+// several chunks per block instead gives every block its own frontier:
+// 1024 partly written runs per block, more than L2 holds at 1 Gbp.)
 constexpr int MID_CHUNK = 4096;    // staged records per level-2 chunk
 constexpr int MID_MAX_BINS = 1024; // sub-partitions per coarse partition
 constexpr int SUB_MAX_BITS = 8;    // buckets per sub-partition: at most 2^8
+constexpr int MID_THREADS = 512;
 
 // Chunk list of level 2: item_start[p] = first chunk of coarse partition p
 // (partition p holds the staged records [boff[p << fb], boff[(p+1) << fb])).
@@ -769,14 +764,11 @@ __global__ void k_mid_items(const unsigned long long* __restrict__ boff, uint32_
 }
 
 template <int NW>
-__global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict__ rkey,
-                                                     const uint32_t* __restrict__ rlink,
-                                                     const uint32_t* __restrict__ rbkt,
-                                                     const unsigned long long* __restrict__ boff,
-                                                     const uint32_t* __restrict__ item_start, uint32_t fb,
-                                                     uint32_t sb, uint32_t mc, unsigned long long* __restrict__ scur,
-                                                     uint64_t* __restrict__ okey, uint32_t* __restrict__ olink,
-                                                     uint32_t* __restrict__ obkt, Counters* ctr) {
+__global__ void __launch_bounds__(MID_THREADS, NW == 1 ? 2 : 1) k_scatter_mid(
+    const uint64_t* __restrict__ rkey, const uint32_t* __restrict__ rlink, const uint32_t* __restrict__ rbkt,
+    const unsigned long long* __restrict__ boff, const uint32_t* __restrict__ item_start, uint32_t fb, uint32_t sb,
+    uint32_t mc, unsigned long long* __restrict__ scur, uint64_t* __restrict__ okey, uint32_t* __restrict__ olink,
+    uint32_t* __restrict__ obkt, Counters* ctr) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);                              // [MID_CHUNK*NW]
   uint32_t* slink = reinterpret_cast<uint32_t*>(skey + MID_CHUNK * NW);              // [MID_CHUNK]
@@ -791,7 +783,10 @@ __global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict_
   for (uint32_t j = threadIdx.x; j <= mc; j += blockDim.x) istart[j] = item_start[j];
   __syncthreads();
   const uint32_t nitems = istart[mc];
-  constexpr int PT = MID_CHUNK / 256;
+  constexpr int PT = MID_CHUNK / MID_THREADS;
+  // the bins this thread scans and reserves
+  const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
+  const uint32_t j0 = min(nb, threadIdx.x * per), j1 = min(nb, j0 + per);
   for (;;) {
     if (threadIdx.x == 0) {
       const uint32_t t = atomicAdd(&ctr->work_next, 1u);
@@ -818,7 +813,7 @@ __global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict_
     Key<NW> kk[PT];
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
-      const uint32_t i = uint32_t(q) * 256u + threadIdx.x;
+      const uint32_t i = uint32_t(q) * MID_THREADS + threadIdx.x;
       if (i < cn) {
         bb[q] = rbkt[c0 + i];
         kk[q] = ld_key<NW>(rkey, c0 + i);
@@ -833,7 +828,7 @@ __global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict_
     // and leave it out rather than index past the counts
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
-      const uint32_t i = uint32_t(q) * 256u + threadIdx.x;
+      const uint32_t i = uint32_t(q) * MID_THREADS + threadIdx.x;
       if (i < cn) {
         const uint32_t bin = (bb[q] >> sb) - sub0;
         if (bin < nb) atomicAdd(hist + bin, 1u);
@@ -843,8 +838,6 @@ __global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict_
     __syncthreads();
     // local offsets and one reservation per non-empty sub-partition
     {
-      const uint32_t per = (nb + blockDim.x - 1) / blockDim.x;
-      const uint32_t j0 = min(nb, threadIdx.x * per), j1 = min(nb, j0 + per);
       uint32_t acc = 0;
       for (uint32_t j = j0; j < j1; ++j) acc += hist[j];
       uint32_t tot;
@@ -862,7 +855,7 @@ __global__ void __launch_bounds__(256) k_scatter_mid(const uint64_t* __restrict_
     // place every record in its sub-partition's run of the staging area
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
-      const uint32_t i = uint32_t(q) * 256u + threadIdx.x;
+      const uint32_t i = uint32_t(q) * MID_THREADS + threadIdx.x;
       const uint32_t bin = (bb[q] >> sb) - sub0;
       if (i < cn && bin < nb) {
         const uint32_t sl = lofs[bin] + atomicAdd(hist + bin, 1u);
@@ -1390,7 +1383,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     const bool starts_p = (roles(skey(m, s)) & ROLE_P) != 0;
     const bool closed = starts_p && (roles(skey(m, i)) & ROLE_S);
     if (closed) mine.a += uint64_t(k) + len;
-    else { mine.b += uint64_t(k) - 1 + len; mine.c += starts_p ? 1 : 0; }
+    else { mine.b += starts_p ? uint64_t(k) - 1 + len : uint64_t(len) - 1; mine.c += starts_p ? 1 : 0; }
   }
   U3 tot;
   U3 pre = G::scan3(mine, &tot);
@@ -1412,7 +1405,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     } else {
       loc = pre.b;
       m.P[s] = IT(starts_p ? uint32_t(pre.c) : OPEN_S);
-      pre.b += uint64_t(k) - 1 + len;
+      pre.b += starts_p ? uint64_t(k) - 1 + len : uint64_t(len) - 1;
       if (starts_p) pre.c += 1;
     }
     if constexpr (sizeof(IT) == 2) {
@@ -1423,8 +1416,10 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     }
   }
   G::sync();
-  // per segment: its first k-mer in full, then its line break or, for an
-  // open segment, its record and links
+  // per segment: its first k-mer in full (a segment that starts at an
+  // S-only copy keeps only the chars it adds to its line: that k-mer ends
+  // the segment before), then its line break or, for an open segment, its
+  // record
   for (uint32_t j = G::rank(); j < nend; j += G::size()) {
     const uint32_t i = end_at(j);
     if (i == NONE_I) continue;
@@ -1434,26 +1429,20 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     if constexpr (sizeof(IT) == 2) loc |= uint64_t(hi_a[s]) << 16;
     const uint32_t sid = m.P[s];
     char* dst = (sid == NONE_I) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
-    spell_key<NW>(dst, skey(m, s), k);
+    if (sid != OPEN_S) spell_key<NW>(dst, skey(m, s), k);
     if (sid == NONE_I) {
       dst[k + r] = '\n';
     } else {
       // the segment's record under its id; a segment that ends at the P-only
-      // copy of cross k-mer ex is the predecessor of segment ex, so it
-      // writes ex's first ranking entry (itself, and the chars it adds to the
-      // line: all k - 1 + len of a line's first segment, len - 1 of the
-      // others, whose first k-mer ends the segment before)
+      // copy of cross k-mer ex continues in segment ex
       const bool head = sid != OPEN_S;
       const bool p_only = (roles(skey(m, i)) & ROLE_S) == 0;
       const uint32_t g = head ? p.xcount + uint32_t(sbase) + sid : p.plink[beg + s];
-      const uint32_t ex = p_only ? p.plink[beg + i] : NONE;
       SegRec rec;
       rec.off_job = (obase + loc) | (static_cast<unsigned long long>(job) << SEG_OFF_BITS);
       rec.len = r + 1;
-      rec.next = ex;
+      rec.next = p_only ? p.plink[beg + i] : NONE;
       p.seg[g] = rec;
-      if (head) p.Xr[g] = pk(g | HEAD_BIT, 0);
-      if (p_only) p.Xr[ex] = pk(g, head ? uint32_t(k) + r : r);
     }
   }
   // every later copy of a segment adds its last char
@@ -1465,7 +1454,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     if constexpr (sizeof(IT) == 2) loc |= uint64_t(hi_a[s]) << 16;
     const uint32_t sid = m.P[s];
     char* dst = (sid == NONE_I) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
-    dst[k - 1 + r] = acgt(key_char(skey(m, i), k - 1));
+    dst[(sid == OPEN_S ? 0u : uint32_t(k)) + r - 1] = acgt(key_char(skey(m, i), k - 1));
   }
 }
 
@@ -1531,12 +1520,16 @@ __global__ void __launch_bounds__(1024) k_tile_big(TileParams p) {
 // Open segments continue through cross k-mers: the segment that ends at the
 // P-only copy of cross k-mer x is followed by segment x (the one that starts
 // at x's S-only copy); both hold x, so every later segment of a line drops
-// its first k chars (write_unitigs4, compact.h:59-112).  The tiles write each
-// segment's record and the ranking's first state (every segment x has a
-// predecessor, written by the segment before it; a line's first segment is
-// a head), so ranking starts at once over the ids [0, X).  Line lengths are
-// written at the heads, scanned over the head pools (per job, in job order)
-// and each segment copies its chars to its line's base plus its offset.
+// its first k chars (write_unitigs4, compact.h:59-112), and the tiles keep
+// only the chars it adds.  The tiles write each segment's record under its
+// id.  The common case is one kernel (k_walk_emit): a thread per line head
+// walks its line twice, once for its length, then, after one output
+// reservation per job and warp, to copy the segments' chars into one
+// contiguous line.  Lines longer than WALK_CAP segments and cycles (no
+// head) go through list ranking (pointer jumping from the first state
+// rebuilt from the records, or HEC), line lengths at the heads
+// (k_chain_len), one reservation per line (k_line_reserve) and a copy per
+// segment (k_seg_copy).
 
 // The chars a segment adds to its line: all k - 1 + len for a line's first
 // segment (a head-pool id), len - 1 for the others.
@@ -1585,15 +1578,16 @@ __global__ void __launch_bounds__(256) k_rank_init(const uint32_t* __restrict__ 
 }
 
 // One round of asynchronous pointer jumping over the active list (act ==
-// nullptr: the first round, over the ids [0, n0)).  Entries are (pointer,
-// distance) pairs in one 64-bit word, so a concurrent reader always sees a
-// consistent pair; the list keeps the entries whose pointer does not yet
-// reach a head.
+// nullptr: the first round, over the ids [0, *act_count)).  Entries are
+// (pointer, distance) pairs in one 64-bit word, so a concurrent reader
+// always sees a consistent pair; the list keeps the entries whose pointer
+// does not yet reach a head.  Any mix of first-state entries (predecessor,
+// its chars) and final ones (head, chars before) is a valid state.
 __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restrict__ X, const uint32_t* __restrict__ act,
-                             const uint32_t* act_count, uint32_t n0, uint32_t* __restrict__ act_out,
+                             const uint32_t* act_count, uint32_t* __restrict__ act_out,
                              uint32_t* act_out_count) {
   __shared__ uint32_t sc[33];
-  const uint32_t na = act ? *act_count : n0;
+  const uint32_t na = *act_count;
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   // whole blocks iterate together (block_append needs every thread)
   for (uint64_t j0 = uint64_t(blockIdx.x) * blockDim.x; j0 < na; j0 += stride) {
@@ -1615,6 +1609,167 @@ __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restri
     if (keep) act_out[slot] = s;
   }
 }
+
+// ---- the line walk
+constexpr uint32_t WALK_CAP = 1024;                // segments a line walk follows
+constexpr unsigned long long LINE_WALKED = ~0ull;  // line base of a line k_walk_emit wrote
+constexpr uint32_t JOB_NONE = 0xFFFFFFFFu;
+
+// Reserves want bytes of job's output for each lane of a warp (every lane
+// calls; a lane with want 0 or job JOB_NONE takes nothing) with one atomic
+// per job present in the warp.  The lanes of one job must be consecutive,
+// apart from lanes that take nothing (head-pool ids lie in job order).
+// Returns the lane's offset in its job's output.
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long* jout, uint32_t job,
+                                                           unsigned long long want) {
+  const uint32_t lane = threadIdx.x & 31u;
+  unsigned long long inc = want;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const unsigned long long v = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+    if (lane >= uint32_t(d)) inc += v;
+  }
+  const uint32_t grp = __match_any_sync(0xFFFFFFFFu, job);
+  const uint32_t first = uint32_t(__ffs(grp)) - 1u, last = 31u - uint32_t(__clz(grp));
+  const unsigned long long before = __shfl_sync(0xFFFFFFFFu, inc - want, first);
+  const unsigned long long total = __shfl_sync(0xFFFFFFFFu, inc, last) - before;
+  unsigned long long base = 0;
+  if (lane == first && job != JOB_NONE && total) base = atomicAdd(jout + job, total);
+  base = __shfl_sync(0xFFFFFFFFu, base, first);
+  return base + (inc - want - before);
+}
+
+// One thread writes one line: whole aligned 4-byte words as they fill, and
+// byte by byte the bytes of its first and last words (which it shares with
+// the neighbouring lines, or which lie outside the output buffer: the
+// buffer may start at any byte).  Positions are addresses.
+struct LineOut {
+  uintptr_t p;   // next byte of the line
+  uintptr_t p0;  // its first byte
+  uint32_t acc;  // the bytes of the word at p & ~3 below p
+};
+
+// 4 bytes at any alignment from two aligned words (the segment chars'
+// allocation ends with slack, so the second word is inside it)
+__device__ __forceinline__ uint32_t load4u(const char* src) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+  const uint32_t sh = 8u * uint32_t(a & 3u);
+  return sh ? __funnelshift_r(w[0], w[1], sh) : w[0];
+}
+
+// Appends bytes [0, n) of v (n <= 4 - (p & 3)) and stores the word they fill.
+__device__ __forceinline__ void line_bytes(LineOut& L, uint32_t v, uint32_t n) {
+  const uint32_t fill = uint32_t(L.p & 3u);
+  const uintptr_t wpos = L.p - fill;
+  L.acc |= (n == 4 ? v : (v & ((1u << (8 * n)) - 1u))) << (8 * fill);
+  L.p += n;
+  if (fill + n == 4) {
+    if (wpos >= L.p0) {
+      *reinterpret_cast<uint32_t*>(wpos) = L.acc;
+    } else {
+      for (uint32_t b = uint32_t(L.p0 - wpos); b < 4; ++b) reinterpret_cast<char*>(wpos)[b] = char(L.acc >> (8 * b));
+    }
+    L.acc = 0;
+  }
+}
+
+__device__ __forceinline__ void line_put(LineOut& L, const char* src, uint32_t n) {
+  while (n) {
+    const uint32_t take = min(n, 4u - uint32_t(L.p & 3u));
+    line_bytes(L, load4u(src), take);
+    src += take;
+    n -= take;
+  }
+}
+
+// The line break, then the bytes of the last word not yet stored.
+__device__ __forceinline__ void line_end(LineOut& L) {
+  line_bytes(L, uint32_t('\n'), 1);
+  const uint32_t fill = uint32_t(L.p & 3u);
+  if (fill) {
+    const uintptr_t wpos = L.p - fill;
+    for (uint32_t b = (wpos >= L.p0 ? 0u : uint32_t(L.p0 - wpos)); b < fill; ++b)
+      reinterpret_cast<char*>(wpos)[b] = char(L.acc >> (8 * b));
+  }
+}
+
+// Every stitched line from its head, one thread per head-pool id: the walk
+// follows the line's records for its length (up to WALK_CAP segments after
+// the head), the warp reserves its lines' bytes, and the walk follows the
+// records again (now mostly in L2) to copy each segment's chars into the
+// line.  A line that goes on past WALK_CAP segments is left to the ranking
+// path: its head goes to longl.  wst[0] counts the segments of the lines
+// written (those with ids below nx), wst[1] the lines left.  cap <=
+// WALK_CAP (smaller only to test the ranking path).
+__global__ void __launch_bounds__(256) k_walk_emit(uint32_t H, const SegRec* __restrict__ seg, uint32_t nx, int k,
+                                                   const JobTab* __restrict__ jobs, unsigned long long* __restrict__ jout,
+                                                   const char* __restrict__ segchars, char* __restrict__ out,
+                                                   uint32_t cap, uint32_t* __restrict__ longl, uint32_t lcap,
+                                                   uint32_t* wst, Counters* ctr) {
+  __shared__ uint32_t sc[33];
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  uint32_t walked = 0;
+  // whole warps iterate together (warp_reserve needs every lane)
+  for (uint64_t h0 = uint64_t(blockIdx.x) * blockDim.x; h0 < H; h0 += stride) {
+    const uint64_t h = h0 + threadIdx.x;
+    SegRec r{0ull, 0u, NONE};
+    if (h < H) r = seg[nx + h];
+    const bool live = r.len != 0;
+    unsigned long long len = live ? uint64_t(k) - 1u + r.len : 0ull;
+    uint32_t s = live ? r.next : NONE, hops = 0;
+    while (s < nx && hops < cap) {
+      const SegRec q = seg[s];
+      len += q.len - 1u;
+      s = q.next;
+      ++hops;
+    }
+    const bool done = live && s == NONE;
+    const uint32_t job = done ? uint32_t(r.off_job >> SEG_OFF_BITS) : JOB_NONE;
+    const unsigned long long o = warp_reserve(jout, job, done ? len + 1u : 0ull);
+    if (live && !done) {
+      const uint32_t i = atomicAdd(wst + 1, 1u);
+      if (i < lcap) longl[i] = uint32_t(h);
+      else atomicOr(&ctr->err, ERR_INTERNAL);  // a left line holds more than cap cross ids
+    }
+    if (done) {
+      walked += hops;
+      const JobTab& J = jobs[job];
+      if (o + len + 1u > J.ocap) {
+        atomicOr(&ctr->err, ERR_CAPACITY);
+      } else {
+        const uintptr_t a = reinterpret_cast<uintptr_t>(out + J.obase + o);
+        LineOut L{a, a, 0u};
+        line_put(L, segchars + (r.off_job & SEG_OFF_MASK), uint32_t(k) - 1u + r.len);
+        uint32_t t = r.next;
+        for (uint32_t q = 0; q < hops; ++q) {
+          const SegRec g = seg[t];
+          line_put(L, segchars + (g.off_job & SEG_OFF_MASK), g.len - 1u);
+          t = g.next;
+        }
+        line_end(L);
+      }
+    }
+  }
+  uint32_t tot;
+  block_excl_scan(walked, sc, &tot);
+  if (threadIdx.x == 0 && tot) atomicAdd(wst, tot);
+}
+
+// The ranking's first state from the segment records (when the walk left
+// lines or cycles, and for HEC): a line's first segment is a head; segment
+// x (x < nx) points at its predecessor, with the chars the predecessor adds.
+__global__ void __launch_bounds__(256) k_seg_xinit(uint32_t S, const SegRec* __restrict__ seg, uint32_t nx, int k,
+                                                   unsigned long long* __restrict__ X) {
+  for (uint64_t s = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; s < S; s += uint64_t(gridDim.x) * blockDim.x) {
+    const SegRec r = seg[s];
+    if (!r.len) continue;
+    if (s >= nx) X[s] = pk(uint32_t(s) | HEAD_BIT, 0);
+    if (r.next < nx) X[r.next] = pk(uint32_t(s), seg_w(uint32_t(s), r.len, nx, k));
+  }
+}
+
+__global__ void k_set_u32(uint32_t* p, uint32_t v) { *p = v; }
 
 // Line length of each chain, stored at its head (every live chain has one
 // tail, which writes it; the array is zeroed before).  A line's tail starts
@@ -1650,18 +1805,36 @@ __global__ void k_chain_len(uint32_t S, const SegRec* __restrict__ seg, const un
   }
 }
 
-// Each head's line base in the output: its job's region, after the job's
-// closed lines, at the job's running offset (the scan of line lengths over
-// the head pools, which lie in job order).
-__global__ void k_line_base(uint32_t H, const SegRec* __restrict__ heads, const JobTab* __restrict__ jobs,
-                            const unsigned long long* __restrict__ jclosed, const unsigned long long* __restrict__ loff,
-                            unsigned long long* __restrict__ lbase) {
-  for (uint32_t h = blockIdx.x * blockDim.x + threadIdx.x; h < H; h += gridDim.x * blockDim.x) {
-    const SegRec r = heads[h];
-    if (!r.len) continue;
-    const uint32_t job = uint32_t(r.off_job >> SEG_OFF_BITS);
-    const JobTab& J = jobs[job];
-    lbase[h] = J.obase + jclosed[job] + (loff[h] - loff[J.seg_base]);
+// Each line's base in the output, reserved after the job's lines so far:
+// over the heads in list (the lines the walk left), or over all head-pool
+// ids (list == nullptr, after HEC ranking: one reservation per job and
+// warp).  A head without a length keeps LINE_WALKED, so no segment copies
+// into it.
+__global__ void __launch_bounds__(256) k_line_reserve(uint32_t n, const uint32_t* __restrict__ list,
+                                                      const SegRec* __restrict__ heads,
+                                                      const JobTab* __restrict__ jobs,
+                                                      unsigned long long* __restrict__ jout,
+                                                      const uint32_t* __restrict__ hlen,
+                                                      unsigned long long* __restrict__ lbase, Counters* ctr) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  // whole warps iterate together (warp_reserve needs every lane)
+  for (uint64_t i0 = uint64_t(blockIdx.x) * blockDim.x; i0 < n; i0 += stride) {
+    const uint64_t i = i0 + threadIdx.x;
+    uint32_t h = 0, job = JOB_NONE, want = 0;
+    if (i < n) {
+      h = list ? list[i] : uint32_t(i);
+      const SegRec r = heads[h];
+      want = r.len ? hlen[h] : 0u;
+      if (want) job = uint32_t(r.off_job >> SEG_OFF_BITS);
+    }
+    // a list's heads come in any job order: one atomic each
+    const unsigned long long o = list ? (want ? atomicAdd(jout + job, (unsigned long long)want) : 0ull)
+                                      : warp_reserve(jout, job, want);
+    if (want) {
+      const JobTab& J = jobs[job];
+      if (o + want > J.ocap) atomicOr(&ctr->err, ERR_CAPACITY);
+      else lbase[h] = J.obase + o;
+    }
   }
 }
 
@@ -1700,15 +1873,24 @@ __global__ void __launch_bounds__(256) k_seg_copy(
         if (live[q]) {
           hd[q] = ptr_of(v) - nx;
           off[q] = pk_o(v);
-          src[q] = (r.off_job & SEG_OFF_MASK) + (s < nx ? uint32_t(k) : 0u);
+          src[q] = r.off_job & SEG_OFF_MASK;
           nb[q] = seg_w(uint32_t(s), r.len, nx, k);
           last[q] = r.next == NONE;
         }
       }
     }
+    // (segments of lines the walk wrote copy nothing)
 #pragma unroll
-    for (int q = 0; q < PER; ++q)
-      if (live[q]) dst[q] = lbase[hd[q]] + off[q];
+    for (int q = 0; q < PER; ++q) {
+      if (!live[q]) continue;
+      const unsigned long long lb = lbase[hd[q]];
+      if (lb == LINE_WALKED) {
+        nb[q] = 0;
+        last[q] = 0;
+      } else {
+        dst[q] = lb + off[q];
+      }
+    }
     // groups of 8 lanes: group g copies, one after another, the segments
     // resolved by its own 8 lanes.  Each lane of the group stores aligned
     // 4-byte words of the destination, funnel-shifted from the two aligned
@@ -1786,7 +1968,7 @@ __global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restri
       for (uint32_t guard = 0; guard <= S; ++guard) {
         const SegRec r = seg[t];
         const uint64_t m = r.len - 1u;
-        if (q < m) return segchars[(r.off_job & SEG_OFF_MASK) + k + q];
+        if (q < m) return segchars[(r.off_job & SEG_OFF_MASK) + q];
         q -= m;
         t = r.next;
       }
@@ -1822,17 +2004,6 @@ __global__ void k_seg_cycles(Counters* ctr, uint32_t S, const uint32_t* __restri
     for (uint64_t t = 0; t + 1 < len; ++t) dst[t] = at((best + N * 64 - (k - 1) + t) % N);
     dst[len - 1] = '\n';
     atomicAdd(&ctr->cycles, 1ull);
-  }
-}
-
-// After the copy: each job's byte count = closed lines + stitched lines
-// (the scan total over its head pool).
-__global__ void k_job_finish(const JobTab* __restrict__ jobs, uint32_t njobs,
-                             const unsigned long long* __restrict__ jclosed,
-                             const unsigned long long* __restrict__ loff, unsigned long long* __restrict__ jout) {
-  for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < njobs; j += gridDim.x * blockDim.x) {
-    const JobTab& J = jobs[j];
-    jout[j] = jclosed[j] + (loff[J.seg_base + J.seg_cap] - loff[J.seg_base]);
   }
 }
 
@@ -2775,19 +2946,21 @@ static int scatter_finish(Env& e, const Front& f, const Scatter& sc, uint64_t*& 
     uint32_t* item_start = reinterpret_cast<uint32_t*>(f.cursor + sc.mc);
     const size_t sm2 = size_t(MID_CHUNK) * (8 * nw + 8) + size_t(nb) * 16 + 4 + size_t(sc.mc + 1) * 4;
     int o2 = 0;
-    if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_scatter_mid<1>, 256, sm2));
-    else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_scatter_mid<2>, 256, sm2));
+    if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_scatter_mid<1>, MID_THREADS, sm2));
+    else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_scatter_mid<2>, MID_THREADS, sm2));
     if (o2 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
     e.launches += 3;
     k_mid_items<<<1, 256, 0, e.stream>>>(f.boff, sc.fb, sc.mc, item_start);
     k_coarse_init<<<grid_for(e, sc.nsub, 256), 256, 0, e.stream>>>(f.boff, sc.sb, sc.nsub, f.fcur);
     UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
     if (nw == 1)
-      k_scatter_mid<1><<<e.sm_count * o2, 256, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start, sc.fb, sc.sb,
-                                                                sc.mc, f.fcur, sc.k2, sc.l2, sc.b2, e.ctr);
+      k_scatter_mid<1><<<e.sm_count * o2, MID_THREADS, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start,
+                                                                        sc.fb, sc.sb, sc.mc, f.fcur, sc.k2, sc.l2,
+                                                                        sc.b2, e.ctr);
     else
-      k_scatter_mid<2><<<e.sm_count * o2, 256, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start, sc.fb, sc.sb,
-                                                                sc.mc, f.fcur, sc.k2, sc.l2, sc.b2, e.ctr);
+      k_scatter_mid<2><<<e.sm_count * o2, MID_THREADS, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start,
+                                                                        sc.fb, sc.sb, sc.mc, f.fcur, sc.k2, sc.l2,
+                                                                        sc.b2, e.ctr);
     pkeys = sc.k1;
     plink = sc.l1;
   }
@@ -3028,15 +3201,15 @@ static int run_graph(Env& e, int slot, uint64_t key, F&& body) {
   return UC_OK;
 }
 
-// first_n >= 0: X already holds the first state (written by the tiles) and
-// the first round runs over the ids [0, first_n).
+// prefilled: X already holds a state (written by the tiles and the line
+// walk) and the first round runs over the ids [0, cnt[0]), cnt[0] set on the
+// device before.
 static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t nmax, bool count_on_device,
                       unsigned long long* X, uint32_t* act0, uint32_t* act1, uint32_t* cnt, uint32_t& rounds,
-                      uint32_t*& act_final, uint32_t*& cnt_final, int64_t first_n = -1) {
+                      uint32_t*& act_final, uint32_t*& cnt_final, bool prefilled = false) {
   rounds = 2;
   for (uint64_t t = 1; t < nmax; t <<= 1) ++rounds;
   const int grid = grid_for(e, nmax ? nmax : 1, 256);
-  const bool prefilled = first_n >= 0;
   if (prefilled) {
     UC_CK(cudaMemsetAsync(cnt + 1, 0, rounds * 4, e.stream));
   } else {
@@ -3048,8 +3221,7 @@ static int rank_lists(Env& e, const uint32_t* prev, const uint32_t* w, uint64_t 
   for (uint32_t r = 0; r < rounds; ++r) {
     ++e.launches;
     const uint32_t* in = (r == 0 && prefilled) ? nullptr : lists[r & 1];
-    k_rank_round<<<grid, 256, 0, e.stream>>>(X, in, cnt + r, prefilled ? uint32_t(first_n) : 0u,
-                                             lists[(r + 1) & 1], cnt + r + 1);
+    k_rank_round<<<grid, 256, 0, e.stream>>>(X, in, cnt + r, lists[(r + 1) & 1], cnt + r + 1);
   }
   UC_CK(cudaGetLastError());
   act_final = lists[rounds & 1];
@@ -3333,18 +3505,28 @@ struct StitchBufs {
   uint32_t *act0, *act1;
   uint8_t* oncyc;
   uint32_t* hlen;
-  unsigned long long *loff, *lbase, *stmp;
+  unsigned long long* lbase;
+  uint32_t* longl;  // heads of the lines the walk leaves (lcap entries)
+  uint32_t lcap;
   uint32_t* rcnt;
   HecPool hp;
 };
 
-// The cross-tile stitch over X cross-indexed segments and Hp head-pool ids:
-// ranking (pointer jumping, or HEC with pointer jumping when its rounds run
-// out), line lengths at the heads, line bases per job, the segment copies
-// into out, each job's byte count in jd.jout (after jd.jclosed), and the
-// rare segment cycles.
+// Heads the walk can leave: each left line holds more than the walk's cap
+// of cross ids.
+static uint32_t walk_cap(const Env& e) {
+  return (e.faults.walk_cap && e.faults.walk_cap < WALK_CAP) ? e.faults.walk_cap : WALK_CAP;
+}
+static uint64_t long_cap(const Env& e, uint64_t X) { return X / walk_cap(e) + 64; }
+
+// The cross-tile stitch over X cross-indexed segments and Hp head-pool ids,
+// into out after each job's closed lines (jd.jout: each job's byte count,
+// closed lines before, all lines after): the line walk, then, for the
+// lines it leaves and for cycles, ranking (pointer jumping, or HEC with
+// pointer jumping when its rounds run out), line lengths at the heads, one
+// reservation per line, the segment copies, and the rare segment cycles.
 static int run_stitch(Env& e, const StitchBufs& b, uint64_t X, uint64_t Hp, int k, int nw, bool want_hec,
-                      uint32_t RH, const JobDev& jd, uint32_t njobs, char* out, uint32_t& rounds) {
+                      uint32_t RH, const JobDev& jd, char* out, uint32_t& rounds) {
   rounds = 0;
   const uint32_t S = uint32_t(X + Hp), nx = uint32_t(X), H = uint32_t(Hp);
   SegRec* seg = b.seg;
@@ -3352,11 +3534,31 @@ static int run_stitch(Env& e, const StitchBufs& b, uint64_t X, uint64_t Hp, int 
   char* segc = b.segc;
   uint32_t *act0 = b.act0, *act1 = b.act1, *hlen = b.hlen, *rcnt = b.rcnt;
   uint8_t* oncyc = b.oncyc;
-  unsigned long long *loff = b.loff, *lbase = b.lbase, *stmp = b.stmp;
+  unsigned long long* lbase = b.lbase;
   HecPool hp = b.hp;
+  uint32_t* wst = rcnt + 48;  // the walk's counters (the rounds use at most 35 list counts)
   int r = UC_OK;
   const int gs = grid_for(e, S, 256);
   uint32_t *act = nullptr, *left = nullptr;
+  uint32_t nlong = 0;
+  if (!want_hec) {
+    // the line walk writes every line its head reaches within WALK_CAP
+    // segments; the rest is ranked from the first state, built below
+    UC_CK(cudaMemsetAsync(wst, 0, 8, e.stream));
+    ++e.launches;
+    k_walk_emit<<<grid_for(e, H, 256), 256, 0, e.stream>>>(H, seg, nx, k, jd.tab, jd.jout, segc, out, walk_cap(e),
+                                                           b.longl, b.lcap, wst, e.ctr);
+    uint32_t hw[2] = {0, 0};
+    UC_CK(cudaMemcpyAsync(hw, wst, 8, cudaMemcpyDeviceToHost, e.stream));
+    UC_CK(cudaStreamSynchronize(e.stream));
+    if (hw[0] == nx && hw[1] == 0) return UC_OK;
+    nlong = std::min(hw[1], b.lcap);
+    ++e.launches;
+    k_set_u32<<<1, 1, 0, e.stream>>>(rcnt, nx);
+  }
+  // the first state (HEC's level 0 takes the predecessors from it)
+  ++e.launches;
+  k_seg_xinit<<<gs, 256, 0, e.stream>>>(S, seg, nx, k, Xr);
   bool hec = want_hec;
   if (hec) {
     // HEC matching rounds, captured as one graph
@@ -3380,16 +3582,16 @@ static int run_stitch(Env& e, const StitchBufs& b, uint64_t X, uint64_t Hp, int 
     }
   }
   if (!hec) {
-    // pointer-jumping rounds, captured as one graph.  Without HEC the tiles
-    // wrote the first state; after a HEC attempt it is rebuilt from the
-    // level-0 links the HEC pool kept
+    // pointer-jumping rounds, captured as one graph: after the walk from the
+    // state rebuilt above (over the ids [0, X)); after a HEC attempt from
+    // the level-0 links the HEC pool kept
     uint32_t rr = 2;
     for (uint64_t t = 1; t < S; t <<= 1) ++rr;
     int rl = UC_OK;
-    const bool first_from_tiles = !want_hec;
-    r = run_graph(e, 0, (uint64_t(rr) << 33) | (uint64_t(first_from_tiles) << 32) | uint32_t(gs), [&] {
-      rl = first_from_tiles ? rank_lists(e, nullptr, nullptr, S, false, Xr, act0, act1, rcnt, rounds, act, left, nx)
-                            : rank_lists(e, hp.prv, hp.wt, S, false, Xr, act0, act1, rcnt, rounds, act, left);
+    const bool prefilled = !want_hec;
+    r = run_graph(e, 0, (uint64_t(rr) << 33) | (uint64_t(prefilled) << 32) | uint32_t(gs), [&] {
+      rl = prefilled ? rank_lists(e, nullptr, nullptr, S, false, Xr, act0, act1, rcnt, rounds, act, left, true)
+                     : rank_lists(e, hp.prv, hp.wt, S, false, Xr, act0, act1, rcnt, rounds, act, left);
       cudaMemsetAsync(oncyc, 0, S, e.stream);
       ++e.launches;
       k_mark_cycle<<<gs, 256, 0, e.stream>>>(act, left, oncyc);
@@ -3397,16 +3599,22 @@ static int run_stitch(Env& e, const StitchBufs& b, uint64_t X, uint64_t Hp, int 
     if (r) return r;
     if (rl) return rl;
   }
-  // line length at each head, the heads' running offsets per job, their line
-  // bases, then every segment's chars
+  // line length at each head, one reservation per line not yet written,
+  // then every segment's chars (the segments of written lines skip)
   UC_CK(cudaMemsetAsync(hlen, 0, size_t(H) * 4, e.stream));
-  e.launches += 4;
+  UC_CK(cudaMemsetAsync(lbase, 0xFF, size_t(H) * 8, e.stream));
+  e.launches += 2;
   k_chain_len<<<gs, 256, 0, e.stream>>>(S, seg, Xr, oncyc, nx, k, hlen, e.ctr);
-  e.launches += scan_launches(H);
-  scan_excl<uint32_t, unsigned long long>(hlen, H, loff, stmp, e.stream);
-  k_line_base<<<grid_for(e, H, 256), 256, 0, e.stream>>>(H, seg + nx, jd.tab, jd.jclosed, loff, lbase);
+  if (want_hec) {
+    ++e.launches;
+    k_line_reserve<<<grid_for(e, H, 256), 256, 0, e.stream>>>(H, nullptr, seg + nx, jd.tab, jd.jout, hlen, lbase,
+                                                              e.ctr);
+  } else if (nlong) {
+    ++e.launches;
+    k_line_reserve<<<grid_for(e, nlong, 256), 256, 0, e.stream>>>(nlong, b.longl, seg + nx, jd.tab, jd.jout, hlen,
+                                                                  lbase, e.ctr);
+  }
   k_seg_copy<<<grid_for(e, S, 256), 256, 0, e.stream>>>(S, seg, Xr, oncyc, nx, lbase, segc, out, k);
-  k_job_finish<<<(njobs + 255) / 256, 256, 0, e.stream>>>(jd.tab, njobs, jd.jclosed, loff, jd.jout);
   uint32_t hleft = 0;
   UC_CK(cudaMemcpyAsync(&hleft, left, 4, cudaMemcpyDeviceToHost, e.stream));
   UC_CK(cudaStreamSynchronize(e.stream));
@@ -3423,7 +3631,7 @@ static int run_stitch(Env& e, const StitchBufs& b, uint64_t X, uint64_t Hp, int 
 
 // Back arena bytes of the fused path: the bucketed copies and their staging,
 // the segment pool (Sp segments for X cross k-mers) and the stitch arrays.
-static size_t back_bytes(uint64_t copies, uint64_t X, uint64_t Sp, int nw, int k, bool want_hec) {
+static size_t back_bytes(const Env& e, uint64_t copies, uint64_t X, uint64_t Sp, int nw, int k, bool want_hec) {
   const uint64_t segchars = Sp * uint64_t(k) + copies + 64;
   const uint32_t R = 64;
   size_t back = 0;
@@ -3433,8 +3641,8 @@ static size_t back_bytes(uint64_t copies, uint64_t X, uint64_t Sp, int nw, int k
   add(Sp * sizeof(SegRec)); add(Sp * 8);                                  // segment records, ranking
   add(segchars);
   add(Sp * 4); add(Sp * 4); add(Sp);                                      // act0, act1, oncyc
-  add(Hp * 4); add((Hp + 1) * 8); add(Hp * 8);                            // line lengths, offsets, bases
-  add(scan_tmp_elems(Hp) * 8); add(R * 4);
+  add(Hp * 4); add(Hp * 8); add(long_cap(e, X) * 4);                         // line lengths, bases, left lines
+  add(R * 4);
   if (want_hec) add(hec_bytes(Sp, hec_rounds(Sp)));
   return back;
 }
@@ -3453,7 +3661,7 @@ void batch_footprint(const Env& e, uint32_t njobs, const size_t* bytes, int k, i
   const size_t slack = size_t(16) << 20;
   front = front_bytes(N, nw, P.M, true) + slack + 4096;
   const uint64_t X = N, copies = N + X, Sp = 2 * X + njobs;
-  back = std::max(back_bytes(copies, X, Sp, nw, k, e.tune.contract_method == UC_CONTRACT_HEC),
+  back = std::max(back_bytes(e, copies, X, Sp, nw, k, e.tune.contract_method == UC_CONTRACT_HEC),
                   line_index_bytes(tb, nmax)) + slack + 4096;
 }
 
@@ -3587,7 +3795,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   const uint32_t R = 64;
   const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
   const uint32_t RH = hec_rounds(e, Sp);
-  const size_t back = back_bytes(copies, X, Sp, nw, k, want_hec);
+  const size_t back = back_bytes(e, copies, X, Sp, nw, k, want_hec);
   r = e.reserve(1, back);
   if (r) return r;
   auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
@@ -3601,9 +3809,8 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   uint32_t* act1 = T32(Sp);
   uint8_t* oncyc = static_cast<uint8_t*>(e.take(1, Sp));
   uint32_t* hlen = T32(Hp);
-  unsigned long long* loff = T64(Hp + 1);
   unsigned long long* lbase = T64(Hp);
-  unsigned long long* stmp = T64(scan_tmp_elems(Hp));
+  uint32_t* longl = T32(long_cap(e, X));
   uint32_t* rcnt = T32(R);
   if (!rcnt) return e.fail(UC_EBUDGET, "back arena overflow");
   HecPool hp{};
@@ -3637,9 +3844,8 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   tp.mode = 1;
   tp.out = out;
   tp.segchars = segc;
-  tp.segchars_cap = segchars;
+  tp.segchars_cap = segchars - 64;  // the line walk reads up to 7 bytes past a segment's chars
   tp.seg = seg;
-  tp.Xr = Xr;
   tp.xcount = uint32_t(X);
   tp.jobs = jd.tab;
   tp.jout = jd.jout;
@@ -3653,8 +3859,8 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   if (e.h_ctr->err) return e.check_err(e.h_ctr);
   UC_CK(cudaMemcpyAsync(jd.jclosed, jd.jout, njobs * 8, cudaMemcpyDeviceToDevice, e.stream));
   uint32_t rounds = 0;
-  StitchBufs sbuf{seg, Xr, segc, act0, act1, oncyc, hlen, loff, lbase, stmp, rcnt, hp};
-  r = run_stitch(e, sbuf, X, Hp, k, nw, want_hec, RH, jd, njobs, out, rounds);
+  StitchBufs sbuf{seg, Xr, segc, act0, act1, oncyc, hlen, lbase, longl, uint32_t(long_cap(e, X)), rcnt, hp};
+  r = run_stitch(e, sbuf, X, Hp, k, nw, want_hec, RH, jd, out, rounds);
   if (r) return r;
   UC_CK(cudaGetLastError());
   cudaEventRecord(e.ev[4], e.stream);
@@ -3861,7 +4067,7 @@ int compact_streamed(Env& e, const char* h_text, size_t bytes, int k, int l, cha
   const uint32_t R = 64;
   const bool want_hec = e.tune.contract_method == UC_CONTRACT_HEC;
   const uint32_t RH = hec_rounds(e, Sp);
-  r = e.reserve(1, back_bytes(copies, X, Sp, nw, k, want_hec) + gout + sout + 4096);
+  r = e.reserve(1, back_bytes(e, copies, X, Sp, nw, k, want_hec) + gout + sout + 4096);
   if (r) return r;
   auto T64 = [&](uint64_t c) { return static_cast<unsigned long long*>(e.take(1, c * 8)); };
   auto T32 = [&](uint64_t c) { return static_cast<uint32_t*>(e.take(1, c * 4)); };
@@ -3874,9 +4080,8 @@ int compact_streamed(Env& e, const char* h_text, size_t bytes, int k, int l, cha
   uint32_t* act1 = T32(Sp);
   uint8_t* oncyc = static_cast<uint8_t*>(e.take(1, Sp));
   uint32_t* hlen = T32(Hp);
-  unsigned long long* loff = T64(Hp + 1);
   unsigned long long* lbase = T64(Hp);
-  unsigned long long* stmp = T64(scan_tmp_elems(Hp));
+  uint32_t* longl = T32(long_cap(e, X));
   uint32_t* rcnt = T32(R);
   char* d_gout = static_cast<char*>(e.take(1, gout));
   char* d_sout = static_cast<char*>(e.take(1, sout));
@@ -3928,9 +4133,8 @@ int compact_streamed(Env& e, const char* h_text, size_t bytes, int k, int l, cha
   tp.mode = 1;
   tp.out = d_gout;
   tp.segchars = segc;
-  tp.segchars_cap = segchars;
+  tp.segchars_cap = segchars - 64;  // the line walk reads up to 7 bytes past a segment's chars
   tp.seg = seg;
-  tp.Xr = Xr;
   tp.xcount = uint32_t(X);
   tp.jobs = jd.tab;
   tp.jout = jd.jout;
@@ -3966,9 +4170,10 @@ int compact_streamed(Env& e, const char* h_text, size_t bytes, int k, int l, cha
   J.ocap = sout;
   UC_CK(cudaMemcpyAsync(jd.tab, &J, sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
   UC_CK(cudaMemsetAsync(jd.jclosed, 0, 8, e.stream));
+  UC_CK(cudaMemsetAsync(jd.jout, 0, 8, e.stream));
   uint32_t rounds = 0;
-  StitchBufs sbuf{seg, Xr, segc, act0, act1, oncyc, hlen, loff, lbase, stmp, rcnt, hp};
-  r = run_stitch(e, sbuf, X, Hp, k, nw, want_hec, RH, jd, 1, d_sout, rounds);
+  StitchBufs sbuf{seg, Xr, segc, act0, act1, oncyc, hlen, lbase, longl, uint32_t(long_cap(e, X)), rcnt, hp};
+  r = run_stitch(e, sbuf, X, Hp, k, nw, want_hec, RH, jd, d_sout, rounds);
   if (r) return r;
   cudaEventRecord(e.ev[4], e.stream);
   unsigned long long sb = 0;
