@@ -599,8 +599,10 @@ __global__ void k_coarse_init(const unsigned long long* __restrict__ boff, uint3
     ccur[j] = boff[uint64_t(j) << fb];
 }
 
+constexpr int COARSE_THREADS = 256;
+
 template <int NW>
-__global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restrict__ keys,
+__global__ void __launch_bounds__(COARSE_THREADS) k_scatter_coarse(const uint64_t* __restrict__ keys,
                                                         const uint32_t* __restrict__ b1,
                                                         const uint32_t* __restrict__ b2, uint64_t n,
                                                         uint32_t fb, uint32_t mc,
@@ -619,12 +621,12 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
   for (uint64_t c0 = uint64_t(blockIdx.x) * SC_CHUNK; c0 < n; c0 += uint64_t(gridDim.x) * SC_CHUNK) {
     const uint32_t cn = uint32_t((n - c0) < uint64_t(SC_CHUNK) ? (n - c0) : uint64_t(SC_CHUNK));
     // every load of the chunk is issued at once; the values stay in registers
-    constexpr int PT = SC_CHUNK / 256;
+    constexpr int PT = SC_CHUNK / COARSE_THREADS;
     Key<NW> kk[PT];
     uint32_t aa[PT], bb[PT];
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
-      const uint32_t t = uint32_t(q) * 256u + threadIdx.x;
+      const uint32_t t = uint32_t(q) * COARSE_THREADS + threadIdx.x;
       if (t < cn) {
         kk[q] = ld_key<NW>(keys, c0 + t);
         aa[q] = b1[c0 + t];
@@ -637,7 +639,7 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
     uint32_t cmask = 0;
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
-      const uint32_t t = uint32_t(q) * 256u + threadIdx.x;
+      const uint32_t t = uint32_t(q) * COARSE_THREADS + threadIdx.x;
       if (t < cn) {
         atomicAdd(hist + (aa[q] >> fb), 1u);
         if (aa[q] != bb[q]) {
@@ -681,7 +683,7 @@ __global__ void __launch_bounds__(256) k_scatter_coarse(const uint64_t* __restri
     // place every copy in its partition's run of the staging area
 #pragma unroll
     for (int q = 0; q < PT; ++q) {
-      const uint32_t t = uint32_t(q) * 256u + threadIdx.x;
+      const uint32_t t = uint32_t(q) * COARSE_THREADS + threadIdx.x;
       const bool live = t < cn;
       uint32_t a = 0, b = 0;
       Key<NW> key;
@@ -1612,6 +1614,7 @@ __global__ void __launch_bounds__(256) k_rank_round(unsigned long long* __restri
 
 // ---- the line walk
 constexpr uint32_t WALK_CAP = 1024;                // segments a line walk follows
+constexpr int WALK_REG = 4;                         // later segments a walk keeps in registers
 constexpr unsigned long long LINE_WALKED = ~0ull;  // line base of a line k_walk_emit wrote
 constexpr uint32_t JOB_NONE = 0xFFFFFFFFu;
 
@@ -1674,13 +1677,41 @@ __device__ __forceinline__ void line_bytes(LineOut& L, uint32_t v, uint32_t n) {
   }
 }
 
+// Appends n bytes from src: up to the destination's next word boundary,
+// then whole words from an aligned source stream (one new load per word),
+// then the rest.
 __device__ __forceinline__ void line_put(LineOut& L, const char* src, uint32_t n) {
-  while (n) {
-    const uint32_t take = min(n, 4u - uint32_t(L.p & 3u));
-    line_bytes(L, load4u(src), take);
-    src += take;
-    n -= take;
+  const uint32_t head = min(n, (4u - uint32_t(L.p & 3u)) & 3u);
+  if (head) {
+    line_bytes(L, load4u(src), head);
+    src += head;
+    n -= head;
   }
+  if (n >= 4) {
+    // the destination is word aligned here and the words lie inside the line
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(a & ~uintptr_t(3));
+    const uint32_t sh = 8u * uint32_t(a & 3u);
+    uint32_t* d = reinterpret_cast<uint32_t*>(L.p);
+    const uint32_t nw = n >> 2;
+    uint32_t cur = w[0];
+    for (uint32_t i = 0; i < nw; ++i) {
+      const uint32_t nxt = sh ? w[i + 1] : 0u;
+      d[i] = sh ? __funnelshift_r(cur, nxt, sh) : w[i];
+      cur = nxt;
+    }
+    L.p += 4u * nw;
+    src += 4u * nw;
+    n &= 3u;
+  }
+  if (n) line_bytes(L, load4u(src), n);
+}
+
+// Appends n <= 4 bytes held in v (its low bytes first).
+__device__ __forceinline__ void line_put4(LineOut& L, uint32_t v, uint32_t n) {
+  const uint32_t take = min(n, 4u - uint32_t(L.p & 3u));
+  if (take) line_bytes(L, v, take);
+  if (n > take) line_bytes(L, v >> (8 * take), n - take);
 }
 
 // The line break, then the bytes of the last word not yet stored.
@@ -1696,9 +1727,9 @@ __device__ __forceinline__ void line_end(LineOut& L) {
 
 // Every stitched line from its head, one thread per head-pool id: the walk
 // follows the line's records for its length (up to WALK_CAP segments after
-// the head), the warp reserves its lines' bytes, and the walk follows the
-// records again (now mostly in L2) to copy each segment's chars into the
-// line.  A line that goes on past WALK_CAP segments is left to the ranking
+// the head; the first WALK_REG records stay in registers), the warp
+// reserves its lines' bytes, and the walk copies each segment's chars into
+// the line (records past the kept ones read again, now mostly in L2).  A line that goes on past WALK_CAP segments is left to the ranking
 // path: its head goes to longl.  wst[0] counts the segments of the lines
 // written (those with ids below nx), wst[1] the lines left.  cap <=
 // WALK_CAP (smaller only to test the ranking path).
@@ -1718,6 +1749,18 @@ __global__ void __launch_bounds__(256) k_walk_emit(uint32_t H, const SegRec* __r
     const bool live = r.len != 0;
     unsigned long long len = live ? uint64_t(k) - 1u + r.len : 0ull;
     uint32_t s = live ? r.next : NONE, hops = 0;
+    // the first WALK_REG later segments stay in registers for the copy
+    SegRec c[WALK_REG];
+#pragma unroll
+    for (int q = 0; q < WALK_REG; ++q) {
+      c[q] = SegRec{0ull, 1u, NONE};
+      if (s < nx && hops < cap) {
+        c[q] = seg[s];
+        len += c[q].len - 1u;
+        s = c[q].next;
+        ++hops;
+      }
+    }
     while (s < nx && hops < cap) {
       const SegRec q = seg[s];
       len += q.len - 1u;
@@ -1738,11 +1781,25 @@ __global__ void __launch_bounds__(256) k_walk_emit(uint32_t H, const SegRec* __r
       if (o + len + 1u > J.ocap) {
         atomicOr(&ctr->err, ERR_CAPACITY);
       } else {
+        // the kept segments' first words load together (most later
+        // segments add no more than 4 chars)
+        uint32_t fw[WALK_REG];
+#pragma unroll
+        for (int q = 0; q < WALK_REG; ++q)
+          fw[q] = (uint32_t(q) < hops && c[q].len > 1u) ? load4u(segchars + (c[q].off_job & SEG_OFF_MASK)) : 0u;
         const uintptr_t a = reinterpret_cast<uintptr_t>(out + J.obase + o);
         LineOut L{a, a, 0u};
         line_put(L, segchars + (r.off_job & SEG_OFF_MASK), uint32_t(k) - 1u + r.len);
-        uint32_t t = r.next;
-        for (uint32_t q = 0; q < hops; ++q) {
+#pragma unroll
+        for (int q = 0; q < WALK_REG; ++q) {
+          if (uint32_t(q) < hops) {
+            const uint32_t n = c[q].len - 1u;
+            if (n <= 4u) line_put4(L, fw[q], n);
+            else line_put(L, segchars + (c[q].off_job & SEG_OFF_MASK), n);
+          }
+        }
+        uint32_t t = c[WALK_REG - 1].next;
+        for (uint32_t q = WALK_REG; q < hops; ++q) {
           const SegRec g = seg[t];
           line_put(L, segchars + (g.off_job & SEG_OFF_MASK), g.len - 1u);
           t = g.next;
@@ -2920,18 +2977,18 @@ static int scatter_l1(Env& e, const Front& f, const Scatter& sc, const uint64_t*
   const size_t sm1 = size_t(2 * chunk) * (8 * nw + 8) + size_t(sc.mc) * 16 + 16;
   // one wave of resident CTAs (the chunks are strided statically)
   int o1 = 0;
-  if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<1>, 256, sm1));
-  else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<2>, 256, sm1));
+  if (nw == 1) UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<1>, COARSE_THREADS, sm1));
+  else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o1, k_scatter_coarse<2>, COARSE_THREADS, sm1));
   if (o1 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
   const int g1 = int(std::max<uint64_t>(1, std::min<uint64_t>((n + chunk - 1) / chunk,
                                                               uint64_t(e.sm_count) * uint64_t(o1))));
   e.launches += 1;
   if (nw == 1)
-    k_scatter_coarse<1><<<g1, 256, sm1, e.stream>>>(keys, b1, b2, n, sc.fb, sc.mc, f.cursor, sc.k1, sc.l1, sc.b1,
-                                                    ids_mode, e.ctr);
+    k_scatter_coarse<1><<<g1, COARSE_THREADS, sm1, e.stream>>>(keys, b1, b2, n, sc.fb, sc.mc, f.cursor, sc.k1, sc.l1,
+                                                               sc.b1, ids_mode, e.ctr);
   else
-    k_scatter_coarse<2><<<g1, 256, sm1, e.stream>>>(keys, b1, b2, n, sc.fb, sc.mc, f.cursor, sc.k1, sc.l1, sc.b1,
-                                                    ids_mode, e.ctr);
+    k_scatter_coarse<2><<<g1, COARSE_THREADS, sm1, e.stream>>>(keys, b1, b2, n, sc.fb, sc.mc, f.cursor, sc.k1, sc.l1,
+                                                               sc.b1, ids_mode, e.ctr);
   UC_CK(cudaGetLastError());
   return UC_OK;
 }
