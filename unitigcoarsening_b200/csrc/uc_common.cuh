@@ -189,20 +189,33 @@ __device__ __forceinline__ uint32_t codes4(const Key<NW>& x, int ch) {
   }
 }
 
-// Write the k chars of a packed key at dst (any alignment): aligned 32-bit
-// stores for the middle, byte stores for the ragged ends.
+// Write the k chars of a packed key at dst (any alignment): byte stores up
+// to the first aligned word, then the key moved down by those chars (one
+// shift) and aligned 32-bit stores from constant shifts, then byte stores
+// for the rest.
 template <int NW>
 __device__ __forceinline__ void spell_key(char* dst, const Key<NW>& x, int k) {
-  int ch = int((4u - uint32_t(reinterpret_cast<uintptr_t>(dst) & 3u)) & 3u);
-  if (ch > k) ch = k;
-  if (ch) {
+  const int ch0 = min(k, int((4u - uint32_t(reinterpret_cast<uintptr_t>(dst) & 3u)) & 3u));
+  Key<NW> y = x;
+  if (ch0) {
     const uint32_t a = ascii4(codes4(x, 0));
-    for (int i = 0; i < ch; ++i) dst[i] = char(a >> (8 * i));
+    for (int i = 0; i < ch0; ++i) dst[i] = char(a >> (8 * i));
+    if constexpr (NW == 1) {
+      y.w[0] = x.w[0] >> (2 * ch0);
+    } else {
+      y.w[0] = (x.w[0] >> (2 * ch0)) | (x.w[1] << (64 - 2 * ch0));
+      y.w[1] = x.w[1] >> (2 * ch0);
+    }
   }
-  for (; ch + 4 <= k; ch += 4) *reinterpret_cast<uint32_t*>(dst + ch) = ascii4(codes4(x, ch));
-  if (ch < k) {
-    const uint32_t a = ascii4(codes4(x, ch));
-    for (int i = 0; ch + i < k; ++i) dst[ch + i] = char(a >> (8 * i));
+  const int rest = k - ch0;
+  const int nw4 = rest >> 2;
+  uint32_t* d = reinterpret_cast<uint32_t*>(dst + ch0);
+#pragma unroll
+  for (int w = 0; w < 8 * NW; ++w)
+    if (w < nw4) d[w] = ascii4(codes4(y, 4 * w));
+  if (rest & 3) {
+    const uint32_t a = ascii4(codes4(y, 4 * nw4));
+    for (int i = 0; i < (rest & 3); ++i) dst[ch0 + 4 * nw4 + i] = char(a >> (8 * i));
   }
 }
 

@@ -89,10 +89,10 @@ struct TileParams {
   uint32_t xcount;              // cross k-mers (the head pool starts there)
 };
 
-// Shared memory of one tile: keys plus four 16-bit arrays per copy, and
-// 16-bit hash slots.
+// Shared memory of one tile: keys plus four 16-bit arrays per copy (sized
+// in fours), and 16-bit hash slots.
 __host__ __device__ inline size_t tile_bytes(int nw, uint32_t cap, uint32_t tslots) {
-  return size_t(cap) * (8u * nw + 8u) + size_t(tslots) * 2u;
+  return size_t(cap) * 8u * nw + size_t((cap + 3u) & ~3u) * 8u + size_t(tslots) * 2u;
 }
 
 // Smallest power of two >= x, for x <= 2^31 (callers bound x first); larger

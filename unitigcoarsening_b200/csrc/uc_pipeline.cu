@@ -559,7 +559,7 @@ __global__ void k_classify(const unsigned long long* __restrict__ tile_begin, Co
       const uint32_t i = atomicAdd(&ctr->nbig, 1u);
       big_list[i] = t;
       const uint64_t ts = big_slots(c, lf);
-      big_size[i] = (c * (8ull * nw + 16ull) + ts * 4ull + 255ull) & ~255ull;
+      big_size[i] = (c * 8ull * nw + ((c + 3ull) & ~3ull) * 16ull + ts * 4ull + 255ull) & ~255ull;
     }
   }
 }
@@ -1029,12 +1029,13 @@ struct TileMem {
 template <int NW, typename IT>
 __device__ __forceinline__ TileMem<NW, IT> carve(char* base, uint32_t cap, uint32_t ts) {
   TileMem<NW, IT> m;
+  const uint32_t cap4 = (cap + 3u) & ~3u;  // the index arrays in fours (vector initialisation)
   m.key = reinterpret_cast<uint64_t*>(base);
   m.A = reinterpret_cast<IT*>(m.key + size_t(cap) * NW);
-  m.B = m.A + cap;
-  m.P = m.B + cap;
-  m.Q = m.P + cap;
-  m.T = m.Q + cap;
+  m.B = m.A + cap4;
+  m.P = m.B + cap4;
+  m.Q = m.P + cap4;
+  m.T = m.Q + cap4;
   m.ts = ts;
   return m;
 }
@@ -1184,12 +1185,15 @@ __device__ void jump_rounds(uint32_t c, IT* px, IT* rx, IT* py, IT* ry, IT*& ptr
   rnk = rx;
 }
 
-template <int NW, typename IT, typename G>
+// KC: k fixed at compile time (0: p.k), so that the masks, shifts and
+// spelling loops of the common shapes are constants.
+template <int NW, typename IT, typename G, int KC = 0>
 __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint64_t beg, uint32_t c,
                              uint32_t job) {
   constexpr uint32_t NONE_I = Ix<IT>::NONE, DUP_I = Ix<IT>::DUP, CNONE_I = Ix<IT>::CNONE;
   constexpr uint32_t OPEN_S = NONE_I - 1u;  // an open segment that starts at an S-only copy
-  const PrefMask pm = pref_mask(p.k);
+  const int k = KC ? KC : p.k;
+  const PrefMask pm = pref_mask(k);
   // this tile's hash slots: the power of two above c * lf / 100, at most the
   // carved table (32-bit arithmetic for shared-memory tiles, c <= 8192)
   uint32_t ts;
@@ -1200,7 +1204,6 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
     ts = ts < m.ts ? ts : m.ts;
   }
   const uint32_t tmask = ts - 1;
-  const int k = p.k;
   // ---- stage the tile's keys (async copies), initialise the work arrays
   if constexpr (sizeof(IT) == 2) {
     // shared-memory tile: asynchronous copies overlap the initialisation
@@ -1214,12 +1217,30 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
       for (int w = 0; w < NW; ++w) m.key[size_t(i) * NW + w] = x.w[w];
     }
   }
-  for (uint32_t i = G::rank(); i < c; i += G::size()) {
-    m.A[i] = IT(CNONE_I);
-    m.B[i] = 0;
-    m.P[i] = IT(NONE_I);
+  if constexpr (sizeof(IT) == 2) {
+    // four 16-bit entries per store (carve sizes the arrays in fours)
+    uint64_t* A4 = reinterpret_cast<uint64_t*>(m.A);
+    uint64_t* B4 = reinterpret_cast<uint64_t*>(m.B);
+    uint64_t* P4 = reinterpret_cast<uint64_t*>(m.P);
+    for (uint32_t i = G::rank(); i < (c + 3u) >> 2; i += G::size()) {
+      A4[i] = 0x7FFF7FFF7FFF7FFFull;  // CNONE
+      B4[i] = 0ull;
+      P4[i] = ~0ull;                  // NONE
+    }
+    if (ts >= 4) {
+      uint64_t* T4 = reinterpret_cast<uint64_t*>(m.T);
+      for (uint32_t i = G::rank(); i < (ts >> 2); i += G::size()) T4[i] = ~0ull;
+    } else {
+      for (uint32_t i = G::rank(); i < ts; i += G::size()) m.T[i] = IT(NONE_I);
+    }
+  } else {
+    for (uint32_t i = G::rank(); i < c; i += G::size()) {
+      m.A[i] = IT(CNONE_I);
+      m.B[i] = 0;
+      m.P[i] = IT(NONE_I);
+    }
+    for (uint32_t i = G::rank(); i < ts; i += G::size()) m.T[i] = IT(NONE_I);
   }
-  for (uint32_t i = G::rank(); i < ts; i += G::size()) m.T[i] = IT(NONE_I);
   if constexpr (sizeof(IT) == 2) __pipeline_wait_prior(0);
   G::sync();
   // ---- prefix table of the P copies (generate_hashmap, assembler.h:120-150):
@@ -1465,7 +1486,7 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
 // global counter, with warp-level synchronisation only.  Block tiles (up to
 // the tile capacity): the whole CTA works one tile.  Larger tiles go to
 // k_tile_big.
-template <int NW>
+template <int NW, int KC>
 __global__ void __launch_bounds__(256) k_tile_warp(TileParams p) {
   extern __shared__ __align__(16) char smem[];
   const uint32_t wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1480,13 +1501,13 @@ __global__ void __launch_bounds__(256) k_tile_warp(TileParams p) {
     const uint32_t t = p.wlist[j];
     const uint64_t beg = p.tile_begin[t];
     const uint32_t c = uint32_t(p.tile_begin[t + 1] - beg);
-    process_tile<NW, uint16_t, WarpGroup>(p, m, beg, c, p.tile_job[t]);
+    process_tile<NW, uint16_t, WarpGroup, KC>(p, m, beg, c, p.tile_job[t]);
     __syncwarp();
     j = __shfl_sync(0xFFFFFFFFu, jn, 0);
   }
 }
 
-template <int NW>
+template <int NW, int KC>
 __global__ void __launch_bounds__(512) k_tile(TileParams p) {
   extern __shared__ __align__(16) char smem[];
   __shared__ uint32_t s_t;
@@ -1501,7 +1522,7 @@ __global__ void __launch_bounds__(512) k_tile(TileParams p) {
     const uint32_t t = p.blist[j];
     const uint64_t beg = p.tile_begin[t];
     const uint32_t c = uint32_t(p.tile_begin[t + 1] - beg);
-    process_tile<NW, uint16_t, BlockGroup>(p, m, beg, c, p.tile_job[t]);
+    process_tile<NW, uint16_t, BlockGroup, KC>(p, m, beg, c, p.tile_job[t]);
     __syncthreads();
   }
 }
@@ -3065,33 +3086,33 @@ static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, i
   return classify_tiles(e, f, P, nw);
 }
 
-template <int NW>
+template <int NW, int KC>
 static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
   tp.wlist = f.wlist;
   tp.blist = f.blist;
   const size_t wsm = size_t(tp.wbytes) * 8;
   int wocc = 0;
   if (tp.wcap) {
-    const int r0 = allow_max_smem(e, k_tile_warp<NW>);
+    const int r0 = allow_max_smem(e, k_tile_warp<NW, KC>);
     if (r0) return r0;
-    UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wocc, k_tile_warp<NW>, 256, wsm));
+    UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&wocc, k_tile_warp<NW, KC>, 256, wsm));
     if (wocc < 1) return e.fail(UC_EINTERNAL, "warp tile kernel does not fit an SM");
   }
   cudaEventRecord(e.ev[8], e.stream);
   if (tp.wcap) {
     ++e.launches;
-    k_tile_warp<NW><<<e.sm_count * wocc, 256, wsm, e.stream>>>(tp);
+    k_tile_warp<NW, KC><<<e.sm_count * wocc, 256, wsm, e.stream>>>(tp);
     UC_CK(cudaGetLastError());
   }
   cudaEventRecord(e.ev[9], e.stream);
   const size_t smem = tile_bytes(NW, tp.cap, tp.tslots);
-  const int r1 = allow_max_smem(e, k_tile<NW>);
+  const int r1 = allow_max_smem(e, k_tile<NW, KC>);
   if (r1) return r1;
   int occ = 0;
-  UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<NW>, int(threads), smem));
+  UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_tile<NW, KC>, int(threads), smem));
   if (occ < 1) return e.fail(UC_EINTERNAL, "tile kernel does not fit an SM");
   ++e.launches;
-  k_tile<NW><<<e.sm_count * occ, threads, smem, e.stream>>>(tp);
+  k_tile<NW, KC><<<e.sm_count * occ, threads, smem, e.stream>>>(tp);
   UC_CK(cudaGetLastError());
   cudaEventRecord(e.ev[5], e.stream);
   e.tiles_timed = true;
@@ -3144,6 +3165,13 @@ static int run_tiles(Env& e, TileParams& tp, const Front& f, uint32_t threads) {
   return UC_OK;
 }
 
+// The tile kernels for tp.k: compile-time k = 31 (64-bit keys) and 63
+// (128-bit keys), the generic form otherwise.
+static int run_tiles_k(Env& e, TileParams& tp, const Front& f, uint32_t threads, int nw) {
+  if (nw == 1) return tp.k == 31 ? run_tiles<1, 31>(e, tp, f, threads) : run_tiles<1, 0>(e, tp, f, threads);
+  return tp.k == 63 ? run_tiles<2, 63>(e, tp, f, threads) : run_tiles<2, 0>(e, tp, f, threads);
+}
+
 int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_t seed, uint32_t* succ,
                uint32_t* pred) {
   if (k < 2 || k > 63) return e.fail(UC_EINPUT, "k must be in [2, 63]");
@@ -3192,7 +3220,7 @@ int find_edges(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
   tp.mode = 0;
   tp.succ = succ;
   tp.pred = pred;
-  r = (nw == 1) ? run_tiles<1>(e, tp, f, 512) : run_tiles<2>(e, tp, f, 512);
+  r = run_tiles_k(e, tp, f, 512, nw);
   if (r) return r;
   r = e.read_ctr();
   e.reset();
@@ -3908,7 +3936,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   tp.jout = jd.jout;
   tp.jseg = jd.jseg;
   const uint32_t threads = e.tune.tile_threads ? e.tune.tile_threads : 512;
-  r = (nw == 1) ? run_tiles<1>(e, tp, f, threads) : run_tiles<2>(e, tp, f, threads);
+  r = run_tiles_k(e, tp, f, threads, nw);
   if (r) return r;
   cudaEventRecord(e.ev[3], e.stream);
   r = e.read_ctr();
@@ -4207,7 +4235,7 @@ int compact_streamed(Env& e, const char* h_text, size_t bytes, int k, int l, cha
     UC_CK(cudaMemsetAsync(jd.jout, 0, 8, e.stream));
     r = classify_tiles(e, f, P, nw, groups[g], groups[g + 1]);
     if (r) return r;
-    r = (nw == 1) ? run_tiles<1>(e, tp, f, threads) : run_tiles<2>(e, tp, f, threads);
+    r = run_tiles_k(e, tp, f, threads, nw);
     if (r) return r;
     float a = 0;
     cudaEventElapsedTime(&a, e.ev[8], e.ev[5]);
