@@ -108,8 +108,13 @@ def test_fused_independent_of_tiling(comp, oracle, texts, cap, bits, wcap, lf):
 
 
 @pytest.mark.parametrize("l", [3, 8, 12, 16])
-def test_fused_independent_of_l(comp, oracle, texts, l):
-    text, k = texts["small_plain"]
+@pytest.mark.parametrize("cfg", ["small_plain", "wide_k63"])
+def test_fused_independent_of_l(comp, oracle, texts, cfg, l):
+    """Any l gives the same lines; a small l gives long runs of k-mers with
+    one minimizer, so warp tiles hold segments longer than k + 1 copies,
+    whose later chars come partly from their copies and partly from their
+    last k-mer."""
+    text, k = texts[cfg]
     want, _, _ = oracle.compact(text, k)
     assert fused_lines(comp, text, k, l) == sorted_lines(want)
 
@@ -137,6 +142,26 @@ def test_cycle_inside_one_tile(comp, oracle):
         assert fused_lines(comp, text, 21, 6) == sorted_lines(want)
     finally:
         comp.set_tuning(bucket_bits=0)
+
+
+@pytest.mark.parametrize("k", [21, 31, 47, 63])
+def test_long_segments_in_one_warp_tile(comp, oracle, k):
+    """One bucket per job (bucket_fill 1 and at most 226 k-mers), so a path
+    is one segment of one warp tile: its later chars come from its copies
+    up to the last k + 1 and from its last k-mer after that.  Paths of 1 to
+    220 k-mers, and a tile with two paths and a cycle."""
+    def path(n, seed):  # n k-mers
+        return walk_kmers(distinct_path(n + k - 1, k, seed=seed), k)
+    jobs = [path(n, n + k) for n in (1, 2, k - 1, k, k + 1, k + 2, 2 * k + 5, 220)]
+    jobs.append(path(90, 3) + path(60, 4) + cyclic_kmers(max(40, k + 5), k, seed=5))
+    comp.set_tuning(bucket_fill=1)
+    try:
+        for km in jobs:
+            text = text_of(shuffled(km, 7))
+            want, _, _ = oracle.compact(text, k)
+            assert fused_lines(comp, text, k, min(8, k - 1)) == sorted_lines(want)
+    finally:
+        comp.set_tuning(bucket_fill=0)
 
 
 def test_general_line_layout(comp, oracle):
