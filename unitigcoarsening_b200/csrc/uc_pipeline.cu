@@ -150,10 +150,16 @@ __device__ __forceinline__ uint32_t job_of_block(const JobTab* __restrict__ jobs
   return lo;
 }
 
-// Bucket counts while packing are 16-bit halves of 32-bit words, so that
-// 2^25 buckets take 64 MiB and the count atomics stay in L2; a half that
-// wraps raises *ovf, and the counts are then taken again at 32 bits
-// (k_count_buckets).  k_widen16 turns them into 32-bit counts.
+// Bucket counts while packing.  The resident path counts copies per group
+// of 2^cshift buckets in 32-bit words, at most 2^20 of them (4 MiB, so the
+// count reductions stay in L2 at 2^25 buckets); level 3 of the scatter counts
+// the buckets of each group itself.  The streamed path (cshift = CNT16)
+// counts every bucket in a 16-bit half of a 32-bit word (64 MiB at 2^25
+// buckets); a half that wraps shows up as a low total, and the counts are
+// then taken again at 32 bits (k_count_buckets).  k_widen16 turns them into
+// 32-bit counts.
+constexpr uint32_t CNT16 = 32;
+constexpr uint32_t COUNT_GROUPS_BITS = 20;
 __device__ __forceinline__ void count16(uint32_t* c16, uint32_t b) {
   // a reduction (no value returned, so no wait): a count that wraps its 16
   // bits carries into its neighbour or out of the word, which shows up on
@@ -186,7 +192,8 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
                                               const unsigned long long* __restrict__ starts, int k_arg,
                                               uint64_t* __restrict__ keys, uint32_t* err, int l_arg, uint64_t seed,
                                               uint32_t jb, uint32_t* __restrict__ b1, uint32_t* __restrict__ b2,
-                                              uint32_t* __restrict__ counts, uint32_t* __restrict__ jcross) {
+                                              uint32_t* __restrict__ counts, uint32_t cshift,
+                                              uint32_t* __restrict__ jcross) {
   __shared__ uint32_t buf[PACK_WORDS];
   __shared__ uint32_t s_cross;
   const int k = KC ? KC : k_arg;
@@ -342,11 +349,15 @@ __global__ void __launch_bounds__(256) k_pack(const JobTab* __restrict__ jobs, c
         __stcs(b1 + koff + line, a);
         __stcs(b2 + koff + line, b);
         if (counts) {  // (the streamed path's second pass only needs the buckets)
-          count16(counts, a);
-          if (a != b) {
-            count16(counts, b);
-            mycross = 1;
+          if (cshift == CNT16) {
+            count16(counts, a);
+            if (a != b) count16(counts, b);
+          } else {
+            // one 32-bit count per group of 2^cshift buckets (a reduction)
+            atomicAdd(counts + (a >> cshift), 1u);
+            if (a != b) atomicAdd(counts + (b >> cshift), 1u);
           }
+          mycross = (a != b) ? 1u : 0u;
         }
       }
     }
@@ -768,9 +779,9 @@ __global__ void k_mid_items(const unsigned long long* __restrict__ boff, uint32_
 template <int NW>
 __global__ void __launch_bounds__(MID_THREADS, NW == 1 ? 2 : 1) k_scatter_mid(
     const uint64_t* __restrict__ rkey, const uint32_t* __restrict__ rlink, const uint32_t* __restrict__ rbkt,
-    const unsigned long long* __restrict__ boff, const uint32_t* __restrict__ item_start, uint32_t fb, uint32_t sb,
-    uint32_t mc, unsigned long long* __restrict__ scur, uint64_t* __restrict__ okey, uint32_t* __restrict__ olink,
-    uint32_t* __restrict__ obkt, Counters* ctr) {
+    const unsigned long long* __restrict__ goff, uint32_t cg, const uint32_t* __restrict__ item_start, uint32_t fb,
+    uint32_t sb, uint32_t mc, unsigned long long* __restrict__ scur, uint64_t* __restrict__ okey,
+    uint32_t* __restrict__ olink, uint32_t* __restrict__ obkt, Counters* ctr) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);                              // [MID_CHUNK*NW]
   uint32_t* slink = reinterpret_cast<uint32_t*>(skey + MID_CHUNK * NW);              // [MID_CHUNK]
@@ -805,8 +816,10 @@ __global__ void __launch_bounds__(MID_THREADS, NW == 1 ? 2 : 1) k_scatter_mid(
     const uint32_t t = s_t, p = s_p;
     __syncthreads();
     if (t >= nitems) break;
-    const unsigned long long pend = boff[uint64_t(p + 1) << fb];
-    const unsigned long long c0 = boff[uint64_t(p) << fb] + uint64_t(t - istart[p]) * MID_CHUNK;
+    // (goff: offsets of count groups of 2^cg buckets; partition p starts at
+    // group p << (fb - cg))
+    const unsigned long long pend = goff[uint64_t(p + 1) << (fb - cg)];
+    const unsigned long long c0 = goff[uint64_t(p) << (fb - cg)] + uint64_t(t - istart[p]) * MID_CHUNK;
     const uint32_t cn = uint32_t(min(pend - c0, (unsigned long long)MID_CHUNK));
     const uint32_t sub0 = p << (fb - sb);  // first sub-partition of partition p
     // the chunk's records, all loads issued at once (in registers), and the
@@ -880,53 +893,70 @@ __global__ void __launch_bounds__(MID_THREADS, NW == 1 ? 2 : 1) k_scatter_mid(
   }
 }
 
-// Level 3: one block owns a sub-partition (2^sb buckets) and places each of
-// its records at its bucket's offset plus a rank from a shared-memory
-// cursor: no global atomics.  A sub-partition of at most `cap` records is
-// assembled in shared memory and written out as one contiguous range; a
-// larger one (a large repeat bucket) is placed straight into global memory.
-// Blocks take sub-partitions from a counter.
+// Level 3: one block owns a sub-partition (2^sb buckets, whole count
+// groups of the pack).  With count groups (cout given) it counts its
+// records per bucket in shared memory, takes the buckets' offsets from a
+// block scan and writes every bucket's count (and offset, to bout) for the
+// tile plan; otherwise goff holds every bucket's offset.  It then places
+// each record at its bucket's offset plus a rank from a shared-memory
+// cursor: no global atomics.  A sub-partition of at most
+// `cap` records is assembled in shared memory and written out as one
+// contiguous range; a larger one (a large repeat bucket) is placed straight
+// into global memory.  Blocks take sub-partitions from a counter.
 template <int NW>
-__global__ void __launch_bounds__(512) k_scatter_sub(const uint64_t* __restrict__ ikey,
+__global__ void __launch_bounds__(512, 2) k_scatter_sub(const uint64_t* __restrict__ ikey,
                                                      const uint32_t* __restrict__ ilink,
                                                      const uint32_t* __restrict__ ibkt,
-                                                     const unsigned long long* __restrict__ boff, uint32_t sb,
-                                                     uint32_t nsub, uint32_t cap, uint64_t* __restrict__ pkeys,
-                                                     uint32_t* __restrict__ plink, Counters* ctr) {
+                                                     const unsigned long long* __restrict__ goff, uint32_t gsh,
+                                                     uint32_t sb, uint32_t nsub, uint32_t cap,
+                                                     uint64_t* __restrict__ pkeys, uint32_t* __restrict__ plink,
+                                                     uint32_t* __restrict__ cout, unsigned long long* __restrict__ bout,
+                                                     Counters* ctr) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   uint64_t* skey = reinterpret_cast<uint64_t*>(sm_raw);        // [cap * NW]
   uint32_t* slink = reinterpret_cast<uint32_t*>(skey + size_t(cap) * NW);  // [cap]
   __shared__ unsigned long long s_off[1 << SUB_MAX_BITS];
   __shared__ uint32_t s_cur[1 << SUB_MAX_BITS];
   __shared__ uint32_t s_sp;
-  const uint32_t nbk = 1u << sb;
-  constexpr int PER = 4;  // records per thread and pass: their loads are in flight together
+  __shared__ uint32_t sc[33];
+  const uint32_t nbk = 1u << sb;  // <= 2^SUB_MAX_BITS <= blockDim.x
+  // records per thread and pass: their loads are in flight together (two
+  // CTAs per SM fit the registers)
+  constexpr int PER = NW == 1 ? 8 : 4;
   for (;;) {
     if (threadIdx.x == 0) s_sp = atomicAdd(&ctr->work_next, 1u);
     __syncthreads();
     const uint32_t sp = s_sp;
     if (sp >= nsub) break;
     const uint64_t b0 = uint64_t(sp) << sb;
+    const unsigned long long lo = goff[uint64_t(sp) << gsh], hi = goff[uint64_t(sp + 1) << gsh];
+    // known: goff holds every bucket's offset (no count groups)
+    const bool known = cout == nullptr;
     for (uint32_t j = threadIdx.x; j < nbk; j += blockDim.x) {
-      s_off[j] = boff[b0 + j];
+      if (known) s_off[j] = goff[b0 + j];
       s_cur[j] = 0;
     }
     __syncthreads();
-    const unsigned long long lo = boff[b0], hi = boff[b0 + nbk];
     const bool staged = hi - lo <= cap;
-    for (unsigned long long i0 = lo; i0 < hi; i0 += uint64_t(blockDim.x) * PER) {
-      uint32_t bk[PER];
-      Key<NW> kk[PER];
-      uint32_t ln[PER];
+    // the first PER x blockDim records stay in registers from the count to
+    // their placement; the rest are counted from their bucket ids and
+    // loaded again to be placed
+    uint32_t bk[PER];
+    Key<NW> kk[PER];
+    uint32_t ln[PER];
+    auto load = [&](unsigned long long i0) {
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
         const unsigned long long i = i0 + uint64_t(q) * blockDim.x + threadIdx.x;
+        bk[q] = 0xFFFFFFFFu;
         if (i < hi) {
           bk[q] = ibkt[i];
           kk[q] = ld_key<NW>(ikey, i);
           ln[q] = ilink[i];
         }
       }
+    };
+    auto place = [&](unsigned long long i0) {
 #pragma unroll
       for (int q = 0; q < PER; ++q) {
         const unsigned long long i = i0 + uint64_t(q) * blockDim.x + threadIdx.x;
@@ -946,6 +976,48 @@ __global__ void __launch_bounds__(512) k_scatter_sub(const uint64_t* __restrict_
           }
         }
       }
+    };
+    const uint64_t batch = uint64_t(blockDim.x) * PER;
+    load(lo);
+    if (!known) {
+      // the sub-partition's counts per bucket (records of another
+      // sub-partition are flagged when placed)
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const uint32_t lb = bk[q] - uint32_t(b0);
+        if (lb < nbk) atomicAdd(s_cur + lb, 1u);
+      }
+      for (unsigned long long i0 = lo + batch; i0 < hi; i0 += batch) {
+        uint32_t bq[PER];
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+          const unsigned long long i = i0 + uint64_t(q) * blockDim.x + threadIdx.x;
+          bq[q] = (i < hi) ? ibkt[i] : 0xFFFFFFFFu;
+        }
+#pragma unroll
+        for (int q = 0; q < PER; ++q) {
+          const uint32_t lb = bq[q] - uint32_t(b0);
+          if (lb < nbk) atomicAdd(s_cur + lb, 1u);
+        }
+      }
+      __syncthreads();
+      {
+        const uint32_t cnt = threadIdx.x < nbk ? s_cur[threadIdx.x] : 0u;
+        uint32_t tot;
+        const uint32_t ex = block_excl_scan(cnt, sc, &tot);
+        if (threadIdx.x < nbk) {
+          s_off[threadIdx.x] = lo + ex;
+          s_cur[threadIdx.x] = 0;
+          cout[b0 + threadIdx.x] = cnt;
+          if (bout) bout[b0 + threadIdx.x] = lo + ex;
+        }
+      }
+      __syncthreads();
+    }
+    place(lo);
+    for (unsigned long long i0 = lo + batch; i0 < hi; i0 += batch) {
+      load(i0);
+      place(i0);
     }
     __syncthreads();
     if (staged) {
@@ -954,8 +1026,8 @@ __global__ void __launch_bounds__(512) k_scatter_sub(const uint64_t* __restrict_
         st_key<NW>(pkeys, lo + t, ld_key<NW>(skey, t));
         plink[lo + t] = slink[t];
       }
-      __syncthreads();  // the staging area, s_off / s_cur / s_sp are reused
     }
+    __syncthreads();  // the staging area, s_off / s_cur / s_sp are reused
   }
 }
 
@@ -2550,7 +2622,9 @@ struct FuseArgs {
   uint64_t seed = 0;
   uint32_t jb = 0;
   uint32_t *b1 = nullptr, *b2 = nullptr, *jcross = nullptr;
-  uint32_t* counts = nullptr;  // 16-bit counts, two per word ((M + 1) / 2 words)
+  uint32_t* counts = nullptr;  // group counts (cshift), or 16-bit counts two per word (CNT16)
+  uint32_t cshift = CNT16;
+  uint64_t cbytes = 0;         // bytes of counts to clear before a second pack
   uint64_t M = 0;
 };
 
@@ -2575,7 +2649,7 @@ static bool launch_pack_fixed_l(Env& e, const JobTab* jobs, const JobTab& J, uin
   ++e.launches;
   k_pack<NW, true, false, KC, LC><<<grid, 256, 0, e.stream>>>(jobs, J, 1, nblocks, nullptr, KC, keys, &e.ctr->err,
                                                                LC, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
-                                                               fz->jcross);
+                                                               fz->cshift, fz->jcross);
   return true;
 }
 
@@ -2615,17 +2689,17 @@ static void launch_pack(Env& e, const JobTab* jobs, const JobTab* one, uint32_t 
   if (fz && one)
     k_pack<NW, true, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
                                                         fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
-                                                        fz->jcross);
+                                                        fz->cshift, fz->jcross);
   else if (fz)
     k_pack<NW, true, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err,
                                                        fz->l, fz->seed, fz->jb, fz->b1, fz->b2, fz->counts,
-                                                       fz->jcross);
+                                                       fz->cshift, fz->jcross);
   else if (one)
     k_pack<NW, false, false><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
-                                                         0, 0, nullptr, nullptr, nullptr, nullptr);
+                                                         0, 0, nullptr, nullptr, nullptr, CNT16, nullptr);
   else
     k_pack<NW, false, true><<<grid, 256, 0, e.stream>>>(jobs, J, njobs, nblocks, starts, k, keys, &e.ctr->err, 0,
-                                                        0, 0, nullptr, nullptr, nullptr, nullptr);
+                                                        0, 0, nullptr, nullptr, nullptr, CNT16, nullptr);
 }
 
 // Grow-only device buffers for the job table and the per-job counters.
@@ -2690,7 +2764,7 @@ static int pack_single(Env& e, const char* d_text, size_t bytes, int k, uint64_t
       fixed = false;
       UC_CK(cudaMemsetAsync(&e.ctr->err, 0, 4, e.stream));
       if (fz) {
-        UC_CK(cudaMemsetAsync(fz->counts, 0, (fz->M + 1) / 2 * 4, e.stream));
+        UC_CK(cudaMemsetAsync(fz->counts, 0, fz->cbytes, e.stream));
         UC_CK(cudaMemsetAsync(fz->jcross, 0, 4, e.stream));
       }
     } else if (e.h_ctr->err) {
@@ -2780,9 +2854,18 @@ int minimizers(Env& e, const uint64_t* d_keys, uint64_t n, int k, int l, uint64_
 // bits = log2 of that).
 struct Plan {
   uint32_t bits, jb, cap, pack, tslots, wcap, wts, wbytes, lf;
+  uint32_t cg;  // the pack's count groups: 2^cg buckets each
   int l_used;
   uint64_t M;
 };
+
+// Count groups of 2^bits buckets: at most 2^COUNT_GROUPS_BITS of them,
+// from 2^24 buckets on (below that one 32-bit count per bucket, at most
+// 32 MiB, stays in L2 and level 3 needs no counting pass).
+static uint32_t count_group_bits(uint32_t bits) {
+  return bits >= 24 ? bits - COUNT_GROUPS_BITS : 0u;
+}
+static uint64_t count_groups(uint64_t M) { return std::min<uint64_t>(M, 1ull << COUNT_GROUPS_BITS); }
 
 static uint32_t ceil_log2(uint64_t x) {
   uint32_t b = 0;
@@ -2834,13 +2917,14 @@ static Plan plan_buckets(const Env& e, uint64_t nmax, uint32_t njobs, int k, int
   P.wbytes = warp_tier ? uint32_t((tile_bytes(nw, wcap, P.wts) + 15) & ~size_t(15)) : 0;
   P.l_used = lu;
   P.M = 1ull << P.bits;
+  P.cg = count_group_bits(P.bits);
   return P;
 }
 
 struct Front {
   uint64_t* keys;
-  uint32_t *b1, *b2, *counts, *c16;
-  unsigned long long *boff, *cursor, *fcur, *tile_begin, *scan_tmp;
+  uint32_t *b1, *b2, *counts, *c16, *gcount;
+  unsigned long long *boff, *cursor, *fcur, *tile_begin, *scan_tmp, *goff;
   uint32_t *flag, *fidx, *big_list, *wlist, *blist, *tile_job;
   unsigned long long* big_size;
 };
@@ -2853,6 +2937,7 @@ static size_t front_bytes(uint64_t n, int nw, uint64_t M, bool own_keys) {
   add(scan_tmp_elems(M) * 8); add(M * 4); add((M + 1) * 4); add(M * 4); add(M * 8);
   add(M * 4); add(M * 4); add(M * 4);
   add((M + 1) / 2 * 4);
+  add(count_groups(M) * 4); add((count_groups(M) + 1) * 8);
   return need;
 }
 
@@ -2874,19 +2959,26 @@ static int take_front(Env& e, uint64_t n, int nw, uint64_t M, bool own_keys, Fro
   f.blist = static_cast<uint32_t*>(e.take(0, M * 4));
   f.tile_job = static_cast<uint32_t*>(e.take(0, M * 4));
   f.c16 = static_cast<uint32_t*>(e.take(0, (M + 1) / 2 * 4));
-  if (!f.c16) return e.fail(UC_EBUDGET, "front arena overflow");
+  f.gcount = static_cast<uint32_t*>(e.take(0, count_groups(M) * 4));
+  f.goff = static_cast<unsigned long long*>(e.take(0, (count_groups(M) + 1) * 8));
+  if (!f.goff) return e.fail(UC_EBUDGET, "front arena overflow");
   return UC_OK;
 }
 
-// counts -> bucket offsets; returns the total number of copies (host sync).
-static int bucket_offsets(Env& e, const Front& f, uint64_t M, uint64_t& copies) {
+// counts -> offsets (M entries: buckets or count groups); returns the total
+// number of copies (host sync).
+static int bucket_offsets(Env& e, const Front& f, const uint32_t* counts, uint64_t M, unsigned long long* offs,
+                          uint64_t& copies) {
   e.launches += 6;
-  scan_excl<uint32_t, unsigned long long>(f.counts, M, f.boff, f.scan_tmp, e.stream);
+  scan_excl<uint32_t, unsigned long long>(counts, M, offs, f.scan_tmp, e.stream);
   unsigned long long tot = 0;
-  UC_CK(cudaMemcpyAsync(&tot, f.boff + M, 8, cudaMemcpyDeviceToHost, e.stream));
+  UC_CK(cudaMemcpyAsync(&tot, offs + M, 8, cudaMemcpyDeviceToHost, e.stream));
   UC_CK(cudaStreamSynchronize(e.stream));
   copies = tot;
   return UC_OK;
+}
+static int bucket_offsets(Env& e, const Front& f, uint64_t M, uint64_t& copies) {
+  return bucket_offsets(e, f, f.counts, M, f.boff, copies);
 }
 
 // Let a kernel take all the dynamic shared memory an SM offers a block.  The
@@ -2941,6 +3033,12 @@ static int plan_tiles(Env& e, const Front& f, const Plan& P) {
 // its cursors and the cross-index counter carry over.
 struct Scatter {
   uint32_t mcb = 0, fb = 0, mc = 0, sb = 0, nsub = 0, cap3 = 0;
+  // offsets of the pack's count groups (2^cg buckets each); level 3 writes
+  // every bucket's count and offset to cout / bout (null: they are known)
+  const unsigned long long* goff = nullptr;
+  uint32_t cg = 0;
+  uint32_t* cout = nullptr;
+  unsigned long long* bout = nullptr;
   bool mid = false;
   int nw = 1;
   uint64_t copies = 0;
@@ -2948,11 +3046,18 @@ struct Scatter {
   uint32_t *l1 = nullptr, *l2 = nullptr, *b1 = nullptr, *b2 = nullptr;
 };
 
+// cg > 0: the copies are counted per group of 2^cg buckets (offsets in
+// f.goff) and level 3 writes f.counts and f.boff; cg = 0 with
+// group_offsets false: f.boff holds every bucket's offset already.
 static int scatter_begin(Env& e, const Front& f, const Plan& P, int nw, char* r1, char* r2, uint64_t copies,
-                         Scatter& sc) {
+                         Scatter& sc, uint32_t cg = 0, bool group_offsets = false) {
   const uint64_t M = P.M;
   sc.nw = nw;
   sc.copies = copies;
+  sc.cg = cg;
+  sc.goff = group_offsets ? f.goff : f.boff;
+  sc.cout = group_offsets ? f.counts : nullptr;
+  sc.bout = group_offsets ? f.boff : nullptr;
   auto region = [&](char* base, uint64_t*& key, uint32_t*& link, uint32_t*& bkt) {
     key = reinterpret_cast<uint64_t*>(base);
     link = reinterpret_cast<uint32_t*>(base + copies * 8ull * nw);
@@ -2971,8 +3076,10 @@ static int scatter_begin(Env& e, const Front& f, const Plan& P, int nw, char* r1
   sbi = std::min(sbi, SUB_MAX_BITS);
   sbi = std::min(sbi, int(sc.fb));
   sbi = std::max(sbi, int(sc.fb) - int(std::log2(double(MID_MAX_BINS))));
+  sbi = std::max(sbi, int(cg));  // a sub-partition is whole count groups
   sbi = std::max(sbi, 0);
-  if (sbi > SUB_MAX_BITS) return e.fail(UC_EINTERNAL, "bucket count beyond the three scatter levels");
+  if (sbi > SUB_MAX_BITS || sbi > int(sc.fb))
+    return e.fail(UC_EINTERNAL, "bucket count beyond the three scatter levels");
   sc.sb = uint32_t(sbi);
   sc.mid = sc.sb < sc.fb;
   sc.nsub = uint32_t(M >> sc.sb);
@@ -2985,7 +3092,7 @@ static int scatter_begin(Env& e, const Front& f, const Plan& P, int nw, char* r1
   if (r0) return r0;
   UC_CK(cudaMemsetAsync(&e.ctr->cross_count, 0, 4, e.stream));
   e.launches += 1;
-  k_coarse_init<<<grid_for(e, sc.mc, 256), 256, 0, e.stream>>>(f.boff, sc.fb, sc.mc, f.cursor);
+  k_coarse_init<<<grid_for(e, sc.mc, 256), 256, 0, e.stream>>>(sc.goff, sc.fb - sc.cg, sc.mc, f.cursor);
   UC_CK(cudaGetLastError());
   return UC_OK;
 }
@@ -3018,7 +3125,14 @@ static int scatter_finish(Env& e, const Front& f, const Scatter& sc, uint64_t*& 
   const int nw = sc.nw;
   pkeys = sc.k2;
   plink = sc.l2;
-  if (sc.copies == 0) return UC_OK;
+  if (sc.copies == 0) {
+    if (sc.bout) {  // no copies: every bucket empty
+      const uint64_t M = uint64_t(sc.nsub) << sc.sb;
+      UC_CK(cudaMemsetAsync(sc.cout, 0, M * 4, e.stream));
+      UC_CK(cudaMemsetAsync(sc.bout, 0, (M + 1) * 8, e.stream));
+    }
+    return UC_OK;
+  }
   if (sc.mid) {
     const uint32_t nb = 1u << (sc.fb - sc.sb);
     uint32_t* item_start = reinterpret_cast<uint32_t*>(f.cursor + sc.mc);
@@ -3028,17 +3142,17 @@ static int scatter_finish(Env& e, const Front& f, const Scatter& sc, uint64_t*& 
     else UC_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o2, k_scatter_mid<2>, MID_THREADS, sm2));
     if (o2 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
     e.launches += 3;
-    k_mid_items<<<1, 256, 0, e.stream>>>(f.boff, sc.fb, sc.mc, item_start);
-    k_coarse_init<<<grid_for(e, sc.nsub, 256), 256, 0, e.stream>>>(f.boff, sc.sb, sc.nsub, f.fcur);
+    k_mid_items<<<1, 256, 0, e.stream>>>(sc.goff, sc.fb - sc.cg, sc.mc, item_start);
+    k_coarse_init<<<grid_for(e, sc.nsub, 256), 256, 0, e.stream>>>(sc.goff, sc.sb - sc.cg, sc.nsub, f.fcur);
     UC_CK(cudaMemsetAsync(&e.ctr->work_next, 0, 4, e.stream));
     if (nw == 1)
-      k_scatter_mid<1><<<e.sm_count * o2, MID_THREADS, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start,
-                                                                        sc.fb, sc.sb, sc.mc, f.fcur, sc.k2, sc.l2,
-                                                                        sc.b2, e.ctr);
+      k_scatter_mid<1><<<e.sm_count * o2, MID_THREADS, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, sc.goff, sc.cg,
+                                                                        item_start, sc.fb, sc.sb, sc.mc, f.fcur,
+                                                                        sc.k2, sc.l2, sc.b2, e.ctr);
     else
-      k_scatter_mid<2><<<e.sm_count * o2, MID_THREADS, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, f.boff, item_start,
-                                                                        sc.fb, sc.sb, sc.mc, f.fcur, sc.k2, sc.l2,
-                                                                        sc.b2, e.ctr);
+      k_scatter_mid<2><<<e.sm_count * o2, MID_THREADS, sm2, e.stream>>>(sc.k1, sc.l1, sc.b1, sc.goff, sc.cg,
+                                                                        item_start, sc.fb, sc.sb, sc.mc, f.fcur,
+                                                                        sc.k2, sc.l2, sc.b2, e.ctr);
     pkeys = sc.k1;
     plink = sc.l1;
   }
@@ -3054,10 +3168,17 @@ static int scatter_finish(Env& e, const Front& f, const Scatter& sc, uint64_t*& 
   if (o3 < 1) return e.fail(UC_EINTERNAL, "scatter kernel does not fit an SM");
   const int g3 = int(std::min<uint64_t>(sc.nsub, uint64_t(e.sm_count) * uint64_t(o3)));
   if (nw == 1)
-    k_scatter_sub<1><<<g3, 512, sm3, e.stream>>>(ik, il, ib, f.boff, sc.sb, sc.nsub, sc.cap3, pkeys, plink, e.ctr);
+    k_scatter_sub<1><<<g3, 512, sm3, e.stream>>>(ik, il, ib, sc.goff, sc.sb - sc.cg, sc.sb, sc.nsub, sc.cap3, pkeys,
+                                                 plink, sc.cout, sc.bout, e.ctr);
   else
-    k_scatter_sub<2><<<g3, 512, sm3, e.stream>>>(ik, il, ib, f.boff, sc.sb, sc.nsub, sc.cap3, pkeys, plink, e.ctr);
+    k_scatter_sub<2><<<g3, 512, sm3, e.stream>>>(ik, il, ib, sc.goff, sc.sb - sc.cg, sc.sb, sc.nsub, sc.cap3, pkeys,
+                                                 plink, sc.cout, sc.bout, e.ctr);
   UC_CK(cudaGetLastError());
+  if (sc.bout) {
+    // the total after the last bucket, for the tile plan
+    UC_CK(cudaMemcpyAsync(sc.bout + (uint64_t(sc.nsub) << sc.sb), sc.goff + (uint64_t(sc.nsub) << (sc.sb - sc.cg)),
+                          8, cudaMemcpyDeviceToDevice, e.stream));
+  }
   return UC_OK;
 }
 
@@ -3071,17 +3192,19 @@ static int classify_tiles(Env& e, const Front& f, const Plan& P, int nw, uint32_
   return UC_OK;
 }
 
-// Tiles, then the bucketed copies of all k-mers in one pass.
+// The bucketed copies of all k-mers in one pass, then the tiles (from the
+// bucket counts, which level 3 writes when the pack counted groups).
 static int plan_and_scatter(Env& e, const Front& f, const Plan& P, uint64_t n, int nw, int ids_mode,
-                            char* r1, char* r2, uint64_t copies, uint64_t*& pkeys, uint32_t*& plink) {
-  int r = plan_tiles(e, f, P);
-  if (r) return r;
+                            char* r1, char* r2, uint64_t copies, uint64_t*& pkeys, uint32_t*& plink,
+                            bool group_offsets = false) {
   Scatter sc;
-  r = scatter_begin(e, f, P, nw, r1, r2, copies, sc);
+  int r = scatter_begin(e, f, P, nw, r1, r2, copies, sc, group_offsets ? P.cg : 0u, group_offsets);
   if (r) return r;
   r = scatter_l1(e, f, sc, f.keys, f.b1, f.b2, n, ids_mode);
   if (r) return r;
   r = scatter_finish(e, f, sc, pkeys, plink);
+  if (r) return r;
+  r = plan_tiles(e, f, P);
   if (r) return r;
   return classify_tiles(e, f, P, nw);
 }
@@ -3813,8 +3936,12 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   Front f{};
   r = take_front(e, N, nw, P.M, true, f);
   if (r) return r;
+  // the pack's counts: per group of 2^cg buckets, or (cg = 0) per bucket
+  const uint64_t G = P.M >> P.cg;
+  uint32_t* gcount = P.cg ? f.gcount : f.counts;
+  unsigned long long* goff = P.cg ? f.goff : f.boff;
   UC_CK(cudaMemsetAsync(e.ctr, 0, sizeof(Counters), e.stream));
-  UC_CK(cudaMemsetAsync(f.c16, 0, (P.M + 1) / 2 * 4, e.stream));
+  UC_CK(cudaMemsetAsync(gcount, 0, G * 4, e.stream));
   UC_CK(cudaMemsetAsync(jd.jcross, 0, njobs * 4, e.stream));
   UC_CK(cudaMemcpyAsync(jd.tab, J.data(), njobs * sizeof(JobTab), cudaMemcpyHostToDevice, e.stream));
   cudaEventRecord(e.ev[0], e.stream);
@@ -3824,7 +3951,9 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   fz.jb = P.jb;
   fz.b1 = f.b1;
   fz.b2 = f.b2;
-  fz.counts = f.c16;
+  fz.counts = gcount;
+  fz.cshift = P.cg;
+  fz.cbytes = G * 4;
   fz.jcross = jd.jcross;
   fz.M = P.M;
   if (njobs == 1) {
@@ -3837,10 +3966,8 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   }
   cudaEventRecord(e.ev[1], e.stream);
   if (e.after_pack) e.after_pack();
-  ++e.launches;
-  k_widen16<<<grid_for(e, P.M, 256), 256, 0, e.stream>>>(f.c16, P.M, f.counts);
   uint64_t copies = 0;
-  r = bucket_offsets(e, f, P.M, copies);
+  r = bucket_offsets(e, f, gcount, G, goff, copies);
   if (r) return r;
   std::vector<uint32_t> xc(njobs);
   UC_CK(cudaMemcpyAsync(xc.data(), jd.jcross, njobs * 4, cudaMemcpyDeviceToHost, e.stream));
@@ -3848,15 +3975,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   if (r) return r;
   uint64_t xsum = 0;
   for (uint32_t j = 0; j < njobs; ++j) xsum += xc[j];
-  if (copies != N + xsum && !e.h_ctr->err) {
-    // a bucket holds 65536 copies or more (its 16-bit count wrapped): count
-    // again at 32 bits
-    UC_CK(cudaMemsetAsync(f.counts, 0, P.M * 4, e.stream));
-    e.launches += 1;
-    k_count_buckets<<<grid_for(e, N, 256), 256, 0, e.stream>>>(f.b1, f.b2, N, f.counts);
-    r = bucket_offsets(e, f, P.M, copies);
-    if (r) return r;
-  }
+  if (copies != N + xsum && !e.h_ctr->err) return e.fail(UC_EINTERNAL, "bucket counts disagree with the copies");
   if (e.h_ctr->err) {
     if (e.h_ctr->err & ERR_LAYOUT) return e.fail(UC_EINPUT, "a k-mer line is shorter than k");
     return e.check_err(e.h_ctr);
@@ -3909,7 +4028,7 @@ int compact_batch(Env& e, uint32_t njobs, const char* const* texts, const size_t
   UC_CK(cudaMemsetAsync(jd.jseg, 0, njobs * 4, e.stream));
   uint64_t* pkeys = nullptr;
   uint32_t* plink = nullptr;
-  r = plan_and_scatter(e, f, P, N, nw, 0, region1, region2, copies, pkeys, plink);
+  r = plan_and_scatter(e, f, P, N, nw, 0, region1, region2, copies, pkeys, plink, P.cg > 0);
   if (r) return r;
   cudaEventRecord(e.ev[2], e.stream);
 
