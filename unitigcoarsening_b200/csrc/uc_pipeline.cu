@@ -1485,61 +1485,60 @@ __device__ void process_tile(const TileParams& p, const TileMem<NW, IT>& m, uint
   unsigned long long s_base[3];
   if (!G::reserve(p, job, tot, s_base)) return;
   const unsigned long long cbase = s_base[0], obase = s_base[1], sbase = s_base[2];
+  // per segment (the lane that sized it): its offset (kept at its start for
+  // the per-copy pass), its first k-mer in full (a segment that starts at an
+  // S-only copy keeps only the chars it adds to its line: that k-mer ends
+  // the segment before), then its line break or, for an open segment, its
+  // record.  The cross indices the record needs are loaded first, so that
+  // they arrive while the rest is worked out.
   for (uint32_t j = G::rank(); j < nend; j += G::size()) {
     const uint32_t i = end_at(j);
     if (i == NONE_I) continue;
     const uint32_t s = ptr[i];
-    const uint32_t len = uint32_t(rnk[i]) + 1;
-    const bool starts_p = (roles(skey(m, s)) & ROLE_P) != 0;
-    const bool closed = starts_p && (roles(skey(m, i)) & ROLE_S);
+    const Key<NW> ks = skey(m, s);
+    const uint64_t re = roles(skey(m, i));
+    const bool starts_p = (roles(ks) & ROLE_P) != 0;
+    const bool p_only = (re & ROLE_S) == 0;
+    const bool closed = starts_p && !p_only;
+    const uint32_t xs = starts_p ? NONE : p.plink[beg + s];  // this segment's id (S-only start)
+    const uint32_t xe = p_only ? p.plink[beg + i] : NONE;   // the next segment's id
+    const uint32_t r = rnk[i];
+    const uint32_t len = r + 1;
     uint64_t loc;
+    uint32_t sid;
     if (closed) {
       loc = pre.a;
-      m.P[s] = IT(NONE_I);
+      sid = NONE_I;
       pre.a += uint64_t(k) + len;
     } else {
       loc = pre.b;
-      m.P[s] = IT(starts_p ? uint32_t(pre.c) : OPEN_S);
+      sid = starts_p ? uint32_t(pre.c) : OPEN_S;
       pre.b += starts_p ? uint64_t(k) - 1 + len : uint64_t(len) - 1;
       if (starts_p) pre.c += 1;
     }
+    m.P[s] = IT(sid);
     if constexpr (sizeof(IT) == 2) {
       lo_a[s] = IT(loc & 0xFFFFu);
       hi_a[s] = IT(loc >> 16);
     } else {
       lo_a[s] = IT(loc);
     }
-  }
-  G::sync();
-  // per segment: its first k-mer in full (a segment that starts at an
-  // S-only copy keeps only the chars it adds to its line: that k-mer ends
-  // the segment before), then its line break or, for an open segment, its
-  // record
-  for (uint32_t j = G::rank(); j < nend; j += G::size()) {
-    const uint32_t i = end_at(j);
-    if (i == NONE_I) continue;
-    const uint32_t s = ptr[i];
-    const uint32_t r = rnk[i];
-    uint64_t loc = lo_a[s];
-    if constexpr (sizeof(IT) == 2) loc |= uint64_t(hi_a[s]) << 16;
-    const uint32_t sid = m.P[s];
-    char* dst = (sid == NONE_I) ? (p.out + cbase + loc) : (p.segchars + obase + loc);
-    if (sid != OPEN_S) spell_key<NW>(dst, skey(m, s), k);
-    if (sid == NONE_I) {
+    char* dst = closed ? (p.out + cbase + loc) : (p.segchars + obase + loc);
+    if (sid != OPEN_S) spell_key<NW>(dst, ks, k);
+    if (closed) {
       dst[k + r] = '\n';
     } else {
       // the segment's record under its id; a segment that ends at the P-only
-      // copy of cross k-mer ex continues in segment ex
-      const bool head = sid != OPEN_S;
-      const bool p_only = (roles(skey(m, i)) & ROLE_S) == 0;
-      const uint32_t g = head ? p.xcount + uint32_t(sbase) + sid : p.plink[beg + s];
+      // copy of cross k-mer xe continues in segment xe
+      const uint32_t g = starts_p ? p.xcount + uint32_t(sbase) + sid : xs;
       SegRec rec;
       rec.off_job = (obase + loc) | (static_cast<unsigned long long>(job) << SEG_OFF_BITS);
-      rec.len = r + 1;
-      rec.next = p_only ? p.plink[beg + i] : NONE;
+      rec.len = len;
+      rec.next = xe;
       p.seg[g] = rec;
     }
   }
+  G::sync();
   // every later copy of a segment adds its last char
   for (uint32_t i = G::rank(); i < c; i += G::size()) {
     const uint32_t r = rnk[i];
