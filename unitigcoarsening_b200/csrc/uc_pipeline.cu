@@ -2200,8 +2200,8 @@ __global__ void k_hec_level0(HecPool h, const uint32_t* __restrict__ prev, const
 }
 
 // Level 0 from the fused path's segments: next from the records, prev from
-// the first ranking state the tiles wrote (ids [0, nx) only: a line's first
-// segment has none), weights from the lengths.  Unused head-pool ids have
+// the ranking's first state built from them (k_seg_xinit; ids [0, nx) only:
+// a line's first segment has none), weights from the lengths.  Unused head-pool ids have
 // length 0 and stay isolated.
 __global__ void k_hec_level0_seg(HecPool h, const SegRec* __restrict__ seg, const unsigned long long* __restrict__ X0,
                                  uint64_t S, uint32_t nx, int k) {
@@ -3467,7 +3467,8 @@ static uint32_t hec_rounds(const Env& e, uint64_t nmax) {
 // HEC contraction of the lists (prev, next, w) into X (pointer | HEAD_BIT,
 // offset) and cycle flags, all rounds enqueued on the stream.
 // With seg, level 0 comes from the fused path's segment records and the
-// first ranking state in X (nx cross indices) instead of (prev, next, w).
+// ranking's first state in X (built from them by k_seg_xinit; nx cross
+// indices) instead of (prev, next, w).
 static void hec_contract(Env& e, HecPool& h, uint32_t R, const uint32_t* prev, const uint32_t* next,
                          const uint32_t* w, uint64_t nmax, bool count_on_device, unsigned long long* X,
                          uint8_t* oncycle, const SegRec* seg = nullptr, uint32_t nx = 0, int k = 0) {
