@@ -107,3 +107,31 @@ def test_cli_check_rejects_bad_arguments(tmp_path):
     inp.write_text("3\nACG\nCGT\nGTA\n")
     r = subprocess.run([B.CLI, str(inp), "3", "3", str(tmp_path / "o.txt"), "--check"], capture_output=True, text=True)
     assert r.returncode != 0  # l must be below k
+
+
+def test_binding_structs_match_the_header(tmp_path):
+    """The ctypes structures of the Python binding have the sizes and field
+    offsets of the C structs in include/uc.h (compiled and printed by the
+    host compiler; a field renamed or reordered on one side fails here)."""
+    from unitigcoarsening_b200 import api
+    structs = {"uc_stats": api.Stats, "uc_tuning": api.Tuning, "uc_faults": api.Faults,
+               "uc_server_config": api.ServerConfig, "uc_server_job_info": api.JobInfo,
+               "uc_server_totals": api.ServerTotals}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "uc.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'  printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        name, field, value = ln.split()
+        got[(name, field)] = int(value)
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == ctypes.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
